@@ -1,0 +1,127 @@
+/* pgc.h -- C ABI of the sm_100a cycle-search library (libpgc.so).
+ *
+ * One handle is one product_graph_generator of the reference (class
+ * ProductGraphGenerators, product_graph_generators/product_graph_generators.hpp:21-91,
+ * bound to Python at pythonbinding/bindings.cpp:32-48 and to MATLAB at
+ * mex/product_graph_generator_mex.cpp:29-151).  Each entry point below names
+ * the reference member it replaces.
+ *
+ * Conventions
+ *  - Matrices are dense, row-major (C order); indices are 0-based int32.
+ *  - Every function returns PGC_OK (0) or a negative PGC_ERR_* code; the
+ *    message of the last failure of the calling thread is pgc_last_error().
+ *    Nothing calls exit().
+ *  - A handle is not thread-safe; distinct handles may be used from
+ *    distinct threads.  All device work of a handle runs on one CUDA stream
+ *    of the device that was current when the handle was created.
+ *  - All solver names of the reference are accepted.  "lawlercpu" and
+ *    "lawlergpu" both run the sm_100a ratio solver, "dijkstracpu" and
+ *    "dijkstragpu" (and, as in the reference, any other name) the sm_100a
+ *    minimum-cost solver; their results are identical by construction.
+ *    "export" writes the inputs as CSV files, as the reference does.
+ */
+#ifndef PGC_H
+#define PGC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGC_OK 0
+#define PGC_ERR_ARG -1        /* bad shape, index or argument */
+#define PGC_ERR_STATE -2      /* call not allowed in the current state */
+#define PGC_ERR_MODE -3       /* unsupported (cost, time) mode */
+#define PGC_ERR_SOLVER -4     /* unknown ratio-solver name */
+#define PGC_ERR_CUDA -5       /* CUDA runtime error (message has details) */
+#define PGC_ERR_INTERNAL -6   /* solver invariant broken (message has details) */
+#define PGC_ERR_TIMEOUT -7    /* a bounded device wait ran out */
+
+typedef struct pgc_graph pgc_graph;
+
+/* ProductGraphGenerators(VX, EX, VY, EY, featDiff, conjugate, regulariser[, pruneIntralayer])
+ * product_graph_generators.hpp:65-66, bindings.cpp:33-34.
+ * VX [nvx x 3] f64, EX [nex x 2] i32 (both orientations of every mesh edge),
+ * VY [nvy x 3] f64, EY [ney x 2] i32 (ordered closed curve),
+ * feat_diff [nvx x nvy] f64.  Inputs are copied. */
+int pgc_create(const double* VX, int64_t nvx, const int32_t* EX, int64_t nex, const double* VY, int64_t nvy,
+               const int32_t* EY, int64_t ney, const double* feat_diff, int use_conjugate_graph,
+               int use_regularising_cost_term, int prune_intralayer, pgc_graph** out);
+
+/* ~ProductGraphGenerators (product_graph_generators.hpp:67). */
+void pgc_destroy(pgc_graph* g);
+
+/* setNormals(NX, NY) -- product_graph_generators.cpp:118-130, bindings.cpp:38.
+ * NX [rows_x x cols_x], NY [rows_y x cols_y]; the shapes must be |VX| x 3 and |VY| x 3. */
+int pgc_set_normals(pgc_graph* g, const double* NX, int64_t rows_x, int64_t cols_x, const double* NY,
+                    int64_t rows_y, int64_t cols_y);
+
+/* setMaxDepth(k) -- product_graph_generators.cpp:305-307, bindings.cpp:47. */
+int pgc_set_max_depth(pgc_graph* g, int max_depth);
+
+/* setCostTimeRatioMode(costName, timeName) -- product_graph_generators.cpp:309-312, bindings.cpp:48. */
+int pgc_set_cost_time_ratio_mode(pgc_graph* g, const char* cost_name, const char* time_name);
+
+/* updateRobustLossParams(alpha, c, pwr) -- product_graph_generators.cpp:259-270, bindings.cpp:37.
+ * Ignored for the plain graph and after generate(), as in the reference. */
+int pgc_update_robust_loss_params(pgc_graph* g, double alpha, double c, double pwr);
+
+/* generate() -- product_graph_generators.cpp:21-89, bindings.cpp:35.
+ * Builds the product graph and its edge costs on the device. */
+int pgc_generate(pgc_graph* g);
+
+/* getCostVector() -- product_graph_generators.cpp:138-143, bindings.cpp:36.
+ * Shape query, then copy of the [rows x cols] cost matrix in edge-id order.
+ * A ratio solve rescales these costs in place, as the reference does. */
+int pgc_cost_vector_shape(pgc_graph* g, int64_t* rows, int64_t* cols);
+int pgc_get_cost_vector(pgc_graph* g, double* out);
+
+/* getProductSpace() -- product_graph_generators.cpp:173-178, bindings.cpp:39.
+ * [rows x 4] (plain) or [rows x 6] (conjugate) int32 edge table. */
+int pgc_product_space_shape(pgc_graph* g, int64_t* rows, int64_t* cols);
+int pgc_get_product_space(pgc_graph* g, int32_t* out);
+
+/* solveWithCostTimeRatio(name, k) -- product_graph_generators.cpp:284-303, bindings.cpp:41-42;
+ * CostTimeRatioSolver::run, cost_time_ratio_solver.cpp:868-900.
+ * max_depth < 1 uses the stored depth (the one-argument overload).
+ * The result (passes_layers_just_once, final_objective, matching) is kept in
+ * the handle and read with pgc_result_*. */
+int pgc_solve_with_cost_time_ratio(pgc_graph* g, const char* solver_name, int max_depth);
+
+/* solveWithDijkstra(name, k) -- product_graph_generators.cpp:314-333, bindings.cpp:44-45;
+ * DijkstraSolver::run, dijkstra_solver.cpp:563-579. */
+int pgc_solve_with_minimum_cost(pgc_graph* g, const char* solver_name, int max_depth);
+
+/* The CTR_CYCLE_SOLVER_OUTPUT / DIJKSTRA_SOLVER_OUTPUT tuple
+ * (cost_time_ratio_solver.hpp:70, dijkstra_solver.hpp:22) of the last solve. */
+int pgc_result(pgc_graph* g, int* passes_layers_just_once, float* final_objective, int64_t* rows, int64_t* cols);
+int pgc_result_matching(pgc_graph* g, int32_t* out);
+/* Edge ids (rows of the product space) of the returned cycle, in matching order. */
+int pgc_result_cycle_edges(pgc_graph* g, int64_t* out, int64_t capacity, int64_t* count);
+
+/* Counters of the last solve: [bf_calls, sweeps, candidates, lawler_iterations,
+ * branches, fallback_walks, device_ms_x1000, kernel_launches]. */
+int pgc_result_stats(pgc_graph* g, int64_t* out8);
+
+/* utils::normals2d (helper/utils.cpp:93-157, bindings.cpp:27): outward
+ * vertex normals of an ordered closed curve lying in a coordinate plane.
+ * V [nv x 3], E [ne x 2] with ne == nv; out [nv x 3]. */
+int pgc_compute_normals_2d(const double* V, int64_t nv, const int32_t* E, int64_t ne, double* out);
+
+/* utils::normals3d (helper/utils.cpp:86-90, bindings.cpp:26): area-weighted
+ * vertex normals of a triangle mesh (libigl per_vertex_normals with its
+ * default weighting).  V [nv x 3], F [nf x 3]; out [nv x 3]. */
+int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_t nf, double* out);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* pgc_last_error(void);
+
+/* Library version string. */
+const char* pgc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGC_H */

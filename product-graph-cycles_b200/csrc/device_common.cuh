@@ -1,0 +1,194 @@
+// device_common.cuh -- types shared by the sm_100a kernels and the host driver.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pgc {
+
+constexpr int kWarp = 32;
+constexpr double kInfD = __builtin_huge_val();
+
+// Status words written by the Bellman-Ford kernels.
+enum BfStatus : int {
+    BF_RUNNING = 0,
+    BF_FOUND_CYCLE = 1,      // a cycle was detected and extracted (ratio solver)
+    BF_LAYER_UNREACHED = 2,  // a layer 1..nY-1 received no finite value
+    BF_WRAP_NO_IMPROVE = 3,  // the wrap-around improved no start node
+    BF_MAX_SWEEPS = 4,       // numNodes-1 sweeps without a detected cycle
+    BF_UB_DONE = 5,          // upper-bound sweep finished, path extracted
+    BF_SWEEP_DONE = 6,       // minimum-cost sweep finished
+    BF_ERR_EMPTY_BRANCH = -1,
+    BF_ERR_BARRIER = -2,     // a grid barrier wait ran out of iterations
+    BF_ERR_CYCLE_CAP = -3,   // the extracted cycle does not fit its buffer
+    BF_ERR_WALK = -4,        // a predecessor walk left the valid index range
+};
+
+// Lap-successor codes (see bf kernel): P[v] >= 0 is the next layer-0 node.
+constexpr int kLapEnd = -1;      // the walk stops here (predecessor -1)
+constexpr int kLapUnknown = -2;  // successor not derivable from this sweep
+
+struct Control {
+    int status;
+    int error;
+    int sweeps;          // sweeps run by the last launch
+    int epoch;           // monotone sweep counter (improve flags)
+    int numInBranch;
+    int indexNodeInLayer;
+    int walkId;          // monotone id for visited marks of literal walks
+    int v0;              // first repeated layer-0 node of the detected cycle
+    long long cLength;   // steps the reference's walk needs to detect it
+    int cycleLen;        // entries written to the cycle buffer
+    int candidateVi;     // candidate whose walk found the cycle
+    int fallbackWalks;   // literal walks run because of undecidable shortcuts
+    long long candidates;  // candidates decided (for statistics)
+    unsigned barCount;
+    unsigned barGen;
+    int pad[6];
+    // minimum-cost outputs
+    double firstLb;
+    int firstV;
+    int firstOrigin;
+    double validLb;
+    int validV;
+    int anyFinite;
+};
+
+struct BfParams {
+    // graph
+    int n, nY, K, Kp, nslices;
+    long long numNodes;            // n * nY
+    const int* spInter;
+    const int* spIntra;
+    const int* srcInter;
+    const int* srcDummy;
+    const int* srcIntra;
+    long long interEntries, intraEntries, layerStride;
+    const void* cost;              // (nY+1) * layerStride values (float or double)
+    const void* time;              // same layout, or nullptr for a constant time
+    double tconst;
+    // state
+    double* dp;                    // [2][n][Kp]
+    double* bak;                   // [n]
+    int* pred;                     // [(nY+1)*K*n], expanded index layer*n*K + k*n + v
+    int* org;                      // [2][n][Kp] origin (layer-0 start node) of the stored path
+    int* hops;                     // [2][n][Kp] predecessor steps back to that origin
+    int* lapNext;                  // [n]
+    int* lapSteps;                 // [n]
+    int* mark;                     // [n] visited marks for literal walks
+    int* candStat;                 // [n] shortcut verdict per candidate (0 none, 1 cycle, 2 no cycle, 3 undecided)
+    int* candV0;                   // [n] first repeated layer-0 node of a candidate's walk
+    long long* candSteps;          // [n] predecessor steps that walk needs
+    int* layerFlag;                // [nY+1] epoch of the last sweep that improved the layer
+    const int* branchOf;
+    int branchId;
+    double lambda, ub;
+    int mode;                      // 0 ratio, 1 ratio upper-bound search, 2 minimum cost
+    int maxSweeps;                 // safety cap on sweeps in one launch (0 = unlimited)
+    Control* ctl;
+    int* cycleBuf;                 // original node ids, walk order (reversed on the host)
+    long long cycleCap;
+    // per-CTA reduction slots
+    double* redVal;
+    int* redIdx;
+    int* redAux;
+    long long* redAux64;
+    // minimum-cost lower bounds
+    double* lbOut;                 // [n] lower bound per node (inf if not in the branch)
+    int* originOut;                // [n] origin of the closing path of the node
+};
+
+// ---------------------------------------------------------------------------
+// Kernel argument blocks and launchers (kernels_energy.cu, kernels_bf.cu).
+// ---------------------------------------------------------------------------
+struct EnergyArgs {
+    int n, nY, nvx, nvy;
+    long long interEntries, layerStride, total;  // total = (nY+1) * layerStride
+    const int* tedgeInter;
+    const int* tedgeIntra;
+    const int* eX;       // 3 per template edge
+    const int8_t* eY;    // YPattern per template edge
+    const int* eSrc;
+    const int* eTrgt;
+    const int8_t* eNext;
+    const int* EY;       // nY x 2
+    const double* VX;    // nvx x 3
+    const double* VY;    // nvy x 3
+    const double* FD;    // nvx x nvy
+    const double4* quat; // nY * n (w, x, y, z) or nullptr
+    // plain graph
+    int lengthMode;      // ("feature", "lengthnormalisation"): columns [fd, length]
+    int lineIntegral;
+    // conjugate graph
+    int costMode, timeMode;
+    double rlAlpha, rlC, rlPwr;
+    double maxSO3, maxFd;  // already rounded through float as in the reference
+    double* out0;
+    double* out1;        // nullptr for one column
+};
+
+struct QuatArgs {
+    int nEX, nY, n, prune;
+    const int* EX;
+    const int* EY;
+    const double* VX;
+    const double* VY;
+    const double* NX;
+    const double* NY;
+    double4* out;
+};
+
+struct SelectArgs {
+    const double* col;
+    long long total, layerStride, interEntries;
+    int nY;
+    const int* tedgeInter;
+    const int* tedgeIntra;
+    unsigned long long prefix, prefixMask;
+    int shift, bits;
+    unsigned long long* hist;  // 1 << bits counters
+};
+
+struct LookupArgs {
+    int n, nY;
+    long long numNodes, eBlock;
+    const int* spInter;
+    const int* spIntra;
+    const int* srcInter;
+    const int* srcDummy;
+    const int* srcIntra;
+    const int* tedgeInter;
+    const int* tedgeIntra;
+    long long interEntries, layerStride;
+    const double* c64;
+    const double* t64;   // nullptr: constant time
+    double tconst;
+    const int* pairSrc;
+    const int* pairTrgt;
+    int count;
+    long long* edgeOut;
+    double* cOut;
+    double* tOut;
+};
+
+cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
+                      cudaStream_t stream);
+cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, int* blocksPerSm);
+cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream);
+cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
+cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);
+cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);
+cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s);
+cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s);
+cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
+                           int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
+                           cudaStream_t s);
+cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,
+                          long long interEntries, int nY, const int* ti, const int* tr, int* exact, cudaStream_t s);
+cudaError_t launch_export(const double* col, double* out, int cols, int c, long long total, long long layerStride,
+                          long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
+                          cudaStream_t s);
+cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
+                               const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
+                               int* countOut, cudaStream_t s);
+
+}  // namespace pgc

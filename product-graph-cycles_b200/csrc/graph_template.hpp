@@ -1,0 +1,70 @@
+// graph_template.hpp -- the layer-invariant structure of a cyclic product graph.
+//
+// Every layer of the reference's product graph has the same topology (only
+// the Y indices of its rows change), so the device keeps ONE in-edge list per
+// node-within-a-layer and streams per-layer edge costs beside it.
+//
+// Layout ("sliced ELL", 32 nodes per slice = one warp): for each part
+// (INTER = in-edges from the previous layer, INTRA = in-edges from the same
+// layer) and each slice s of 32 consecutive target nodes there are
+// width(s) slots; slot j of slice s holds, for lane i, the j-th in-edge of
+// target node 32*s + i in ascending edge-id order, or -1 past the node's
+// in-degree.  Slot j of slice s lives at entries [32*(sp[s]+j), 32*(sp[s]+j)+32).
+//
+// Edge ids follow the reference's generation order: block b (= the Y edge b)
+// holds eBlock consecutive ids; the edge with template offset t in block b
+// has id b*eBlock + t.  An INTER slot of layer l holds an edge of block l-1
+// (block nY-1 for the closing "dummy" layer l = nY); an INTRA slot of layer l
+// holds an edge of block l.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace pgc {
+
+enum Part { INTER = 0, INTRA = 1 };
+
+// How the Y columns of a productspace row are formed from block b:
+//   s2 = EY(b,0), m2 = EY(b,1), t2 = EY((b+1) % nY, 1)
+enum YPattern : int8_t {
+    Y_SS = 0,   // plain intralayer       [s2, s2]
+    Y_SM = 1,   // plain interlayer       [s2, m2]
+    Y_SSS = 2,  // conj deg2d -> deg2d    [s2, s2, s2]
+    Y_SSM = 3,  // conj deg2d -> non-deg  [s2, s2, m2]
+    Y_SMT = 4,  // conj interlayer        [s2, m2, t2]
+    Y_SMM = 5,  // conj non-deg -> deg2d  [s2, m2, m2]
+};
+
+struct LayerTemplate {
+    bool conj = false, prune = false;
+    int n = 0;          // nodes per layer
+    int nvx = 0;        // max(EX) + 1
+    int nY = 0;         // number of layers (|EY|)
+    int nslices = 0;
+    int64_t eBlock = 0; // edges per block
+    // sliced-ELL in-edge lists, per part
+    std::vector<int> sp[2];        // nslices + 1 slot offsets
+    std::vector<int> src[2];       // 32 * slots: local source node or -1
+    std::vector<int> tedge[2];     // 32 * slots: template edge offset or -1
+    std::vector<int> srcDummy;     // INTER src list used by the closing layer
+    int64_t entries[2] = {0, 0};   // 32 * slots per part
+    // per template edge offset (eBlock entries)
+    std::vector<int> eSrc, eTrgt;  // local source / target node
+    std::vector<int8_t> eNext;     // 1 if the target is in the next layer
+    std::vector<int> eX;           // 3 ints per edge: x columns of the row (x2 unused for plain)
+    std::vector<int8_t> eY;        // YPattern
+    std::vector<int> ePos;         // entry index (part encoded in bit 30) of the edge in its part
+
+    int64_t layerStride() const { return entries[0] + entries[1]; }
+    int cols() const { return conj ? 6 : 4; }
+};
+
+// Builds the template; returns an empty string or an error message.
+std::string build_template(const int* EX, int64_t nEX, const int* EY, int64_t nEY, int64_t nVX, bool conj,
+                           bool prune, LayerTemplate& T);
+
+// productspace row of global edge id e (product_space.cpp / conj_product_space.cpp order).
+void product_row(const LayerTemplate& T, const int* EY, int64_t e, int* out);
+
+}  // namespace pgc

@@ -1,0 +1,435 @@
+// kernels_energy.cu -- edge costs of the product graph, computed on the device
+// straight into the per-layer streams that the relaxation reads.
+//
+// Stream layout: layer l (0..nY) owns layerStride = entries[INTER] +
+// entries[INTRA] consecutive values; entry j < entries[INTER] is INTER slot
+// entry j (an edge of block l-1), the rest are INTRA entries (edges of block
+// l).  Entries that hold no edge are NaN.
+//
+// Cost formulas restate deformationEnergy.cpp:11-78 (plain graph) and
+// higherOrderDeformationEnergy.cpp:209-339 (conjugate graph).  The whole file
+// is compiled with --fmad=false so no product is fused into a sum; pure
+// arithmetic modes are therefore bit-identical to the CPU formulas.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_common.cuh"
+
+namespace pgc {
+
+
+enum HoMode { NOMODE = 0, VANILLA, FEATURE, LENGTH, SO3_PLAIN, SO3_ROBUST, PENALISE_DEGENERATE };
+
+__device__ __forceinline__ bool entry_edge(const EnergyArgs& a, long long idx, int& block, int& tedge) {
+    const long long l = idx / a.layerStride;
+    const long long pos = idx - l * a.layerStride;
+    if (pos < a.interEntries) {
+        if (l < 1) return false;
+        tedge = a.tedgeInter[pos];
+        block = (int)(l - 1);
+    } else {
+        if (l >= a.nY) return false;
+        tedge = a.tedgeIntra[pos - a.interEntries];
+        block = (int)l;
+    }
+    return tedge >= 0;
+}
+
+__device__ __forceinline__ double line_integral(const EnergyArgs& a, int y0, int y1, int x0, int x1) {
+    double li = 0.0;
+    for (int j = 0; j < 3; ++j) {
+        const double dy = a.VY[3 * y0 + j] - a.VY[3 * y1 + j];
+        li = li + dy * dy;
+        const double dx = a.VX[3 * x0 + j] - a.VX[3 * x1 + j];
+        li = li + dx * dx;
+    }
+    return sqrt(li);
+}
+
+__global__ void plain_energy_kernel(EnergyArgs a) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int b, t;
+        if (!entry_edge(a, idx, b, t)) {
+            a.out0[idx] = nan;
+            if (a.out1) a.out1[idx] = nan;
+            continue;
+        }
+        const int y0 = a.EY[2 * b];
+        const int y1 = a.eY[t] == 0 ? y0 : a.EY[2 * b + 1];
+        const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1];
+        const double li = a.lineIntegral ? line_integral(a, y0, y1, x0, x1) : 1.0;
+        const double fd = a.FD[(long long)x0 * a.nvy + y0] + a.FD[(long long)x1 * a.nvy + y1];
+        if (a.lengthMode) {
+            a.out0[idx] = fd;
+            a.out1[idx] = li;
+        } else {
+            a.out0[idx] = 0.5 * fd * li;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// SO(3) frame alignment (higherOrderDeformationEnergy.cpp:16-53, :95-134).
+// The reference takes R = U diag(1,1,det(UV^T)) V^T from the SVD of X^T Y.
+// The same rotation is the maximiser of tr(R^T M), M = X^T Y, which Horn's
+// closed-form method (J. Opt. Soc. Am. A 4(4), 1987) gives directly as the
+// eigenvector of the largest eigenvalue of a symmetric 4x4 matrix built from
+// S = M^T; the eigenvector is found with cyclic Jacobi rotations.
+// ---------------------------------------------------------------------------
+__device__ void normalize3(double v[3]) {
+    const double sq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (sq > 0.0) {
+        const double r = sqrt(sq);
+        v[0] /= r; v[1] /= r; v[2] /= r;
+    }
+}
+
+__device__ double4 frame_quaternion(const double v2[3], const double n2[3], const double v3[3],
+                                    const double n3[3]) {
+    double X[3][3], Y[3][3];
+    // rows [n, e, e x n], each normalised
+    double c2[3] = {v2[1] * n2[2] - v2[2] * n2[1], v2[2] * n2[0] - v2[0] * n2[2], v2[0] * n2[1] - v2[1] * n2[0]};
+    double c3[3] = {v3[1] * n3[2] - v3[2] * n3[1], v3[2] * n3[0] - v3[0] * n3[2], v3[0] * n3[1] - v3[1] * n3[0]};
+    for (int k = 0; k < 3; ++k) {
+        X[0][k] = n2[k]; X[1][k] = v2[k]; X[2][k] = c2[k];
+        Y[0][k] = n3[k]; Y[1][k] = v3[k]; Y[2][k] = c3[k];
+    }
+    for (int r = 0; r < 3; ++r) { normalize3(X[r]); normalize3(Y[r]); }
+    double S[3][3];  // S = M^T with M = X^T Y, i.e. S[a][b] = sum_r Y[r][a] X[r][b]
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) S[i][j] = Y[0][i] * X[0][j] + Y[1][i] * X[1][j] + Y[2][i] * X[2][j];
+    const double Sxx = S[0][0], Sxy = S[0][1], Sxz = S[0][2];
+    const double Syx = S[1][0], Syy = S[1][1], Syz = S[1][2];
+    const double Szx = S[2][0], Szy = S[2][1], Szz = S[2][2];
+    double A[4][4] = {{Sxx + Syy + Szz, Syz - Szy, Szx - Sxz, Sxy - Syx},
+                      {Syz - Szy, Sxx - Syy - Szz, Sxy + Syx, Szx + Sxz},
+                      {Szx - Sxz, Sxy + Syx, -Sxx + Syy - Szz, Syz + Szy},
+                      {Sxy - Syx, Szx + Sxz, Syz + Szy, -Sxx - Syy + Szz}};
+    double V[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < 4; ++i) {
+            diag += A[i][i] * A[i][i];
+            for (int j = i + 1; j < 4; ++j) off += A[i][j] * A[i][j];
+        }
+        if (off <= 1e-32 * (diag + 1e-300)) break;
+        for (int pp = 0; pp < 3; ++pp)
+            for (int q = pp + 1; q < 4; ++q) {
+                const double apq = A[pp][q];
+                if (fabs(apq) < 1e-300) continue;
+                const double theta = (A[q][q] - A[pp][pp]) / (2.0 * apq);
+                const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(tt * tt + 1.0), s = tt * c;
+                for (int k = 0; k < 4; ++k) {
+                    const double akp = A[k][pp], akq = A[k][q];
+                    A[k][pp] = c * akp - s * akq;
+                    A[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 4; ++k) {
+                    const double apk = A[pp][k], aqk = A[q][k];
+                    A[pp][k] = c * apk - s * aqk;
+                    A[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 4; ++k) {
+                    const double vkp = V[k][pp], vkq = V[k][q];
+                    V[k][pp] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    int best = 0;
+    for (int i = 1; i < 4; ++i)
+        if (A[i][i] > A[best][best]) best = i;
+    double q[4] = {V[0][best], V[1][best], V[2][best], V[3][best]};
+    const double nq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    return make_double4(q[0] / nq, q[1] / nq, q[2] / nq, q[3] / nq);
+}
+
+
+__global__ void quaternion_kernel(QuatArgs a) {
+    const long long total = (long long)a.nY * a.n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / a.n), j = (int)(idx % a.n);
+        const int e3 = j - (j / a.nEX) * a.nEX;
+        int i2 = i;
+        if (j >= a.nEX && j < 2 * a.nEX && !a.prune) i2 = (i + a.nY - 1) % a.nY;  // degenerate-2d node
+        double v2[3], n2[3], v3[3], n3[3];
+        const int ya = a.EY[2 * i2], yb = a.EY[2 * i2 + 1];
+        const int xa = a.EX[2 * e3], xb = a.EX[2 * e3 + 1];
+        for (int k = 0; k < 3; ++k) {
+            v2[k] = a.VY[3 * yb + k] - a.VY[3 * ya + k];
+            n2[k] = a.NY[3 * ya + k];
+            v3[k] = a.VX[3 * xb + k] - a.VX[3 * xa + k];
+            n3[k] = (a.NX[3 * xa + k] + a.NX[3 * xb + k]) / 2;
+        }
+        a.out[idx] = frame_quaternion(v2, n2, v3, n3);
+    }
+}
+
+__device__ __forceinline__ double so3_distance(const double4 a, const double4 b) {
+    double ip = fabs(a.x * b.x + (a.y * b.y + a.z * b.z + a.w * b.w));
+    if (ip > 1) ip = 1;
+    if (isnan(ip)) return 0;
+    return 2 * acos(ip);
+}
+
+__device__ __forceinline__ double robust_loss(const EnergyArgs& a, double x) {
+    const double t = pow(x / a.rlC, a.rlPwr);
+    const double am2 = fabs(a.rlAlpha - 2);
+    return am2 / a.rlAlpha * (pow(t / am2 + 1, 0.5 * a.rlAlpha) - 1);
+}
+
+__global__ void ho_energy_kernel(EnergyArgs a) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    const double twoPi = 2 * 3.14159265358979323846;
+    const bool needLi = (a.costMode == LENGTH || a.timeMode == LENGTH);
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int b, t;
+        if (!entry_edge(a, idx, b, t)) {
+            a.out0[idx] = nan;
+            if (a.out1) a.out1[idx] = nan;
+            continue;
+        }
+        const int s2 = a.EY[2 * b], m2 = a.EY[2 * b + 1], t2 = a.EY[2 * ((b + 1) % a.nY) + 1];
+        int y0, y1, y2;
+        switch (a.eY[t]) {
+            case 2: y0 = s2; y1 = s2; y2 = s2; break;
+            case 3: y0 = s2; y1 = s2; y2 = m2; break;
+            case 4: y0 = s2; y1 = m2; y2 = t2; break;
+            default: y0 = s2; y1 = m2; y2 = m2; break;
+        }
+        const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1], x2 = a.eX[3 * t + 2];
+        double so3 = 0.0;
+        if (a.quat) {
+            const long long q0 = (long long)b * a.n + a.eSrc[t];
+            const long long q1 = (long long)((b + a.eNext[t]) % a.nY) * a.n + a.eTrgt[t];
+            so3 = so3_distance(a.quat[q0], a.quat[q1]);
+        }
+        const double fd = a.FD[(long long)x2 * a.nvy + y2];
+        const double li = needLi ? line_integral(a, y0, y1, x0, x1) : 0.0;
+        const bool degenerate = (y2 == y1 || x2 == x1);
+        const int cm = a.costMode, tm = a.timeMode;
+        double c0 = 0, c1 = 0;
+        if (cm == VANILLA && tm == VANILLA) {
+            c0 = robust_loss(a, so3) + fd;
+        } else if (cm == VANILLA && tm == LENGTH) {
+            c0 = robust_loss(a, so3) + fd;
+            c1 = li;
+        } else if (cm == LENGTH && tm == VANILLA) {
+            c0 = li;
+        } else if (cm == VANILLA && tm == PENALISE_DEGENERATE) {
+            c0 = robust_loss(a, so3) + fd;
+            c1 = degenerate ? 0.1 : 1;
+        } else if (cm == PENALISE_DEGENERATE && tm == VANILLA) {
+            c0 = degenerate ? 0.1 : 1;
+        } else if (cm == FEATURE && tm == SO3_PLAIN) {
+            c0 = fd;
+            c1 = fmax(0.0, twoPi - so3);
+        } else if (cm == FEATURE && tm == SO3_ROBUST) {
+            c0 = fd;
+            c1 = fmax(0.0, a.maxSO3 - robust_loss(a, so3));
+        } else if (cm == SO3_ROBUST && tm == FEATURE) {
+            c0 = robust_loss(a, so3);
+            c1 = fmax(0.0, a.maxFd - fd);
+        } else {  // SO3_PLAIN, FEATURE
+            c0 = so3;
+            c1 = fmax(0.0, a.maxFd - fd);
+        }
+        a.out0[idx] = c0;
+        if (a.out1) a.out1[idx] = c1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Median by radix selection over the valid entries of one column.  Keys are
+// the order-preserving 64-bit images of the doubles; 11-bit digits, six
+// passes from the most significant digit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long order_key(double x) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+}
+
+
+__device__ __forceinline__ bool entry_valid(const SelectArgs& a, long long idx) {
+    const long long l = idx / a.layerStride;
+    const long long pos = idx - l * a.layerStride;
+    if (pos < a.interEntries) return l >= 1 && a.tedgeInter[pos] >= 0;
+    return l < a.nY && a.tedgeIntra[pos - a.interEntries] >= 0;
+}
+
+__global__ void select_hist_kernel(SelectArgs a) {
+    extern __shared__ unsigned int sh[];
+    const int nb = 1 << a.bits;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        if (!entry_valid(a, idx)) continue;
+        const unsigned long long k = order_key(a.col[idx]);
+        if ((k & a.prefixMask) != a.prefix) continue;
+        atomicAdd(&sh[(k >> a.shift) & (unsigned long long)(nb - 1)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+        if (sh[i]) atomicAdd(a.hist + i, (unsigned long long)sh[i]);
+}
+
+// x <- min(round(factor * x), clip), in place on the valid entries; also
+// writes the float copy and clears *exact when a value is not a float.
+__global__ void rescale_kernel(double* col, float* col32, long long total, long long layerStride,
+                               long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
+                               double factor, double clip, int* exact) {
+    SelectArgs a{};
+    a.layerStride = layerStride;
+    a.interEntries = interEntries;
+    a.nY = nY;
+    a.tedgeInter = tedgeInter;
+    a.tedgeIntra = tedgeIntra;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        if (!entry_valid(a, idx)) {
+            if (col32) col32[idx] = __int_as_float(0x7fc00000);
+            continue;
+        }
+        double x = round(factor * col[idx]);
+        if (x > clip) x = clip;
+        col[idx] = x;
+        const float f = (float)x;
+        if (col32) col32[idx] = f;
+        if ((double)f != x) *exact = 0;
+    }
+}
+
+__global__ void to_f32_kernel(const double* col, float* col32, long long total, long long layerStride,
+                              long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
+                              int* exact) {
+    SelectArgs a{};
+    a.layerStride = layerStride;
+    a.interEntries = interEntries;
+    a.nY = nY;
+    a.tedgeInter = tedgeInter;
+    a.tedgeIntra = tedgeIntra;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        if (!entry_valid(a, idx)) {
+            col32[idx] = __int_as_float(0x7fc00000);
+            continue;
+        }
+        const double x = col[idx];
+        const float f = (float)x;
+        col32[idx] = f;
+        if ((double)f != x) *exact = 0;
+    }
+}
+
+// Scatter a stream column to edge-id order: out[e * cols + c].
+__global__ void export_kernel(const double* col, double* out, int cols, int c, long long total,
+                              long long layerStride, long long interEntries, int nY, long long eBlock,
+                              const int* tedgeInter, const int* tedgeIntra) {
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long l = idx / layerStride;
+        const long long pos = idx - l * layerStride;
+        long long block;
+        int t;
+        if (pos < interEntries) {
+            if (l < 1) continue;
+            t = tedgeInter[pos];
+            block = l - 1;
+        } else {
+            if (l >= nY) continue;
+            t = tedgeIntra[pos - interEntries];
+            block = l;
+        }
+        if (t < 0) continue;
+        out[(block * eBlock + t) * cols + c] = col[idx];
+    }
+}
+
+// Mean incoming cost of every node of layer 1, accumulated in float in
+// in-edge order (cost_time_ratio_solver.cpp:656-675).
+__global__ void layer1_mean_kernel(const double* cost, long long layerStride, long long interEntries, int n,
+                                   int nslices, const int* spInter, const int* spIntra, const int* srcInter,
+                                   const int* srcIntra, float* meanOut, int* countOut) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const int s = v >> 5, lane = v & 31;
+    const double* c1 = cost + layerStride;  // layer 1
+    float mean = 0;
+    int num = 0;
+    for (int j = spInter[s]; j < spInter[s + 1]; ++j) {
+        const long long e = (long long)j * 32 + lane;
+        if (srcInter[e] < 0) continue;
+        mean = (float)((double)mean + c1[e]);
+        ++num;
+    }
+    for (int j = spIntra[s]; j < spIntra[s + 1]; ++j) {
+        const long long e = (long long)j * 32 + lane;
+        if (srcIntra[e] < 0) continue;
+        mean = (float)((double)mean + c1[interEntries + e]);
+        ++num;
+    }
+    meanOut[v] = mean / (float)num;
+    countOut[v] = num;
+    (void)nslices;
+}
+
+// Host wrappers -------------------------------------------------------------
+static int grid_for(long long total, int threads) {
+    long long b = (total + threads - 1) / threads;
+    if (b > 148LL * 32) b = 148LL * 32;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s) {
+    plain_energy_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
+    ho_energy_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
+    quaternion_kernel<<<grid_for((long long)a.nY * a.n, 128), 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
+    select_hist_kernel<<<grid_for(a.total, 512), 512, (1 << a.bits) * sizeof(unsigned), s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
+                           int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
+                           cudaStream_t s) {
+    rescale_kernel<<<grid_for(total, 256), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
+                                                        factor, clip, exact);
+    return cudaGetLastError();
+}
+cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,
+                          long long interEntries, int nY, const int* ti, const int* tr, int* exact, cudaStream_t s) {
+    to_f32_kernel<<<grid_for(total, 256), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
+                                                       exact);
+    return cudaGetLastError();
+}
+cudaError_t launch_export(const double* col, double* out, int cols, int c, long long total, long long layerStride,
+                          long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
+                          cudaStream_t s) {
+    export_kernel<<<grid_for(total, 256), 256, 0, s>>>(col, out, cols, c, total, layerStride, interEntries, nY,
+                                                       eBlock, ti, tr);
+    return cudaGetLastError();
+}
+cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
+                               const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
+                               int* countOut, cudaStream_t s) {
+    layer1_mean_kernel<<<(n + 255) / 256, 256, 0, s>>>(cost, layerStride, interEntries, n, nslices, spI, spA, srcI,
+                                                       srcA, meanOut, countOut);
+    return cudaGetLastError();
+}
+
+}  // namespace pgc

@@ -1,0 +1,1499 @@
+// pgc_host.cpp -- host side of libpgc: the generator facade, the solver
+// control loops and the C ABI declared in include/pgc.h.
+//
+// Division of labour: the device builds the edge costs, rescales them and
+// runs every Bellman-Ford call (one launch per call, see kernels_bf.cu);
+// the host keeps only the scalar control of the reference's solvers -- the
+// Lawler ratio updates, the branch-and-bound heap and the branching rules --
+// which touch O(cycle length) or O(nodes per layer) data.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pgc.h"
+#include "branch_heap.hpp"
+#include "device_common.cuh"
+#include "graph_template.hpp"
+
+namespace pgc {
+
+namespace {
+
+thread_local std::string g_lastError;
+
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define PGC_CUDA(call)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            throw Failure(PGC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) count = 1;
+        PGC_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const T* src, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count && src) PGC_CUDA(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void zero(cudaStream_t s) { PGC_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+};
+
+enum HoMode { NOMODE = 0, VANILLA, FEATURE, LENGTH, SO3_PLAIN, SO3_ROBUST, PENALISE_DEGENERATE };
+
+// higherOrderDeformationEnergy.cpp:396-412 including its missing "== 0" on
+// the last comparison: "penalisedegenerate" maps to VANILLA and any other
+// unknown name (the default "") to PENALISE_DEGENERATE.
+int string_to_mode(const std::string& s) {
+    if (s == "nomode") return NOMODE;
+    if (s == "vanilla") return VANILLA;
+    if (s == "feature") return FEATURE;
+    if (s == "lengthnormalisation") return LENGTH;
+    if (s == "plainso3") return SO3_PLAIN;
+    if (s == "robustso3") return SO3_ROBUST;
+    if (s != "penalisedegenerate") return PENALISE_DEGENERATE;
+    return VANILLA;
+}
+
+bool ho_supported(int cm, int tm) {
+    return (cm == VANILLA && tm == VANILLA) || (cm == VANILLA && tm == LENGTH) || (cm == LENGTH && tm == VANILLA) ||
+           (cm == VANILLA && tm == PENALISE_DEGENERATE) || (cm == PENALISE_DEGENERATE && tm == VANILLA) ||
+           (cm == FEATURE && tm == SO3_PLAIN) || (cm == FEATURE && tm == SO3_ROBUST) ||
+           (cm == SO3_ROBUST && tm == FEATURE) || (cm == SO3_PLAIN && tm == FEATURE);
+}
+
+double robust_loss_host(double x, double alpha, double c, double pwr) {
+    const double t = std::pow(x / c, pwr);
+    const double am2 = std::fabs(alpha - 2);
+    return am2 / alpha * (std::pow(t / am2 + 1, 0.5 * alpha) - 1);
+}
+
+// (int)std::round(x) as the reference's x86-64 build evaluates it.
+int round_to_int(double x) {
+    const double r = std::round(x);
+    if (!(r >= -2147483648.0 && r <= 2147483647.0)) return INT_MIN;
+    return (int)r;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    return std::atoi(v);
+}
+
+}  // namespace
+
+// A closed walk of the product graph as the reference stores it: original
+// node ids (targets in layer 0 that close a lap are written as the closing
+// copy numNodes + v only at the end), plus the edge and its cost/time for
+// every consecutive pair.
+struct CycleRec {
+    std::vector<int> nodes;
+    std::vector<long long> edges;
+    std::vector<double> c, t;
+    bool valid() const { return !nodes.empty(); }
+};
+
+enum class BfOutcome { NO_NEGATIVE_CYCLE, FOUND_NEGATIVE_CYCLE, ZERO_CYCLE };
+
+struct Stats {
+    long long bfCalls = 0, sweeps = 0, candidates = 0, lawlerIters = 0, branches = 0, fallbackWalks = 0;
+    double deviceMs = 0;
+    long long launches = 0;
+};
+
+class Graph {
+  public:
+    // inputs
+    std::vector<double> VX, VY, FD, NX, NY;
+    std::vector<int> EX, EY;
+    int64_t nvx = 0, nvy = 0, nex = 0, ney = 0;
+    bool conj = false, reg = false, prune = false, normalsGiven = false;
+    double rlAlpha = 0.7, rlC = 0.6, rlPwr = 4;
+    int maxDepth = 4;
+    std::string costName = "vanilla", timeName = "";
+
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    // generated state
+    bool generated = false;
+    LayerTemplate T;
+    int ncols = 1;
+    DBuf<int> dSp[2], dSrc[2], dTedge[2], dSrcDummy, dEX, dEY, dESrc, dETrgt, dEXcols;
+    DBuf<int8_t> dEYpat, dENext;
+    DBuf<double> dVX, dVY, dFD, dNX, dNY;
+    DBuf<double4> dQuat;
+    DBuf<double> e64[2];
+    DBuf<float> e32[2];
+    bool f32Valid[2] = {false, false};  // e32 mirrors e64 exactly
+    bool f32Known[2] = {false, false};  // e32 state computed since the last energy change
+
+    // solver workspace
+    DBuf<double> wDp, wBak, wRedVal, wLb, wCOut, wTOut;
+    DBuf<int> wPred, wOrg, wHops, wLapNext, wLapSteps, wMark, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
+        wRedIdx, wRedAux, wOrigin, wPairS, wPairT, wCount;
+    DBuf<long long> wCandSteps, wRedAux64, wEdgeOut;
+    DBuf<float> wMean;
+    DBuf<Control> wCtl;
+    int wsK = -1;
+    int ctlEpoch = 0, ctlWalkId = 0;
+    bool workspaceFresh = false;
+
+    // last result
+    bool resPasses = false;
+    float resObjective = 0;
+    int64_t resRows = 0, resCols = 0;
+    std::vector<int> resMatching;
+    std::vector<long long> resEdges;
+    Stats stats;
+
+    ~Graph() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    long numNodes() const { return (long)T.n * T.nY; }
+
+    // -------------------------------------------------------------------
+    void generate();
+    void ensure_generated() {
+        if (!generated) generate();
+    }
+    void energy_changed() {
+        f32Known[0] = f32Known[1] = false;
+    }
+
+    // -------------------------------------------------------------------
+    void solve_ratio(int K);
+    void solve_min_cost(int K);
+    void export_csv();
+
+    // cost export / product space
+    void cost_vector(double* out);
+    void product_space(int32_t* out);
+
+  private:
+    // solver helpers
+    struct Run {
+        int K, Kp;
+        int costF32, timeKind;
+        const void* cost;
+        const void* time;
+        double tconst;
+        int blocks, threads;
+        bool coop;
+    };
+    Run prepare_run(int K, bool ratio);
+    void ensure_workspace(int K, int blocks);
+    void upload_branch(const std::vector<int>& branchOf);
+    // Every solve starts from an unwritten predecessor table (-1), like the
+    // reference's freshly allocated solver state.
+    void reset_predecessors() {
+        PGC_CUDA(cudaMemsetAsync(wPred.p, 0xff, wPred.n * sizeof(int), stream));
+    }
+    BfParams params(const Run& r, int mode, int branchId, double lambda, double ub);
+    Control launch_bf_call(const Run& r, const BfParams& p);
+    std::vector<int> read_cycle_buffer(int len);
+    void lookup_pairs(const std::vector<int>& src, const std::vector<int>& trgt, std::vector<long long>& edges,
+                      std::vector<double>& c, std::vector<double>& t, double tconst);
+    double median_of_column(int col);
+    void rescale_column(int col, double scaling);
+    void ensure_f32(int col);
+    void rows_for_edges(const std::vector<long long>& edges);
+};
+
+// ---------------------------------------------------------------------------
+// generate(): product_graph_generators.cpp:21-89
+// ---------------------------------------------------------------------------
+void Graph::generate() {
+    if (conj && !normalsGiven)
+        throw Failure(PGC_ERR_STATE, "cannot generate the conjugate product graph without normals (set_normals)");
+    const std::string err = build_template(EX.data(), nex, EY.data(), ney, nvx, conj, prune, T);
+    if (!err.empty()) throw Failure(PGC_ERR_ARG, err);
+    for (int64_t i = 0; i < 2 * ney; ++i)
+        if (EY[(size_t)i] >= nvy) throw Failure(PGC_ERR_ARG, "EY refers to a vertex outside VY");
+
+    cudaStream_t s = stream;
+    for (int p = 0; p < 2; ++p) {
+        dSp[p].upload(T.sp[p].data(), T.sp[p].size(), s);
+        dSrc[p].upload(T.src[p].data(), T.src[p].size(), s);
+        dTedge[p].upload(T.tedge[p].data(), T.tedge[p].size(), s);
+    }
+    dSrcDummy.upload(T.srcDummy.data(), T.srcDummy.size(), s);
+    dESrc.upload(T.eSrc.data(), T.eSrc.size(), s);
+    dETrgt.upload(T.eTrgt.data(), T.eTrgt.size(), s);
+    dENext.upload(T.eNext.data(), T.eNext.size(), s);
+    dEXcols.upload(T.eX.data(), T.eX.size(), s);
+    dEYpat.upload(T.eY.data(), T.eY.size(), s);
+    dEY.upload(EY.data(), EY.size(), s);
+    dEX.upload(EX.data(), EX.size(), s);
+    dVX.upload(VX.data(), VX.size(), s);
+    dVY.upload(VY.data(), VY.size(), s);
+    dFD.upload(FD.data(), FD.size(), s);
+
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    EnergyArgs a{};
+    a.n = T.n;
+    a.nY = T.nY;
+    a.nvx = (int)nvx;
+    a.nvy = (int)nvy;
+    a.interEntries = T.entries[INTER];
+    a.layerStride = stride;
+    a.total = total;
+    a.tedgeInter = dTedge[INTER].p;
+    a.tedgeIntra = dTedge[INTRA].p;
+    a.eX = dEXcols.p;
+    a.eY = dEYpat.p;
+    a.eSrc = dESrc.p;
+    a.eTrgt = dETrgt.p;
+    a.eNext = dENext.p;
+    a.EY = dEY.p;
+    a.VX = dVX.p;
+    a.VY = dVY.p;
+    a.FD = dFD.p;
+    if (!conj) {
+        // deformationEnergy.cpp:97-103: two columns only for ("feature", "lengthnormalisation")
+        const bool lengthMode = costName == "feature" && timeName == "lengthnormalisation";
+        ncols = lengthMode ? 2 : 1;
+        a.lengthMode = lengthMode;
+        a.lineIntegral = reg || lengthMode;
+        e64[0].alloc((size_t)total);
+        a.out0 = e64[0].p;
+        if (ncols > 1) {
+            e64[1].alloc((size_t)total);
+            a.out1 = e64[1].p;
+        }
+        PGC_CUDA(launch_plain_energy(a, s));
+    } else {
+        const int cm = string_to_mode(costName), tm = string_to_mode(timeName);
+        if (!ho_supported(cm, tm))
+            throw Failure(PGC_ERR_MODE, "cost time mode not supported: (" + costName + ", " + timeName + ")");
+        ncols = (tm == NOMODE || tm == VANILLA) ? 1 : 2;
+        a.costMode = cm;
+        a.timeMode = tm;
+        a.rlAlpha = rlAlpha;
+        a.rlC = rlC;
+        a.rlPwr = rlPwr;
+        a.maxSO3 = (double)(float)robust_loss_host(2 * M_PI, rlAlpha, rlC, rlPwr);
+        if (tm == FEATURE) {
+            double m = -std::numeric_limits<double>::infinity();
+            for (double x : FD) m = std::max(m, x);
+            a.maxFd = (double)(float)m;
+        }
+        if (reg) {
+            dNX.upload(NX.data(), NX.size(), s);
+            dNY.upload(NY.data(), NY.size(), s);
+            dQuat.alloc((size_t)T.nY * (size_t)T.n);
+            QuatArgs q{};
+            q.nEX = (int)nex;
+            q.nY = T.nY;
+            q.n = T.n;
+            q.prune = prune ? 1 : 0;
+            q.EX = dEX.p;
+            q.EY = dEY.p;
+            q.VX = dVX.p;
+            q.VY = dVY.p;
+            q.NX = dNX.p;
+            q.NY = dNY.p;
+            q.out = dQuat.p;
+            PGC_CUDA(launch_quaternions(q, s));
+            a.quat = dQuat.p;
+        }
+        e64[0].alloc((size_t)total);
+        a.out0 = e64[0].p;
+        if (ncols > 1) {
+            e64[1].alloc((size_t)total);
+            a.out1 = e64[1].p;
+        }
+        PGC_CUDA(launch_ho_energy(a, s));
+        dQuat.release();
+    }
+    PGC_CUDA(cudaStreamSynchronize(s));
+    energy_changed();
+    generated = true;
+}
+
+// ---------------------------------------------------------------------------
+// Rescaling: cost_time_ratio_solver.cpp:709-721 with utils::median
+// (utils.hpp:196-209).  The k-th value is found by radix selection.
+// ---------------------------------------------------------------------------
+double Graph::median_of_column(int col) {
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    const long long count = (long long)T.nY * T.eBlock;
+    if (count <= 0) throw Failure(PGC_ERR_STATE, "empty product graph");
+    const int bits = 11;
+    DBuf<unsigned long long> hist;
+    hist.alloc((size_t)1 << bits);
+    std::vector<unsigned long long> h((size_t)1 << bits);
+    auto select = [&](long long k) -> double {
+        unsigned long long prefix = 0, mask = 0;
+        int shift = 64;
+        long long rank = k;
+        while (shift > 0) {
+            const int b = std::min(bits, shift);
+            shift -= b;
+            SelectArgs a{};
+            a.col = e64[col].p;
+            a.total = total;
+            a.layerStride = stride;
+            a.interEntries = T.entries[INTER];
+            a.nY = T.nY;
+            a.tedgeInter = dTedge[INTER].p;
+            a.tedgeIntra = dTedge[INTRA].p;
+            a.prefix = prefix;
+            a.prefixMask = mask;
+            a.shift = shift;
+            a.bits = b;
+            a.hist = hist.p;
+            PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
+            PGC_CUDA(launch_select_hist(a, stream));
+            stats.launches++;
+            PGC_CUDA(cudaMemcpyAsync(h.data(), hist.p, sizeof(unsigned long long) << b, cudaMemcpyDeviceToHost,
+                                     stream));
+            PGC_CUDA(cudaStreamSynchronize(stream));
+            int digit = 0;
+            long long acc = 0;
+            for (; digit < (1 << b); ++digit) {
+                if (acc + (long long)h[(size_t)digit] > rank) break;
+                acc += (long long)h[(size_t)digit];
+            }
+            if (digit >= (1 << b)) throw Failure(PGC_ERR_INTERNAL, "median selection lost its rank");
+            rank -= acc;
+            prefix |= (unsigned long long)digit << shift;
+            mask |= (((unsigned long long)1 << b) - 1) << shift;
+        }
+        const unsigned long long u = (prefix >> 63) ? (prefix & 0x7fffffffffffffffULL) : ~prefix;
+        double x;
+        std::memcpy(&x, &u, sizeof(x));
+        return x;
+    };
+    if (count % 2 == 0) {
+        const double a = select((count - 2) / 2), b = select((count - 2) / 2 + 1);
+        return (a + b) / 2.0;
+    }
+    return select(count / 2);
+}
+
+void Graph::rescale_column(int col, double scaling) {
+    const double med = std::max(median_of_column(col), 0.001);
+    const double factor = scaling / (2.0 * med);
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    e32[col].alloc((size_t)total);
+    wCount.alloc(1);
+    const int one = 1;
+    PGC_CUDA(cudaMemcpyAsync(wCount.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    PGC_CUDA(launch_rescale(e64[col].p, e32[col].p, total, stride, T.entries[INTER], T.nY, dTedge[INTER].p,
+                            dTedge[INTRA].p, factor, 100 * scaling, wCount.p, stream));
+    stats.launches++;
+    int exact = 0;
+    PGC_CUDA(cudaMemcpyAsync(&exact, wCount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+    f32Valid[col] = exact != 0;
+    f32Known[col] = true;
+}
+
+void Graph::ensure_f32(int col) {
+    if (f32Known[col]) return;
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    e32[col].alloc((size_t)total);
+    wCount.alloc(1);
+    const int one = 1;
+    PGC_CUDA(cudaMemcpyAsync(wCount.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    PGC_CUDA(launch_to_f32(e64[col].p, e32[col].p, total, stride, T.entries[INTER], T.nY, dTedge[INTER].p,
+                           dTedge[INTRA].p, wCount.p, stream));
+    stats.launches++;
+    int exact = 0;
+    PGC_CUDA(cudaMemcpyAsync(&exact, wCount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+    f32Valid[col] = exact != 0;
+    f32Known[col] = true;
+}
+
+// ---------------------------------------------------------------------------
+// Solver plumbing
+// ---------------------------------------------------------------------------
+Graph::Run Graph::prepare_run(int K, bool ratio) {
+    if (K < 1) throw Failure(PGC_ERR_ARG, "max depth must be >= 1");
+    const long long expanded = (long long)T.n * (T.nY + 1) * K;
+    if (expanded >= INT_MAX) throw Failure(PGC_ERR_ARG, "product graph too large for 32-bit expanded node ids");
+    Run r{};
+    r.K = K;
+    r.Kp = 1;
+    while (r.Kp < K) r.Kp <<= 1;
+    ensure_f32(0);
+    r.costF32 = f32Valid[0] ? 1 : 0;
+    r.cost = r.costF32 ? (const void*)e32[0].p : (const void*)e64[0].p;
+    if (ratio && ncols > 1) {
+        ensure_f32(1);
+        r.timeKind = f32Valid[1] ? 1 : 2;
+        r.time = f32Valid[1] ? (const void*)e32[1].p : (const void*)e64[1].p;
+        r.tconst = 0;
+    } else {
+        r.timeKind = 0;
+        r.time = nullptr;
+        r.tconst = ratio ? 50000.0 : 0.0;
+    }
+    r.threads = env_int("PGC_BF_THREADS", 512);
+    int blocks = env_int("PGC_BF_BLOCKS", 0);
+    const int warpsPerBlock = r.threads / 32;
+    const int needed = (T.nslices + warpsPerBlock - 1) / warpsPerBlock;
+    if (blocks <= 0) {
+        if (T.n <= env_int("PGC_BF_SINGLE_CTA_MAX_NODES", 8192)) {
+            blocks = 1;
+        } else {
+            int sms = 0, perSm = 0;
+            PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+            PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, &perSm));
+            blocks = sms * std::max(1, std::min(perSm, 1));
+        }
+    }
+    blocks = std::max(1, std::min(blocks, std::max(1, needed)));
+    if (blocks > 1) {
+        int sms = 0, perSm = 0;
+        PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, &perSm));
+        blocks = std::min(blocks, sms * std::max(1, perSm));
+    }
+    r.blocks = blocks;
+    r.coop = blocks > 1;
+    ensure_workspace(K, blocks);
+    return r;
+}
+
+void Graph::ensure_workspace(int K, int blocks) {
+    const size_t n = (size_t)T.n;
+    int Kp = 1;
+    while (Kp < K) Kp <<= 1;
+    const size_t expanded = n * (size_t)(T.nY + 1) * (size_t)K;
+    if (wsK != K || wPred.n < expanded) {
+        wDp.alloc(2 * n * Kp);
+        wOrg.alloc(2 * n * Kp);
+        wHops.alloc(2 * n * Kp);
+        wPred.alloc(expanded);
+        PGC_CUDA(cudaMemsetAsync(wPred.p, 0xff, expanded * sizeof(int), stream));  // -1
+        wsK = K;
+    }
+    if (wBak.n < n) {
+        wBak.alloc(n);
+        wLapNext.alloc(n);
+        wLapSteps.alloc(n);
+        wMark.alloc(n);
+        wMark.zero(stream);
+        ctlWalkId = 0;
+        wCandStat.alloc(n);
+        wCandV0.alloc(n);
+        wCandSteps.alloc(n);
+        wBranch.alloc(n);
+        wLb.alloc(n);
+        wOrigin.alloc(n);
+        wMean.alloc(n);
+    }
+    if (wLayerFlag.n < (size_t)T.nY + 1) {
+        wLayerFlag.alloc((size_t)T.nY + 1);
+        wLayerFlag.zero(stream);
+        ctlEpoch = 0;
+    }
+    wCtl.alloc(1);
+    wRedVal.alloc(2 * (size_t)blocks);
+    wRedIdx.alloc(2 * (size_t)blocks);
+    wRedAux.alloc((size_t)blocks);
+    wRedAux64.alloc((size_t)blocks);
+    const size_t cap = std::min<size_t>((size_t)numNodes() + 4, (size_t)1 << 26);
+    wCycle.alloc(cap);
+}
+
+void Graph::upload_branch(const std::vector<int>& branchOf) {
+    PGC_CUDA(cudaMemcpyAsync(wBranch.p, branchOf.data(), branchOf.size() * sizeof(int), cudaMemcpyHostToDevice,
+                             stream));
+}
+
+BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, double ub) {
+    BfParams p{};
+    p.n = T.n;
+    p.nY = T.nY;
+    p.K = r.K;
+    p.Kp = r.Kp;
+    p.nslices = T.nslices;
+    p.numNodes = numNodes();
+    p.spInter = dSp[INTER].p;
+    p.spIntra = dSp[INTRA].p;
+    p.srcInter = dSrc[INTER].p;
+    p.srcDummy = dSrcDummy.p;
+    p.srcIntra = dSrc[INTRA].p;
+    p.interEntries = T.entries[INTER];
+    p.intraEntries = T.entries[INTRA];
+    p.layerStride = T.layerStride();
+    p.cost = r.cost;
+    p.time = r.time;
+    p.tconst = r.tconst;
+    p.dp = wDp.p;
+    p.bak = wBak.p;
+    p.pred = wPred.p;
+    p.org = wOrg.p;
+    p.hops = wHops.p;
+    p.lapNext = wLapNext.p;
+    p.lapSteps = wLapSteps.p;
+    p.mark = wMark.p;
+    p.candStat = wCandStat.p;
+    p.candV0 = wCandV0.p;
+    p.candSteps = wCandSteps.p;
+    p.layerFlag = wLayerFlag.p;
+    p.branchOf = wBranch.p;
+    p.branchId = branchId;
+    p.lambda = lambda;
+    p.ub = ub;
+    p.mode = mode;
+    p.maxSweeps = 0;
+    p.ctl = wCtl.p;
+    p.cycleBuf = wCycle.p;
+    p.cycleCap = (long long)wCycle.n;
+    p.redVal = wRedVal.p;
+    p.redIdx = wRedIdx.p;
+    p.redAux = wRedAux.p;
+    p.redAux64 = wRedAux64.p;
+    p.lbOut = wLb.p;
+    p.originOut = wOrigin.p;
+    return p;
+}
+
+Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
+    Control c{};
+    c.epoch = ctlEpoch;
+    c.walkId = ctlWalkId;
+    PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
+    cudaEvent_t e0, e1;
+    PGC_CUDA(cudaEventCreate(&e0));
+    PGC_CUDA(cudaEventCreate(&e1));
+    PGC_CUDA(cudaEventRecord(e0, stream));
+    PGC_CUDA(launch_bf(p, r.costF32, r.timeKind, r.blocks, r.threads, r.coop, stream));
+    PGC_CUDA(cudaEventRecord(e1, stream));
+    stats.launches++;
+    PGC_CUDA(cudaMemcpyAsync(&c, wCtl.p, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    stats.deviceMs += ms;
+    ctlEpoch = c.epoch;
+    ctlWalkId = c.walkId;
+    stats.bfCalls++;
+    stats.sweeps += c.sweeps;
+    stats.candidates += c.candidates;
+    stats.fallbackWalks += c.fallbackWalks;
+    if (c.error) throw Failure(PGC_ERR_TIMEOUT, "a grid barrier wait of the Bellman-Ford kernel ran out");
+    if (c.status == BF_ERR_EMPTY_BRANCH) throw Failure(PGC_ERR_INTERNAL, "no nodes in branch");
+    if (c.status == BF_ERR_CYCLE_CAP) throw Failure(PGC_ERR_INTERNAL, "cycle longer than its buffer");
+    if (c.status == BF_ERR_WALK) throw Failure(PGC_ERR_INTERNAL, "predecessor walk left the node range");
+    if (c.status == BF_RUNNING) throw Failure(PGC_ERR_INTERNAL, "Bellman-Ford launch ended without a verdict");
+    return c;
+}
+
+std::vector<int> Graph::read_cycle_buffer(int len) {
+    std::vector<int> out((size_t)std::max(0, len));
+    if (len > 0)
+        PGC_CUDA(cudaMemcpyAsync(out.data(), wCycle.p, sizeof(int) * (size_t)len, cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+    return out;
+}
+
+void Graph::lookup_pairs(const std::vector<int>& src, const std::vector<int>& trgt, std::vector<long long>& edges,
+                         std::vector<double>& c, std::vector<double>& t, double tconst) {
+    const size_t m = src.size();
+    edges.assign(m, -2);
+    c.assign(m, 0);
+    t.assign(m, 0);
+    if (m == 0) return;
+    wPairS.upload(src.data(), m, stream);
+    wPairT.upload(trgt.data(), m, stream);
+    wEdgeOut.alloc(m);
+    wCOut.alloc(m);
+    wTOut.alloc(m);
+    LookupArgs a{};
+    a.n = T.n;
+    a.nY = T.nY;
+    a.numNodes = numNodes();
+    a.eBlock = T.eBlock;
+    a.spInter = dSp[INTER].p;
+    a.spIntra = dSp[INTRA].p;
+    a.srcInter = dSrc[INTER].p;
+    a.srcDummy = dSrcDummy.p;
+    a.srcIntra = dSrc[INTRA].p;
+    a.tedgeInter = dTedge[INTER].p;
+    a.tedgeIntra = dTedge[INTRA].p;
+    a.interEntries = T.entries[INTER];
+    a.layerStride = T.layerStride();
+    a.c64 = e64[0].p;
+    a.t64 = ncols > 1 ? e64[1].p : nullptr;
+    a.tconst = tconst;
+    a.pairSrc = wPairS.p;
+    a.pairTrgt = wPairT.p;
+    a.count = (int)m;
+    a.edgeOut = wEdgeOut.p;
+    a.cOut = wCOut.p;
+    a.tOut = wTOut.p;
+    PGC_CUDA(launch_lookup_pairs(a, stream));
+    stats.launches++;
+    PGC_CUDA(cudaMemcpyAsync(edges.data(), wEdgeOut.p, m * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaMemcpyAsync(c.data(), wCOut.p, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaMemcpyAsync(t.data(), wTOut.p, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Graph::rows_for_edges(const std::vector<long long>& edges) {
+    resCols = T.cols();
+    resRows = (int64_t)edges.size();
+    resMatching.assign((size_t)(resRows * resCols), 0);
+    for (size_t i = 0; i < edges.size(); ++i) product_row(T, EY.data(), edges[i], &resMatching[i * (size_t)resCols]);
+    resEdges = edges;
+}
+
+// ---------------------------------------------------------------------------
+// Cost/time-ratio solver (cost_time_ratio_solver.cpp:741-900)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct RatioEval {
+    double ratio, wsum;
+};
+
+// computeRatioForCycle (cost_time_ratio_solver.cpp:88-133) over the per-pair
+// costs and times of a stored cycle.
+RatioEval eval_cycle(const CycleRec& cy, double lambda) {
+    double C = 0, Tm = 0, W = 0;
+    for (size_t i = 0; i < cy.c.size(); ++i) {
+        C += cy.c[i];
+        Tm += cy.t[i];
+        W += cy.c[i] - lambda * cy.t[i];
+    }
+    return {C / Tm, W};
+}
+
+}  // namespace
+
+void Graph::solve_ratio(int K) {
+    ensure_generated();
+    stats = Stats();
+    const auto wall0 = std::chrono::steady_clock::now();
+    const double scaling = 100000.0;
+    // In-place rescale of the generator's costs (cost_time_ratio_solver.cpp:875-882).
+    rescale_column(0, scaling);
+    if (ncols > 1) rescale_column(1, scaling);
+
+    Run r = prepare_run(K, true);
+    reset_predecessors();
+    const int n = T.n;
+    const long long nn = numNodes();
+    const double tconst = ncols > 1 ? 0.0 : scaling / 2;
+    const double tolerance = (double)(float)1e-8;
+
+    // A cycle from the device walk (p(v0), ..., v0) -> reference order
+    // [v0, ..., p(v0), v0 + numNodes], with its edges.
+    auto make_cycle = [&](std::vector<int> walk, bool closeWithCopy) {
+        CycleRec cy;
+        std::reverse(walk.begin(), walk.end());
+        if (closeWithCopy) walk.push_back(walk.front() + (int)nn);
+        cy.nodes = walk;
+        std::vector<int> s, t;
+        for (size_t i = 0; i + 1 < walk.size(); ++i) {
+            int a = walk[i], b = walk[i + 1];
+            if (b < n && a > n) b += (int)nn;  // cost_time_ratio_solver.cpp:109-111
+            s.push_back(a);
+            t.push_back(b);
+        }
+        lookup_pairs(s, t, cy.edges, cy.c, cy.t, tconst);
+        for (long long e : cy.edges)
+            if (e < 0) throw Failure(PGC_ERR_INTERNAL, "cycle edge not found in the product graph");
+        return cy;
+    };
+
+    std::vector<int> branchOf((size_t)n, 0);
+    CycleRec negativeCycle;
+    double currentRatio = 0;
+    int numNodesInBranch = 0;
+
+    // ---- initial upper bound (cost_time_ratio_solver.cpp:652-707) ----
+    {
+        std::vector<float> mean((size_t)n);
+        std::vector<int> cnt((size_t)n);
+        PGC_CUDA(launch_layer1_mean(e64[0].p, T.layerStride(), T.entries[INTER], n, T.nslices, dSp[INTER].p,
+                                    dSp[INTRA].p, dSrc[INTER].p, dSrc[INTRA].p, wMean.p, wCandStat.p, stream));
+        stats.launches++;
+        PGC_CUDA(cudaMemcpyAsync(mean.data(), wMean.p, sizeof(float) * n, cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaMemcpyAsync(cnt.data(), wCandStat.p, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaStreamSynchronize(stream));
+        float bestCost = std::numeric_limits<float>::infinity();
+        int bestV = 0;
+        for (int v = 0; v < n; ++v)
+            if (mean[(size_t)v] < bestCost && cnt[(size_t)v] > 3) {
+                bestCost = mean[(size_t)v];
+                bestV = v;
+            }
+        std::fill(branchOf.begin(), branchOf.end(), 1);
+        branchOf[(size_t)bestV] = 0;
+        upload_branch(branchOf);
+        currentRatio = 10;
+        const double ub = (double)std::numeric_limits<float>::infinity();
+        const Control c = launch_bf_call(r, params(r, 1, 0, currentRatio, ub));
+        if (c.status != BF_UB_DONE)
+            throw Failure(PGC_ERR_INTERNAL, "no closed path through the upper-bound start node");
+        numNodesInBranch = c.numInBranch;
+        negativeCycle = make_cycle(read_cycle_buffer(c.cycleLen), false);
+        RatioEval ev = eval_cycle(negativeCycle, currentRatio);
+        double cycleCost = (double)(float)ev.wsum;
+        int guard = 0;
+        while (cycleCost > 0 || std::isnan(cycleCost)) {
+            if (++guard > 4000) throw Failure(PGC_ERR_INTERNAL, "upper-bound ratio search does not terminate");
+            currentRatio += currentRatio;
+            ev = eval_cycle(negativeCycle, currentRatio);
+            cycleCost = (double)(float)ev.wsum;
+        }
+        currentRatio = (double)(float)ev.ratio;
+    }
+
+    // ---- branch and bound (cost_time_ratio_solver.cpp:794-851) ----
+    int branchId = 0, maxBranchId = 0;
+    double ratioUpperBound = currentRatio;
+    double lowerBoundOfCurrentBranch = 0;
+    std::vector<int> zeroLayerHits;
+    BranchHeap heap(n);
+    heap.push(0, branchId);
+    std::vector<unsigned char> validLb((size_t)n, 0);
+    std::map<int, CycleRec> validCycles;
+    std::fill(branchOf.begin(), branchOf.end(), 0);
+    upload_branch(branchOf);
+
+    auto bellman_ford = [&](double lambda) -> BfOutcome {
+        const Control c = launch_bf_call(r, params(r, 0, branchId, lambda, std::numeric_limits<float>::infinity()));
+        numNodesInBranch = c.numInBranch;
+        auto old_is_zero = [&]() {
+            return round_to_int(eval_cycle(negativeCycle, lambda).wsum) == 0;
+        };
+        switch (c.status) {
+            case BF_LAYER_UNREACHED:
+            case BF_WRAP_NO_IMPROVE:
+                return old_is_zero() ? BfOutcome::ZERO_CYCLE : BfOutcome::NO_NEGATIVE_CYCLE;
+            case BF_MAX_SWEEPS:
+                return BfOutcome::NO_NEGATIVE_CYCLE;
+            case BF_FOUND_CYCLE: {
+                CycleRec cy = make_cycle(read_cycle_buffer(c.cycleLen), true);
+                const int integral = round_to_int(eval_cycle(cy, lambda).wsum);
+                if (integral < 0) {
+                    negativeCycle = std::move(cy);
+                    return BfOutcome::FOUND_NEGATIVE_CYCLE;
+                }
+                if (integral == 0) return BfOutcome::NO_NEGATIVE_CYCLE;
+                return old_is_zero() ? BfOutcome::ZERO_CYCLE : BfOutcome::NO_NEGATIVE_CYCLE;
+            }
+            default:
+                throw Failure(PGC_ERR_INTERNAL, "unexpected Bellman-Ford status " + std::to_string(c.status));
+        }
+    };
+
+    // lawlerSoubroutine (cost_time_ratio_solver.cpp:558-635)
+    auto lawler = [&]() -> bool {
+        int i = 0;
+        const int maxiter = 1000;
+        double oldRatio = currentRatio;
+        for (;;) {
+            const BfOutcome s = bellman_ford(currentRatio);
+            stats.lawlerIters++;
+            if (s != BfOutcome::FOUND_NEGATIVE_CYCLE) break;
+            currentRatio = eval_cycle(negativeCycle, currentRatio).ratio;
+            if (std::fabs(oldRatio - currentRatio) < tolerance) break;
+            if (currentRatio - tolerance > oldRatio) break;
+            oldRatio = currentRatio;
+            if (i > maxiter) break;
+            ++i;
+        }
+        lowerBoundOfCurrentBranch = currentRatio;
+        int numWraps = 0;
+        zeroLayerHits.clear();
+        bool entered = true, left = false;
+        for (int vtx : negativeCycle.nodes) {
+            if (left && vtx < n) { entered = true; left = false; }
+            if (entered) { zeroLayerHits.push_back(vtx); entered = false; }
+            if (vtx >= n && !left) { ++numWraps; left = true; }
+        }
+        return numWraps > 1;
+    };
+
+    while (!heap.isEmpty()) {
+        const auto top = heap.pop();
+        branchId = (int)top.second;
+        if (validLb[(size_t)branchId]) {
+            ratioUpperBound = top.first;
+            negativeCycle = validCycles.at(branchId);
+            break;
+        }
+        stats.branches++;
+        currentRatio = ratioUpperBound;
+        const bool wraps = lawler();
+        if (ratioUpperBound < heap.peak() && !wraps) break;
+        if (!wraps) {
+            // ratioLowerBoundOfCurrentBranch is never assigned in the reference
+            // (cost_time_ratio_solver.cpp:835); the branch's final ratio is used.
+            heap.push(lowerBoundOfCurrentBranch, branchId);
+            validLb[(size_t)branchId] = 1;
+            validCycles.emplace(branchId, negativeCycle);
+            continue;
+        }
+        if (numNodesInBranch == 1) continue;
+        // branch() (cost_time_ratio_solver.cpp:142-179; the rest is unreachable)
+        int offset = 0;
+        for (int hit : zeroLayerHits) {
+            if (offset > 0) branchOf[(size_t)hit] = maxBranchId + offset;
+            ++offset;
+        }
+        for (int v = 0; v < n; ++v)
+            if (branchOf[(size_t)v] == branchId) branchOf[(size_t)v] = maxBranchId;
+        maxBranchId += offset;
+        for (int hit : zeroLayerHits) heap.push(lowerBoundOfCurrentBranch, branchOf[(size_t)hit]);
+        upload_branch(branchOf);
+    }
+
+    const RatioEval fin = eval_cycle(negativeCycle, currentRatio);
+    resPasses = true;
+    resObjective = (float)fin.ratio;
+    rows_for_edges(negativeCycle.edges);
+    (void)wall0;
+}
+
+// ---------------------------------------------------------------------------
+// Minimum-cost solver (dijkstra_solver.cpp:203-579)
+// ---------------------------------------------------------------------------
+void Graph::solve_min_cost(int K) {
+    ensure_generated();
+    stats = Stats();
+    Run r = prepare_run(K, false);
+    reset_predecessors();
+    const int n = T.n;
+    const long long nn = numNodes();
+
+    // branch graph: the reference's branchGraph when it exists (conjugate
+    // graph, or plain graph with pruning), else the in-edge sets of layer 0.
+    // Entries are used as edge ids (SRCIds(e)), exactly as the reference does.
+    std::vector<std::vector<long>> bg;
+    const bool haveBranchGraph = conj || prune;
+    if (haveBranchGraph) {
+        std::vector<std::set<long>> sets((size_t)n);
+        if (!conj) {
+            for (int64_t j = 0; j < nex; ++j) sets[(size_t)EX[2 * j]].insert(EX[2 * j + 1]);
+        } else {
+            std::vector<std::vector<int>> out((size_t)T.nvx);
+            for (int64_t e = 0; e < nex; ++e) out[(size_t)EX[2 * e]].push_back((int)e);
+            const long nE = (long)nex;
+            for (long j = 0; j < nE; ++j) {
+                sets[(size_t)j].insert(j + nE);
+                if (!prune) {
+                    sets[(size_t)(j + nE)].insert(j + 2 * nE);
+                    sets[(size_t)(j + 2 * nE)].insert(j);
+                } else {
+                    sets[(size_t)(j + nE)].insert(j);
+                }
+                for (int e : out[(size_t)EX[2 * j]]) {
+                    sets[(size_t)j].insert(e);
+                    sets[(size_t)(j + nE)].insert(e + nE);
+                    if (!prune) sets[(size_t)(j + 2 * nE)].insert(e + 2 * nE);
+                }
+            }
+        }
+        bg.resize((size_t)n);
+        for (int v = 0; v < n; ++v) bg[(size_t)v].assign(sets[(size_t)v].begin(), sets[(size_t)v].end());
+    } else {
+        bg.assign((size_t)n, std::vector<long>{-1});
+        for (int64_t t = 0; t < T.eBlock; ++t)
+            if (!T.eNext[(size_t)t]) bg[(size_t)T.eTrgt[(size_t)t]].push_back((long)t);
+    }
+    // SRCIds(e) of an edge id (block * eBlock + offset).
+    auto src_of = [&](long e) -> long {
+        if (e < 0) return -1;
+        const long long b = e / T.eBlock, t = e % T.eBlock;
+        if (b >= T.nY) return LONG_MAX;
+        return (long)(b * n + T.eSrc[(size_t)t]);
+    };
+
+    std::vector<int> branchOf((size_t)n, 0);
+    upload_branch(branchOf);
+    int branchId = 0, maxBranchId = 0, numNodesInBranch = 0;
+    double upperBound = std::numeric_limits<double>::infinity();
+    double lowerBoundOfCurrentBranch = 0;
+    bool upperboundFoundOnFirstTry = false;
+    int branchingSrcNode = -1, branchingTargetNode = -1;
+    std::vector<int> cycle;  // walk order: [p(vLast), ..., start]
+    std::vector<std::pair<double, int>> lowerBounds;
+
+    auto extract = [&](int v) {
+        BfParams p = params(r, 2, branchId, 0.0, upperBound);
+        Control c{};
+        c.epoch = ctlEpoch;
+        c.walkId = ctlWalkId;
+        PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
+        PGC_CUDA(launch_extract_path(p, v, stream));
+        stats.launches++;
+        PGC_CUDA(cudaMemcpyAsync(&c, wCtl.p, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaStreamSynchronize(stream));
+        if (c.status < 0) throw Failure(PGC_ERR_INTERNAL, "minimum-cost path extraction failed");
+        return read_cycle_buffer(c.cycleLen);
+    };
+
+    // mooreBellmanFordSubroutineCPU (dijkstra_solver.cpp:203-388)
+    auto bellman_ford = [&]() -> bool {
+        const Control c = launch_bf_call(r, params(r, 2, branchId, 0.0, upperBound));
+        numNodesInBranch = c.numInBranch;
+        if (c.status == BF_LAYER_UNREACHED) return false;
+        if (!c.anyFinite) return false;
+        lowerBounds.clear();
+        upperboundFoundOnFirstTry = false;
+        const float lb1 = (float)c.firstLb;
+        if (!std::isinf(lb1)) {
+            lowerBoundOfCurrentBranch = lb1;
+            if (c.validV == c.firstV) {
+                upperboundFoundOnFirstTry = true;
+                const float newUb = lb1;
+                if (newUb > upperBound) return false;
+                if (newUb < upperBound) {
+                    upperBound = newUb;
+                    cycle = extract(c.firstV);
+                }
+                return true;
+            }
+            // The branching pair is the candidate vertex and the start vertex of
+            // its path (dijkstra_bnb_subroutine.cu:444-445; the CPU solver's
+            // source id at dijkstra_solver.cpp:381 is negative and seeds nothing).
+            branchingSrcNode = c.firstV;
+            branchingTargetNode = c.firstOrigin;
+        }
+        if (c.validV >= 0) {
+            const float newUb = (float)c.validLb;
+            if (newUb < upperBound) {
+                upperBound = newUb;
+                cycle = extract(c.validV);
+            }
+        }
+        return true;
+    };
+
+    // branch (dijkstra_solver.cpp:87-174)
+    auto branch = [&](int newId) {
+        std::vector<double> lb((size_t)n);
+        PGC_CUDA(cudaMemcpyAsync(lb.data(), wLb.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaStreamSynchronize(stream));
+        lowerBounds.clear();
+        for (int v = 0; v < n; ++v)
+            if (branchOf[(size_t)v] == branchId) lowerBounds.push_back({lb[(size_t)v], v});
+        std::sort(lowerBounds.begin(), lowerBounds.end());
+        std::vector<double> mark((size_t)n, -1.0);
+        BranchHeap h(n);
+        for (int i = 0; i < n; ++i) {
+            mark[(size_t)i] = -1;
+            if (i == branchingSrcNode || i == branchingTargetNode) { mark[(size_t)i] = 1; continue; }
+            if (branchOf[(size_t)i] == branchId) h.push(std::numeric_limits<double>::infinity(), i);
+        }
+        h.push(0.0, branchingSrcNode);
+        h.push(0.0, branchingTargetNode);
+        if (branchingTargetNode >= 0 && branchingTargetNode < n) branchOf[(size_t)branchingTargetNode] = newId;
+        int counter = 0;
+        for (const auto& e : lowerBounds) {
+            const int v = e.second;
+            if (v == branchingSrcNode || v == branchingTargetNode) continue;
+            if (branchOf[(size_t)v] != branchId) continue;
+            if (counter > std::max(1, numNodesInBranch / 4)) {
+                h.push(0.1, v);
+                branchOf[(size_t)v] = newId;
+            }
+            ++counter;
+        }
+        while (!h.isEmpty()) {
+            const auto cur = h.pop();
+            const int node = (int)cur.second;
+            const float nodeCost = (float)cur.first;
+            mark[(size_t)node] = 1.0;
+            for (long e : bg[(size_t)node]) {
+                if (e == -1) continue;
+                const long s = haveBranchGraph ? src_of(e) : src_of(e);
+                if (s < 0 || s >= n) continue;
+                if (mark[(size_t)s] < 0) {
+                    const float oldV = (float)h.peakKey(s);
+                    const float newV = nodeCost + 1.0f;
+                    if (newV < oldV) {
+                        h.decrease(s, newV);
+                        branchOf[(size_t)s] = branchOf[(size_t)node];
+                    }
+                }
+            }
+        }
+        branchingSrcNode = -1;
+        branchingTargetNode = -1;
+        upload_branch(branchOf);
+    };
+
+    BranchHeap heap(n);
+    heap.push(0.0, branchId);
+    std::vector<unsigned char> validLb((size_t)n, 0);
+    std::map<int, std::vector<int>> validCycles;
+    while (!heap.isEmpty()) {
+        const auto top = heap.pop();
+        branchId = (int)top.second;
+        if (validLb[(size_t)branchId]) {
+            upperBound = top.first;
+            cycle = validCycles.at(branchId);
+            break;
+        }
+        stats.branches++;
+        if (!bellman_ford()) continue;
+        if (upperBound < heap.peak() && upperboundFoundOnFirstTry) break;
+        if (upperboundFoundOnFirstTry) {
+            heap.push(lowerBoundOfCurrentBranch, branchId);
+            validLb[(size_t)branchId] = 1;
+            validCycles.emplace(branchId, cycle);
+            continue;
+        }
+        ++maxBranchId;
+        if (maxBranchId >= n) throw Failure(PGC_ERR_INTERNAL, "branch id exceeds the node count");
+        branch(maxBranchId);
+        heap.push(lowerBoundOfCurrentBranch, branchId);
+        heap.push(lowerBoundOfCurrentBranch, maxBranchId);
+    }
+    if (cycle.empty()) throw Failure(PGC_ERR_INTERNAL, "no cycle found");
+
+    // path output (dijkstra_solver.cpp:511-557)
+    std::vector<int> cyc = cycle;
+    std::reverse(cyc.begin(), cyc.end());
+    cyc.push_back(cyc.front() + (int)nn);
+    const size_t loopmax = cyc.size();
+    std::vector<int> ps, pt;
+    std::vector<size_t> pairIndex;
+    int loops = 0;
+    for (size_t i = 0; i < loopmax; ++i) {
+        const int s = cyc[i % loopmax], t = cyc[(i + 1) % loopmax];
+        if (t >= nn) ++loops;
+        if (t < n && s >= nn && t == s - nn) continue;  // the dummy marker -1 matches first
+        ps.push_back(s);
+        pt.push_back(t);
+    }
+    std::vector<long long> edges;
+    std::vector<double> cc, tt;
+    lookup_pairs(ps, pt, edges, cc, tt, 0.0);
+    std::vector<long long> found;
+    for (long long e : edges)
+        if (e >= 0) found.push_back(e);
+    resPasses = loops < 2;
+    resObjective = (float)upperBound;
+    rows_for_edges(found);
+}
+
+void Graph::cost_vector(double* out) {
+    ensure_generated();
+    const long long rows = (long long)T.nY * T.eBlock;
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    DBuf<double> tmp;
+    tmp.alloc((size_t)(rows * ncols));
+    for (int c = 0; c < ncols; ++c)
+        PGC_CUDA(launch_export(e64[c].p, tmp.p, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
+                               dTedge[INTER].p, dTedge[INTRA].p, stream));
+    PGC_CUDA(cudaMemcpyAsync(out, tmp.p, sizeof(double) * (size_t)(rows * ncols), cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Graph::product_space(int32_t* out) {
+    ensure_generated();
+    const long long rows = (long long)T.nY * T.eBlock;
+    const int cols = T.cols();
+    for (long long e = 0; e < rows; ++e) product_row(T, EY.data(), e, out + e * cols);
+}
+
+// writeToFile (product_graph_generators.cpp:272-282) with
+// utils::writeMatrixToFile (utils.hpp:24-32): full precision, ", " between
+// columns, a newline between rows and none after the last row.
+void Graph::export_csv() {
+    auto writeD = [](const std::vector<double>& m, int64_t rows, int64_t cols, const std::string& name) {
+        std::ofstream f(name + ".csv");
+        if (!f.is_open()) return;
+        f.precision(17);
+        for (int64_t i = 0; i < rows; ++i) {
+            for (int64_t j = 0; j < cols; ++j) {
+                if (j) f << ", ";
+                f << m[(size_t)(i * cols + j)];
+            }
+            if (i + 1 < rows) f << "\n";
+        }
+    };
+    auto writeI = [](const std::vector<int>& m, int64_t rows, int64_t cols, const std::string& name) {
+        std::ofstream f(name + ".csv");
+        if (!f.is_open()) return;
+        for (int64_t i = 0; i < rows; ++i) {
+            for (int64_t j = 0; j < cols; ++j) {
+                if (j) f << ", ";
+                f << m[(size_t)(i * cols + j)];
+            }
+            if (i + 1 < rows) f << "\n";
+        }
+    };
+    writeD(VX, nvx, 3, "VX");
+    writeD(VY, nvy, 3, "VY");
+    writeI(EX, nex, 2, "EX");
+    writeI(EY, ney, 2, "EY");
+    writeD(FD, nvx, nvy, "FeatDiffMatrix");
+    if (conj) {
+        writeD(NX, nvx, 3, "NX");
+        writeD(NY, nvy, 3, "NY");
+    }
+}
+
+}  // namespace pgc
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using pgc::Failure;
+using pgc::Graph;
+
+struct pgc_graph {
+    Graph g;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        pgc::g_lastError.clear();
+        return PGC_OK;
+    } catch (const Failure& e) {
+        pgc::g_lastError = e.what();
+        // consume a non-sticky runtime error so that it is not reported again
+        // by the next launch check
+        if (e.code == PGC_ERR_CUDA) (void)cudaGetLastError();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        pgc::g_lastError = "host allocation failed";
+        return PGC_ERR_INTERNAL;
+    } catch (const std::exception& e) {
+        pgc::g_lastError = e.what();
+        return PGC_ERR_INTERNAL;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgc_create(const double* VX, int64_t nvx, const int32_t* EX, int64_t nex, const double* VY, int64_t nvy,
+               const int32_t* EY, int64_t ney, const double* feat_diff, int use_conjugate_graph,
+               int use_regularising_cost_term, int prune_intralayer, pgc_graph** out) {
+    return guarded([&] {
+        if (!out) throw Failure(PGC_ERR_ARG, "out is null");
+        *out = nullptr;
+        if (!VX || !EX || !VY || !EY || !feat_diff) throw Failure(PGC_ERR_ARG, "null input");
+        if (nvx < 1 || nex < 1 || nvy < 1 || ney < 1) throw Failure(PGC_ERR_ARG, "empty input");
+        std::unique_ptr<pgc_graph> h(new pgc_graph());
+        Graph& g = h->g;
+        g.nvx = nvx; g.nex = nex; g.nvy = nvy; g.ney = ney;
+        g.VX.assign(VX, VX + 3 * nvx);
+        g.EX.assign(EX, EX + 2 * nex);
+        g.VY.assign(VY, VY + 3 * nvy);
+        g.EY.assign(EY, EY + 2 * ney);
+        g.FD.assign(feat_diff, feat_diff + nvx * nvy);
+        g.conj = use_conjugate_graph != 0;
+        g.reg = use_regularising_cost_term != 0;
+        g.prune = prune_intralayer != 0;
+        PGC_CUDA(cudaGetDevice(&g.device));
+        PGC_CUDA(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        *out = h.release();
+    });
+}
+
+void pgc_destroy(pgc_graph* g) { delete g; }
+
+int pgc_set_normals(pgc_graph* h, const double* NX, int64_t rx, int64_t cx, const double* NY, int64_t ry,
+                    int64_t cy) {
+    return guarded([&] {
+        Graph& g = h->g;
+        if (rx != g.nvx || cx != 3)
+            throw Failure(PGC_ERR_ARG,
+                          "normals for shape X do not contain as many entries as expected. Assumed shape = |VX| x 3");
+        if (ry != g.nvy || cy != 3)
+            throw Failure(PGC_ERR_ARG,
+                          "normals for shape Y do not contain as many entries as expected. Assumed shape = |VY| x 3");
+        g.NX.assign(NX, NX + 3 * rx);
+        g.NY.assign(NY, NY + 3 * ry);
+        g.normalsGiven = true;
+    });
+}
+
+int pgc_set_max_depth(pgc_graph* h, int k) {
+    return guarded([&] { h->g.maxDepth = k; });
+}
+
+int pgc_set_cost_time_ratio_mode(pgc_graph* h, const char* cost, const char* time) {
+    return guarded([&] {
+        h->g.costName = cost ? cost : "";
+        h->g.timeName = time ? time : "";
+    });
+}
+
+int pgc_update_robust_loss_params(pgc_graph* h, double alpha, double c, double pwr) {
+    return guarded([&] {
+        Graph& g = h->g;
+        if (!g.conj) return;
+        if (g.generated) throw Failure(PGC_ERR_STATE, "cannot update robust loss params after model has been generated");
+        g.rlAlpha = alpha;
+        g.rlC = c;
+        g.rlPwr = pwr;
+    });
+}
+
+int pgc_generate(pgc_graph* h) {
+    return guarded([&] {
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.generate();
+    });
+}
+
+int pgc_cost_vector_shape(pgc_graph* h, int64_t* rows, int64_t* cols) {
+    return guarded([&] {
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.ensure_generated();
+        *rows = (int64_t)h->g.T.nY * h->g.T.eBlock;
+        *cols = h->g.ncols;
+    });
+}
+
+int pgc_get_cost_vector(pgc_graph* h, double* out) {
+    return guarded([&] {
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.cost_vector(out);
+    });
+}
+
+int pgc_product_space_shape(pgc_graph* h, int64_t* rows, int64_t* cols) {
+    return guarded([&] {
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.ensure_generated();
+        *rows = (int64_t)h->g.T.nY * h->g.T.eBlock;
+        *cols = h->g.T.cols();
+    });
+}
+
+int pgc_get_product_space(pgc_graph* h, int32_t* out) {
+    return guarded([&] {
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.product_space(out);
+    });
+}
+
+int pgc_solve_with_cost_time_ratio(pgc_graph* h, const char* solver, int max_depth) {
+    return guarded([&] {
+        Graph& g = h->g;
+        const std::string name = solver ? solver : "";
+        const int K = max_depth >= 1 ? max_depth : g.maxDepth;
+        if (name == "export") {
+            g.export_csv();
+            g.resPasses = false;
+            g.resObjective = -1.0f;
+            g.resRows = 4;
+            g.resCols = 1;
+            g.resMatching.assign(4, 0);
+            g.resEdges.clear();
+            return;
+        }
+        if (name != "lawlercpu" && name != "lawlergpu")
+            throw Failure(PGC_ERR_SOLVER, "Solver >>" + name + "<< is not implemented");
+        PGC_CUDA(cudaSetDevice(g.device));
+        g.solve_ratio(K);
+    });
+}
+
+int pgc_solve_with_minimum_cost(pgc_graph* h, const char* solver, int max_depth) {
+    return guarded([&] {
+        Graph& g = h->g;
+        const std::string name = solver ? solver : "";
+        const int K = max_depth >= 1 ? max_depth : g.maxDepth;
+        if (name == "export") {
+            g.export_csv();
+            g.resPasses = false;
+            g.resObjective = -1.0f;
+            g.resRows = 4;
+            g.resCols = 1;
+            g.resMatching.assign(4, 0);
+            g.resEdges.clear();
+            return;
+        }
+        PGC_CUDA(cudaSetDevice(g.device));
+        g.solve_min_cost(K);
+    });
+}
+
+int pgc_result(pgc_graph* h, int* passes, float* objective, int64_t* rows, int64_t* cols) {
+    return guarded([&] {
+        const Graph& g = h->g;
+        if (passes) *passes = g.resPasses ? 1 : 0;
+        if (objective) *objective = g.resObjective;
+        if (rows) *rows = g.resRows;
+        if (cols) *cols = g.resCols;
+    });
+}
+
+int pgc_result_matching(pgc_graph* h, int32_t* out) {
+    return guarded([&] {
+        const Graph& g = h->g;
+        std::memcpy(out, g.resMatching.data(), sizeof(int32_t) * g.resMatching.size());
+    });
+}
+
+int pgc_result_cycle_edges(pgc_graph* h, int64_t* out, int64_t capacity, int64_t* count) {
+    return guarded([&] {
+        const Graph& g = h->g;
+        *count = (int64_t)g.resEdges.size();
+        for (int64_t i = 0; i < *count && i < capacity; ++i) out[i] = g.resEdges[(size_t)i];
+    });
+}
+
+int pgc_result_stats(pgc_graph* h, int64_t* out8) {
+    return guarded([&] {
+        const pgc::Stats& s = h->g.stats;
+        out8[0] = s.bfCalls;
+        out8[1] = s.sweeps;
+        out8[2] = s.candidates;
+        out8[3] = s.lawlerIters;
+        out8[4] = s.branches;
+        out8[5] = s.fallbackWalks;
+        out8[6] = (int64_t)(s.deviceMs * 1000.0);
+        out8[7] = s.launches;
+    });
+}
+
+// utils::normals2d (helper/utils.cpp:93-157).
+int pgc_compute_normals_2d(const double* Vin, int64_t nv, const int32_t* E, int64_t ne, double* out) {
+    return guarded([&] {
+        if (nv != ne) throw Failure(PGC_ERR_ARG, "V.rows() != E.rows()");
+        std::vector<double> V(Vin, Vin + 3 * nv);
+        int zero = -1;
+        for (int i = 0; i < 3; ++i) {
+            double s = 0;
+            for (int64_t r = 0; r < nv; ++r) s += V[(size_t)(3 * r + i)];
+            if (std::fabs(s) < 1e-4) { zero = i; break; }
+        }
+        if (zero == -1) throw Failure(PGC_ERR_ARG, "points dont lie on xy, xz or yz plane");
+        if (zero != 2) {
+            const int order[3] = {zero == 1 ? 0 : 1, 2, zero == 1 ? 1 : 0};
+            std::vector<double> W(V.size());
+            for (int64_t r = 0; r < nv; ++r)
+                for (int k = 0; k < 3; ++k) W[(size_t)(3 * r + k)] = V[(size_t)(3 * r + order[k])];
+            V.swap(W);
+        }
+        std::vector<double> en((size_t)(3 * ne)), el((size_t)ne);
+        for (int64_t i = 0; i < ne; ++i) {
+            const int a = E[2 * i], b = E[2 * i + 1];
+            const double ev[3] = {V[(size_t)(3 * a)] - V[(size_t)(3 * b)], V[(size_t)(3 * a + 1)] - V[(size_t)(3 * b + 1)],
+                                  V[(size_t)(3 * a + 2)] - V[(size_t)(3 * b + 2)]};
+            el[(size_t)i] = std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+            // rotation about z: (x, y, z) -> (y, -x, z)
+            double nrm[3] = {ev[1], -ev[0], ev[2]};
+            const double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+            for (int k = 0; k < 3; ++k) en[(size_t)(3 * i + k)] = len > 0 ? nrm[k] / len : nrm[k];
+        }
+        float maxX = -INFINITY, minX = INFINITY, maxY = -INFINITY, minY = INFINITY;
+        {
+            double mx = -INFINITY, mn = INFINITY, my = -INFINITY, mny = INFINITY;
+            for (int64_t r = 0; r < nv; ++r) {
+                mx = std::max(mx, V[(size_t)(3 * r)]); mn = std::min(mn, V[(size_t)(3 * r)]);
+                my = std::max(my, V[(size_t)(3 * r + 1)]); mny = std::min(mny, V[(size_t)(3 * r + 1)]);
+            }
+            maxX = (float)mx; minX = (float)mn; maxY = (float)my; minY = (float)mny;
+        }
+        const float mult = (float)(0.1 * std::min(std::fabs(maxX - minX), std::fabs(maxY - minY)));
+        double mm = -INFINITY;
+        for (int64_t r = 0; r < nv; ++r) mm = std::max(mm, V[(size_t)(3 * r)] + (double)mult * en[(size_t)(3 * r)]);
+        if ((float)mm < maxX)
+            for (auto& x : en) x = -x;
+        for (int64_t i = 1; i < nv + 1; ++i) {
+            const int64_t j = i % nv;
+            double v[3];
+            for (int k = 0; k < 3; ++k)
+                v[k] = el[(size_t)(i - 1)] * en[(size_t)(3 * (i - 1) + k)] + el[(size_t)j] * en[(size_t)(3 * j + k)];
+            const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            for (int k = 0; k < 3; ++k) out[3 * j + k] = len > 0 ? v[k] / len : v[k];
+        }
+    });
+}
+
+// utils::normals3d (helper/utils.cpp:86-90): libigl's per_vertex_normals
+// with its default (area) weighting -- the sum of the incident faces' unit
+// normals weighted by twice their area, i.e. of their edge cross products.
+int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_t nf, double* out) {
+    return guarded([&] {
+        for (int64_t i = 0; i < 3 * nv; ++i) out[i] = 0.0;
+        for (int64_t f = 0; f < nf; ++f) {
+            const int a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
+            if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv)
+                throw Failure(PGC_ERR_ARG, "F refers to a vertex outside V");
+            double u[3], w[3];
+            for (int k = 0; k < 3; ++k) {
+                u[k] = V[3 * b + k] - V[3 * a + k];
+                w[k] = V[3 * c + k] - V[3 * a + k];
+            }
+            const double nrm[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+            for (int k = 0; k < 3; ++k) {
+                out[3 * a + k] += nrm[k];
+                out[3 * b + k] += nrm[k];
+                out[3 * c + k] += nrm[k];
+            }
+        }
+        for (int64_t i = 0; i < nv; ++i) {
+            const double len = std::sqrt(out[3 * i] * out[3 * i] + out[3 * i + 1] * out[3 * i + 1] +
+                                         out[3 * i + 2] * out[3 * i + 2]);
+            if (len > 0)
+                for (int k = 0; k < 3; ++k) out[3 * i + k] /= len;
+        }
+    });
+}
+
+const char* pgc_last_error(void) { return pgc::g_lastError.c_str(); }
+
+const char* pgc_version(void) { return "pgc-b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,225 @@
+"""cyclic_product_graphs -- drop-in Python front-end of the sm_100a cycle search.
+
+Mirrors the reference module of the same name (pythonbinding/bindings.cpp:22-48):
+the class ``product_graph_generator`` with ``generate``, ``get_cost_vector``,
+``update_robust_loss_params``, ``set_normals``, ``get_product_space``,
+``solve_with_cost_time_ratio``, ``solve_with_minimum_cost``,
+``set_max_depth_cost_time_ratio`` and ``set_cost_time_ratio_mode``, and the
+helpers ``compute_normals_3d`` / ``compute_normals_2d``.  Solves return the
+reference's tuple ``(passes_layers_just_once: bool, final_objective: float,
+matching: int32 ndarray)``.
+
+Everything runs through the C ABI of ``lib/libpgc.so`` (include/pgc.h); the
+solvers execute on the GPU.  There is no CPU fallback: importing this module
+without the built library raises ImportError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
+           "compute_local_thickness_2d", "library_path", "PGCError"]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
+
+if not os.path.exists(library_path):
+    raise ImportError(f"cyclic_product_graphs: {library_path} is missing; build it with "
+                      "`python -c 'import __graft_entry__ as g; g.build()'` (or make -C product-graph-cycles_b200/csrc)")
+
+_lib = ctypes.CDLL(library_path)
+_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lp = ctypes.POINTER(ctypes.c_int64)
+_h = ctypes.c_void_p
+
+_lib.pgc_create.argtypes = [_dp, _i64, _ip, _i64, _dp, _i64, _ip, _i64, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                            ctypes.POINTER(_h)]
+_lib.pgc_destroy.argtypes = [_h]
+_lib.pgc_destroy.restype = None
+_lib.pgc_set_normals.argtypes = [_h, _dp, _i64, _i64, _dp, _i64, _i64]
+_lib.pgc_set_max_depth.argtypes = [_h, ctypes.c_int]
+_lib.pgc_set_cost_time_ratio_mode.argtypes = [_h, ctypes.c_char_p, ctypes.c_char_p]
+_lib.pgc_update_robust_loss_params.argtypes = [_h, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+_lib.pgc_generate.argtypes = [_h]
+_lib.pgc_cost_vector_shape.argtypes = [_h, _lp, _lp]
+_lib.pgc_get_cost_vector.argtypes = [_h, _dp]
+_lib.pgc_product_space_shape.argtypes = [_h, _lp, _lp]
+_lib.pgc_get_product_space.argtypes = [_h, _ip]
+_lib.pgc_solve_with_cost_time_ratio.argtypes = [_h, ctypes.c_char_p, ctypes.c_int]
+_lib.pgc_solve_with_minimum_cost.argtypes = [_h, ctypes.c_char_p, ctypes.c_int]
+_lib.pgc_result.argtypes = [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), _lp, _lp]
+_lib.pgc_result_matching.argtypes = [_h, _ip]
+_lib.pgc_result_cycle_edges.argtypes = [_h, _lp, _i64, _lp]
+_lib.pgc_result_stats.argtypes = [_h, _lp]
+_lib.pgc_compute_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
+_lib.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
+_lib.pgc_last_error.restype = ctypes.c_char_p
+_lib.pgc_version.restype = ctypes.c_char_p
+
+
+class PGCError(RuntimeError):
+    """A libpgc call failed; ``code`` is the PGC_ERR_* value."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[pgc {code}] {message}")
+        self.code = code
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise PGCError(rc, _lib.pgc_last_error().decode(errors="replace"))
+
+
+def _f64(a, cols=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if cols is not None and (a.ndim != 2 or a.shape[1] != cols):
+        raise ValueError(f"expected an [n x {cols}] matrix, got shape {a.shape}")
+    return a
+
+
+def _i32(a, cols=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+    if cols is not None and (a.ndim != 2 or a.shape[1] != cols):
+        raise ValueError(f"expected an [n x {cols}] matrix, got shape {a.shape}")
+    return a
+
+
+def version() -> str:
+    return _lib.pgc_version().decode()
+
+
+class product_graph_generator:
+    """product_graph_generator(VX, EX, VY, EY, feat_diff, use_conjugate_graph,
+    use_regularising_cost_term[, prune_intralayer])  (bindings.cpp:33-34)."""
+
+    def __init__(self, VX, EX, VY, EY, feat_diff, use_conjugate_graph: bool, use_regularising_cost_term: bool,
+                 prune_intralayer: bool = False):
+        VX = _f64(VX, 3)
+        EX = _i32(EX, 2)
+        VY = _f64(VY, 3)
+        EY = _i32(EY, 2)
+        FD = _f64(feat_diff)
+        if FD.shape != (VX.shape[0], VY.shape[0]):
+            raise ValueError(f"feat_diff must be |VX| x |VY| = {(VX.shape[0], VY.shape[0])}, got {FD.shape}")
+        h = _h()
+        _check(_lib.pgc_create(VX.ctypes.data_as(_dp), VX.shape[0], EX.ctypes.data_as(_ip), EX.shape[0],
+                               VY.ctypes.data_as(_dp), VY.shape[0], EY.ctypes.data_as(_ip), EY.shape[0],
+                               FD.ctypes.data_as(_dp), int(bool(use_conjugate_graph)),
+                               int(bool(use_regularising_cost_term)), int(bool(prune_intralayer)), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.pgc_destroy(h)
+            self._h = None
+
+    # -- configuration -----------------------------------------------------
+    def set_normals(self, NX, NY):
+        """setNormals (product_graph_generators.cpp:118-130); shapes |VX| x 3 and |VY| x 3."""
+        NX = _f64(NX)
+        NY = _f64(NY)
+        if NX.ndim != 2 or NY.ndim != 2:
+            raise ValueError("normals must be 2-d matrices")
+        _check(_lib.pgc_set_normals(self._h, NX.ctypes.data_as(_dp), NX.shape[0], NX.shape[1],
+                                    NY.ctypes.data_as(_dp), NY.shape[0], NY.shape[1]))
+
+    def set_max_depth_cost_time_ratio(self, max_depth: int):
+        _check(_lib.pgc_set_max_depth(self._h, int(max_depth)))
+
+    def set_cost_time_ratio_mode(self, cost_name: str, time_name: str):
+        _check(_lib.pgc_set_cost_time_ratio_mode(self._h, str(cost_name).encode(), str(time_name).encode()))
+
+    def update_robust_loss_params(self, alpha: float, c: float, pwr: float):
+        _check(_lib.pgc_update_robust_loss_params(self._h, float(alpha), float(c), float(pwr)))
+
+    # -- graph ---------------------------------------------------------------
+    def generate(self):
+        _check(_lib.pgc_generate(self._h))
+
+    def get_cost_vector(self) -> np.ndarray:
+        r, c = _i64(), _i64()
+        _check(_lib.pgc_cost_vector_shape(self._h, ctypes.byref(r), ctypes.byref(c)))
+        out = np.empty((r.value, c.value), dtype=np.float64)
+        _check(_lib.pgc_get_cost_vector(self._h, out.ctypes.data_as(_dp)))
+        return out
+
+    def get_product_space(self) -> np.ndarray:
+        r, c = _i64(), _i64()
+        _check(_lib.pgc_product_space_shape(self._h, ctypes.byref(r), ctypes.byref(c)))
+        out = np.empty((r.value, c.value), dtype=np.int32)
+        _check(_lib.pgc_get_product_space(self._h, out.ctypes.data_as(_ip)))
+        return out
+
+    # -- solvers -------------------------------------------------------------
+    def _result(self):
+        p = ctypes.c_int()
+        o = ctypes.c_float()
+        r, c = _i64(), _i64()
+        _check(_lib.pgc_result(self._h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(r), ctypes.byref(c)))
+        m = np.empty((r.value, c.value), dtype=np.int32)
+        _check(_lib.pgc_result_matching(self._h, m.ctypes.data_as(_ip)))
+        return bool(p.value), float(o.value), m
+
+    def solve_with_cost_time_ratio(self, solver_name: str, max_depth: int | None = None):
+        """Minimum cost/time-ratio cycle (Lawler), bindings.cpp:41-42."""
+        _check(_lib.pgc_solve_with_cost_time_ratio(self._h, str(solver_name).encode(),
+                                                   -1 if max_depth is None else int(max_depth)))
+        return self._result()
+
+    def solve_with_minimum_cost(self, solver_name: str, max_depth: int | None = None):
+        """Minimum-cost cycle, bindings.cpp:44-45."""
+        _check(_lib.pgc_solve_with_minimum_cost(self._h, str(solver_name).encode(),
+                                                -1 if max_depth is None else int(max_depth)))
+        return self._result()
+
+    # -- extras (no counterpart in the reference's binding) ------------------
+    def last_cycle_edges(self) -> np.ndarray:
+        """Edge ids (rows of get_product_space()) of the last returned cycle."""
+        cnt = _i64()
+        _check(_lib.pgc_result_cycle_edges(self._h, None, 0, ctypes.byref(cnt)))
+        out = np.empty(cnt.value, dtype=np.int64)
+        _check(_lib.pgc_result_cycle_edges(self._h, out.ctypes.data_as(_lp), cnt.value, ctypes.byref(cnt)))
+        return out
+
+    def last_stats(self) -> dict:
+        buf = (ctypes.c_int64 * 8)()
+        _check(_lib.pgc_result_stats(self._h, buf))
+        keys = ["bf_calls", "sweeps", "candidates", "lawler_iters", "branches", "fallback_walks", "device_us",
+                "kernel_launches"]
+        return dict(zip(keys, list(buf)))
+
+
+def compute_normals_2d(V, E) -> np.ndarray:
+    """utils::normals2d (helper/utils.cpp:93-157)."""
+    V = _f64(V, 3)
+    E = _i32(E, 2)
+    out = np.empty_like(V)
+    _check(_lib.pgc_compute_normals_2d(V.ctypes.data_as(_dp), V.shape[0], E.ctypes.data_as(_ip), E.shape[0],
+                                       out.ctypes.data_as(_dp)))
+    return out
+
+
+def compute_normals_3d(V, F) -> np.ndarray:
+    """utils::normals3d (helper/utils.cpp:86-90): area-weighted vertex normals."""
+    V = _f64(V, 3)
+    F = _i32(F, 3)
+    out = np.empty_like(V)
+    _check(_lib.pgc_compute_normals_3d(V.ctypes.data_as(_dp), V.shape[0], F.ctypes.data_as(_ip), F.shape[0],
+                                       out.ctypes.data_as(_dp)))
+    return out
+
+
+def compute_local_thickness_3d(*args, **kwargs):
+    """Unimplemented in the reference as well (bindings.cpp:18-20, :28)."""
+    print("TODO: IMPL")
+
+
+def compute_local_thickness_2d(*args, **kwargs):
+    """Unimplemented in the reference as well (bindings.cpp:18-20, :29)."""
+    print("TODO: IMPL")
