@@ -1,0 +1,373 @@
+"""Benchmark of the cycle-search hot path on B200.
+
+Workload (default): one shape pair on the GPU -- a perturbed genus-0 mesh X
+with 5,000 vertices (both orientations of its ~30k edges) and normals, a
+200-point closed silhouette curve Y with in-plane normals, 64-d float32
+features -> feat_diff; conjugate product graph, k = 3, cost/time mode
+("vanilla", "lengthnormalisation") [cost = feature difference, time = edge
+length].  Inputs are seeded synthetic data of that shape (no dataset).
+
+One step = recompute the edge costs on the device (generate) + one minimum
+cost/time-ratio cycle solve (lawlergpu).  `value` is solves/s with the inputs
+resident in HBM, timed with CUDA events on the solver's stream; `e2e` is the
+same solve through the public API from host arrays (handle creation, host ->
+device copies, template build, solve, matching read back).
+
+--impl reference times the reference algorithm's CPU implementation (the
+restatement under oracle/; the reference itself cannot be compiled in this
+environment) on the host cores: a full lawlercpu solve during warm-up gives
+the sweep count, each timed step times a bounded sample (one Bellman-Ford
+sweep), and solves/s = 1 / (energy + rescale + in-edge sets + sweeps x sweep).
+
+Multi-GPU: the path does not shard within a pair; --gpus N runs N independent
+replicas (one pair per rank, seed = rank), value = total solves / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "product-graph-cycles_b200"))
+
+METRIC = "ratio-cycle solves/s + fwd/bwd pairs/s, 1 B200, vs plain GPU Lawler; BF HBM GB/s"
+WORKLOADS = {
+    # name: (n_vertices, n_curve, feat_dim, conj, reg, prune, cost, time, k)
+    "single_pair_conj_5k_200_k3": (5000, 200, 64, True, False, False, "vanilla", "lengthnormalisation", 3),
+    "plain_642_60_k2": (642, 60, 32, False, False, False, "vanilla", "nomode", 2),
+    # smaller conjugate pair used for ncu captures (inputs still larger than L2)
+    "conj_2k_100_k3": (2000, 100, 64, True, False, False, "vanilla", "lengthnormalisation", 3),
+}
+DEFAULT_WORKLOAD = "single_pair_conj_5k_200_k3"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _make_pair(name, seed):
+    from cyclic_product_graphs import synthetic
+
+    nv, ny, dim, conj, reg, prune, cost, tme, k = WORKLOADS[name]
+    if name.startswith("plain_642"):
+        p = synthetic.make_pair(icosphere_level=3, n_curve=ny, feat_dim=dim, seed=seed)
+    else:
+        p = synthetic.make_pair(n_vertices=nv, n_curve=ny, feat_dim=dim, seed=seed)
+    return p, dict(conj=conj, reg=reg, prune=prune, cost=cost, time=tme, k=k)
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def algorithmic_bytes_per_sweep(info, k, ratio_mode):
+    """HBM bytes one Bellman-Ford sweep must move (roofline).
+
+    Every real edge's cost (and time, in ratio mode with two cost columns)
+    is streamed once per sweep as float32; every (node, depth) of every layer
+    writes its int32 predecessor.  The in-edge template (one layer), the
+    distance rows and the origin rows are L2-resident and not counted.
+    """
+    L = info["layers"]
+    edges = L * (info["inter_edges_per_layer"] + info["intra_edges_per_layer"])
+    per_edge = 4 * (2 if (ratio_mode and info["cost_columns"] > 1) else 1)
+    preds = 4 * k * info["nodes_per_layer"] * (L + 1)
+    return edges * per_edge + preds
+
+
+def run_ours(args, world, rank):
+    import numpy as np
+    import torch
+
+    import cyclic_product_graphs as cpg
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dev = torch.cuda.current_device()
+    pair, cfg = _make_pair(args.workload, seed=args.seed + rank)
+    k = cfg["k"]
+    hargs = (pair["VX"], pair["EX"], pair["VY"], pair["EY"], pair["feat_diff"], cfg["conj"], cfg["reg"], cfg["prune"])
+
+    g = cpg.product_graph_generator(*hargs)
+    if cfg["conj"]:
+        g.set_normals(pair["NX"], pair["NY"])
+    g.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+    stream = torch.cuda.Stream()
+    g.set_stream(stream.cuda_stream)
+    g.generate()
+    info = g.graph_info()
+
+    def step():
+        g.generate()
+        return g.solve_with_cost_time_ratio("lawlergpu", k)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sweeps = bf_us = launches = 0
+    result = None
+    with ClockSampler(dev) as clocks:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            result = step()
+            ev[i][1].record(stream)
+            st = g.last_stats()
+            sweeps += st["sweeps"]
+            bf_us += st["device_us"]
+            launches += st["kernel_launches"] + 1  # + the energy kernel of generate()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1000.0)
+
+    # roofline of the dominant kernel (the Bellman-Ford launch)
+    peak, peak_kind = _peaks()
+    b_sweep = algorithmic_bytes_per_sweep(info, k, True)
+    achieved = (b_sweep * sweeps) / (bf_us * 1e-6) / 1e9 if bf_us else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"bf_kernel_{args.workload}.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # end to end through the public API from host buffers
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    h2d = sum(int(np.asarray(pair[key]).nbytes) for key in ("VX", "EX", "VY", "EY", "feat_diff"))
+    if cfg["conj"]:
+        h2d += int(pair["NX"].nbytes + pair["NY"].nbytes)
+    d2h = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ge = cpg.product_graph_generator(*hargs)
+        if cfg["conj"]:
+            ge.set_normals(pair["NX"], pair["NY"])
+        ge.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+        out = ge.solve_with_cost_time_ratio("lawlergpu", k)
+        d2h = int(out[2].nbytes) + 8
+        del ge
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = world * e2e_steps / e2e_s
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 (fp32 integer-valued cost streams)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "k": k, "nodes_per_layer": info["nodes_per_layer"],
+                   "layers": info["layers"], "edges": info["layers"] * info["edges_per_block"],
+                   "cost_mode": [cfg["cost"], cfg["time"]], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (cost streams > 126 MB)"},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_kernel",
+                     "algorithmic_bytes_per_sweep": b_sweep, "sweeps_per_solve": sweeps / args.steps,
+                     "bf_ms_per_solve": bf_us / 1000.0 / args.steps},
+        "clocks": clocks.summary(),
+        "result": {"objective": result[1], "cycle_edges": int(result[2].shape[0])},
+        "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pair, cfg, sweeps / args.steps, args.cpu_sweeps)
+    return line
+
+
+def cpu_baseline(pair, cfg, sweeps_per_solve, sample_sweeps):
+    """The reference algorithm on the host cores: measured phases of one ratio
+    solve, with `sample_sweeps` Bellman-Ford sweeps timed and scaled to the
+    solve's sweep count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    hargs = (pair["VX"], pair["EX"], pair["VY"], pair["EY"], pair["feat_diff"], cfg["conj"], cfg["reg"], cfg["prune"])
+    o = orc.OracleGenerator(*hargs)
+    if cfg["conj"]:
+        o.set_normals(pair["NX"], pair["NY"])
+    o.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+    t0 = time.perf_counter()
+    o.generate()
+    t_gen = time.perf_counter() - t0
+    ph = o.time_phases(cfg["k"], 0.3, sample_sweeps)
+    t_solve = ph["energy_s"] + ph["rescale_s"] + ph["in_graph_s"] + sweeps_per_solve * ph["sweep_s"]
+    return {"value": 1.0 / t_solve, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": (f"oracle lawlercpu restatement, OpenMP x{cores}: energy {ph['energy_s']:.2f}s + rescale "
+                       f"{ph['rescale_s']:.2f}s + in-edge sets {ph['in_graph_s']:.2f}s measured, "
+                       f"{sample_sweeps} Bellman-Ford sweeps timed ({ph['sweep_s']:.3f}s each) and scaled to "
+                       f"{sweeps_per_solve:.1f} sweeps/solve; product-graph build {t_gen:.1f}s not counted"),
+            "phases_s": ph}
+
+
+def run_reference(args):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    pair, cfg = _make_pair(args.workload, seed=args.seed)
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    hargs = (pair["VX"], pair["EX"], pair["VY"], pair["EY"], pair["feat_diff"], cfg["conj"], cfg["reg"], cfg["prune"])
+    o = orc.OracleGenerator(*hargs)
+    if cfg["conj"]:
+        o.set_normals(pair["NX"], pair["NY"])
+    o.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+    o.generate()
+    # warm-up: one full solve fixes the sweep count of a solve
+    t0 = time.perf_counter()
+    res = o.solve_with_cost_time_ratio("lawlercpu", cfg["k"])
+    t_full = time.perf_counter() - t0
+    stats = o.last_stats()
+    sweeps = stats["sweeps"]
+    samples = []
+    for _ in range(args.steps):
+        samples.append(o.time_phases(cfg["k"], 0.3, 1))
+    sweep_s = statistics.median(s["sweep_s"] for s in samples)
+    fixed = statistics.median(s["energy_s"] + s["rescale_s"] + s["in_graph_s"] for s in samples)
+    t_solve = fixed + sweeps * sweep_s
+    value = 1.0 / t_solve
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * (fixed + sweep_s), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "k": cfg["k"]},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": f"one Bellman-Ford sweep + energy/rescale/in-edge phases per step, scaled to "
+                                   f"{sweeps} sweeps/solve; a full warm-up solve took {t_full:.1f}s"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "full_solve_s": t_full, "result": {"objective": res[1], "cycle_edges": int(res[2].shape[0])},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sweeps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = _dist_env()
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    line = run_ours(args, world, rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -67,6 +67,11 @@ int pgc_set_cost_time_ratio_mode(pgc_graph* g, const char* cost_name, const char
  * Ignored for the plain graph and after generate(), as in the reference. */
 int pgc_update_robust_loss_params(pgc_graph* g, double alpha, double c, double pwr);
 
+/* Runs all device work of the handle on the given cudaStream_t (passed as a
+ * pointer; NULL restores the handle's own stream).  No reference counterpart:
+ * lets a caller order the solver with its own work and time it with events. */
+int pgc_set_stream(pgc_graph* g, void* cuda_stream);
+
 /* generate() -- product_graph_generators.cpp:21-89, bindings.cpp:35.
  * Builds the product graph and its edge costs on the device. */
 int pgc_generate(pgc_graph* g);
@@ -113,6 +118,16 @@ int pgc_compute_normals_2d(const double* V, int64_t nv, const int32_t* E, int64_
  * vertex normals of a triangle mesh (libigl per_vertex_normals with its
  * default weighting).  V [nv x 3], F [nf x 3]; out [nv x 3]. */
 int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_t nf, double* out);
+
+/* Sizes of the generated graph (no reference counterpart): [nodes per layer,
+ * layers, edges per Y edge, interlayer edges per layer, intralayer edges per
+ * layer, interlayer slots per layer, intralayer slots per layer (slots include
+ * the sliced-ELL padding), cost columns]. */
+int pgc_graph_info(pgc_graph* g, int64_t* out8);
+
+/* Returns the device memory cached by the library's allocator to CUDA (no
+ * reference counterpart; freed buffers are otherwise kept for reuse). */
+int pgc_release_cached_memory(void);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char* pgc_last_error(void);

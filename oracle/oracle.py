@@ -58,6 +58,8 @@ def lib():
         L.orc_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(_i64)]
         L.orc_last_error.restype = ctypes.c_char_p
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_time_phases.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_double)]
         L.orc_time_sweeps.restype = ctypes.c_double
         L.orc_time_sweeps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         _lib = L
@@ -178,6 +180,12 @@ class OracleGenerator:
         buf = (_i64 * 5)()
         lib().orc_stats(self._h, buf)
         return dict(zip(["bf_calls", "sweeps", "candidates_walked", "lawler_iters", "branches"], buf[:5]))
+
+    def time_phases(self, k, lam, sweeps):
+        """[energy, rescale, in-edge sets, seconds per sweep] of a CPU ratio solve."""
+        buf = (ctypes.c_double * 4)()
+        lib().orc_time_phases(self._h, int(k), float(lam), int(sweeps), buf)
+        return dict(zip(["energy_s", "rescale_s", "in_graph_s", "sweep_s"], list(buf)))
 
     def time_sweeps(self, k, lam, sweeps):
         return lib().orc_time_sweeps(self._h, int(k), float(lam), int(sweeps))

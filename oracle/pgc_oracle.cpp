@@ -1568,6 +1568,61 @@ void orc_stats(void* h, long long* out5) {
     out5[0] = s.bfCalls; out5[1] = s.sweeps; out5[2] = s.candidatesWalked; out5[3] = s.lawlerIters; out5[4] = s.branches;
 }
 
+// Phase timings of one ratio solve on the CPU, for the benchmark's CPU
+// baseline: out4 = [energy, rescale, in-edge sets, seconds per sweep].  The
+// energy is recomputed and rescaled in place; `sweeps` sweeps are run at
+// ratio `lambda` by repeated Bellman-Ford calls.
+void orc_time_phases(void* h, int k, double lambda, int sweeps, double* out4) {
+    Generator* G = (Generator*)h;
+    if (!G->generated) G->generate();
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto secs = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+        return std::chrono::duration<double>(b - a).count();
+    };
+    auto t0 = now();
+    if (G->conj)
+        G->energy = ho_energy(G->VX, G->EX, G->NX, G->VY, G->EY, G->NY, G->g, G->FD, G->reg,
+                              RobustLoss{G->rlAlpha, G->rlC, G->rlPwr}, G->prune, G->costName, G->timeName);
+    else
+        G->energy = plain_energy(G->VX, G->VY, G->g.ps, G->FD, G->reg, G->costName, G->timeName);
+    auto t1 = now();
+    rescale_column(G->energy, 0, 100000.0);
+    if (G->energy.cols > 1) rescale_column(G->energy, 1, 100000.0);
+    auto t2 = now();
+    CtrState st;
+    SolveStats stats;
+    st.stats = &stats;
+    st.n = G->nodesPerLayer();
+    st.K = k;
+    st.numNodes = G->numNodes();
+    st.numLayers = st.numNodes / st.n;
+    st.inGraph = build_in_graph(G->g.src, G->g.trgt, st.numNodes + st.n, st.numNodes, st.n);
+    auto t3 = now();
+    st.pred.assign((size_t)(st.n * (st.numLayers + 1) * k), -1);
+    st.branchOf.assign((size_t)st.n, 0);
+    st.dp.assign((size_t)((2 * k + 1) * st.n), kInf);
+    st.seen.assign((size_t)st.n * (size_t)thread_count(), 0);
+    st.cost.resize((size_t)G->energy.rows);
+    st.time.resize((size_t)G->energy.rows);
+    for (i64 e = 0; e < G->energy.rows; ++e) {
+        st.cost[(size_t)e] = G->energy(e, 0);
+        st.time[(size_t)e] = G->energy.cols > 1 ? G->energy(e, 1) : 50000.0;
+    }
+    st.currentRatio = lambda;
+    st.upperBound = kInf;
+    st.tolerance = (double)(float)1e-8;
+    auto t4 = now();
+    while (stats.sweeps < sweeps) {
+        try { bellman_ford_ctr(st, G->g.ps, G->g.src, false, false); }
+        catch (const std::exception&) { break; }
+    }
+    auto t5 = now();
+    out4[0] = secs(t0, t1);
+    out4[1] = secs(t1, t2);
+    out4[2] = secs(t2, t3);
+    out4[3] = secs(t4, t5) / (double)std::max<long long>(1, stats.sweeps);
+}
+
 // Time `sweeps` Bellman-Ford sweeps of the ratio solver at ratio `lambda` on
 // the generated graph (the per-sweep CPU cost used by the benchmark's CPU
 // baseline).  Returns seconds.

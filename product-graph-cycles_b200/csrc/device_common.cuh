@@ -170,8 +170,9 @@ struct LookupArgs {
     double* tOut;
 };
 
+size_t bf_shared_table_bytes(int n, int Kp);
 cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
-                      cudaStream_t stream);
+                      size_t sharedBytes, cudaStream_t stream);
 cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, int* blocksPerSm);
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
@@ -179,6 +180,10 @@ cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s);
 cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s);
+cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,
+                                  cudaStream_t s);
+cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long above, unsigned long long* out,
+                                    cudaStream_t s);
 cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
                            int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
                            cudaStream_t s);

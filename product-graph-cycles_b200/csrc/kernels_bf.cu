@@ -55,22 +55,32 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     return v;
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Team barrier.  One CTA: __syncthreads.  Several CTAs (cooperative launch,
-// all resident): arrive on a global counter, the last arrival bumps the
-// generation word; waiters poll with a bounded number of iterations and
-// raise the error word if it runs out.  Returns false when the team must stop.
+// all resident): after the CTA-wide barrier, thread 0 arrives on a global
+// counter with release semantics (cumulative over the CTA's writes); the last
+// arrival resets the counter and bumps the generation word with release
+// semantics; the others poll the generation with acquire loads, spinning
+// briefly and then backing off, for a bounded number of iterations after
+// which the error word is raised.  Returns false when the team must stop.
 __device__ bool team_sync(const Team& t) {
     __shared__ int s_stop;
     __syncthreads();
     if (threadIdx.x == 0) {
         if (t.ncta > 1) {
             const unsigned g = ld_acquire_u32(t.gen);
-            __threadfence();
-            const unsigned arrived = atomicAdd(t.cnt, 1u);
+            const unsigned arrived = atom_add_acq_rel_u32(t.cnt, 1u);
             if (arrived == (unsigned)t.ncta - 1) {
                 atomicExch(t.cnt, 0u);
-                __threadfence();
-                atomicAdd(t.gen, 1u);
+                red_add_release_u32(t.gen, 1u);
             } else {
                 unsigned spins = 0;
                 while (ld_acquire_u32(t.gen) == g) {
@@ -78,10 +88,9 @@ __device__ bool team_sync(const Team& t) {
                         atomicExch(t.err, 1);
                         break;
                     }
-                    __nanosleep(100);
+                    if (spins > 4096) __nanosleep(64);
                 }
             }
-            __threadfence();
         }
         s_stop = *(volatile int*)t.err;
     }
@@ -142,10 +151,39 @@ __device__ __forceinline__ int original_index(int n, int K, int e) {
     return rem - depth * n + layer * n;
 }
 
+// Loads of the distance / origin tables: from shared memory when the whole
+// team is one CTA that keeps them there (S), else through L2 (other CTAs
+// write them during the launch, so L1 must not serve stale lines).
+template <bool S>
+__device__ __forceinline__ double ldD(const double* p) {
+    if constexpr (S) return *p;
+    else return __ldcg(p);
+}
+template <bool S>
+__device__ __forceinline__ double2 ldD2(const double* p) {
+    if constexpr (S) return *reinterpret_cast<const double2*>(p);
+    else return __ldcg(reinterpret_cast<const double2*>(p));
+}
+template <bool S>
+__device__ __forceinline__ int ldI(const int* p) {
+    if constexpr (S) return *p;
+    else return __ldcg(p);
+}
+
 // ---------------------------------------------------------------------------
 // One (layer, depth) step of the sweep.
+//
+// A warp owns a slice of 32 target nodes (lane = node).  The in-edges of the
+// slice are consumed in batches of kBatch slots: first every source index,
+// cost and time of the batch is loaded (independent, coalesced 128-byte
+// loads), then every source distance (one 16/32-byte vector gather per
+// source row), then the batch is folded into the running minimum in edge
+// order, so one batch costs about two memory latencies instead of two per
+// edge.
 // ---------------------------------------------------------------------------
-template <class CT, int TK>
+constexpr int kBatch = 4;
+
+template <class CT, int TK, bool S>
 __device__ void relax_step(const BfParams& p, const Team& t, int l, int k, int epoch) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const int par = l & 1;
@@ -165,6 +203,9 @@ __device__ void relax_step(const BfParams& p, const Team& t, int l, int k, int e
     const double* tstD = (TK == 2) ? (const double*)p.time + base : nullptr;
     int* predRow = p.pred + (size_t)l * n * K + (size_t)k * n;
     const int srcLayer = inter ? l - 1 : l;
+    const int nk = inter ? K : 1;            // source depths per edge
+    const int kofs = inter ? 0 : k - 1;      // first source depth
+    const double* srow = inter ? prv : cur;  // source rows
     const int lane = threadIdx.x & 31;
     const double lam = p.lambda, ub = p.ub;
     bool any = false;
@@ -172,33 +213,76 @@ __device__ void relax_step(const BfParams& p, const Team& t, int l, int k, int e
         const int v = s * 32 + lane;
         const bool valid = v < n;
         double best = kInfD;
-        if (l == 0 && valid) best = __ldcg(cur + (size_t)v * Kp + k);
+        if (l == 0 && valid) best = ldD<S>(cur + (size_t)v * Kp + k);
         int bs = -1, bk = -1;
         if (!empty) {
             const int j0 = __ldg(sp + s), j1 = __ldg(sp + s + 1);
-            for (int j = j0; j < j1; ++j) {
-                const size_t e = (size_t)j * 32 + lane;
-                const int sv = __ldg(src + e);
-                if (sv < 0) continue;
-                const double c = ld_stream(cst + e);
-                double tt;
-                if (TK == 0) tt = p.tconst;
-                else if (TK == 1) tt = (double)__ldg(tstF + e);
-                else tt = __ldg(tstD + e);
-                const double w = __dsub_rn(c, __dmul_rn(lam, tt));
-                if (inter) {
-                    const double* row = prv + (size_t)sv * Kp;
-                    for (int kk = 0; kk < K; ++kk) {
-                        const double d = __ldcg(row + kk);
-                        if (isinf(d)) continue;
-                        const double cand = __dadd_rn(d, w);
-                        if (cand < best && cand < ub) { best = cand; bs = sv; bk = kk; }
+            if (nk <= 4) {
+                for (int jb = j0; jb < j1; jb += kBatch) {
+                    int sv[kBatch];
+                    double cv[kBatch], tv[kBatch];
+#pragma unroll
+                    for (int u = 0; u < kBatch; ++u) {
+                        sv[u] = -1;
+                        cv[u] = 0.0;
+                        tv[u] = p.tconst;
+                        if (jb + u < j1) {
+                            const size_t e = (size_t)(jb + u) * 32 + lane;
+                            sv[u] = __ldg(src + e);
+                            cv[u] = ld_stream(cst + e);
+                            if (TK == 1) tv[u] = (double)__ldg(tstF + e);
+                            else if (TK == 2) tv[u] = __ldg(tstD + e);
+                        }
                     }
-                } else {
-                    const double d = __ldcg(cur + (size_t)sv * Kp + (k - 1));
-                    if (!isinf(d)) {
-                        const double cand = __dadd_rn(d, w);
-                        if (cand < best && cand < ub) { best = cand; bs = sv; bk = k - 1; }
+                    double d[kBatch][4];
+#pragma unroll
+                    for (int u = 0; u < kBatch; ++u) {
+                        d[u][0] = d[u][1] = d[u][2] = d[u][3] = kInfD;
+                        if (sv[u] >= 0) {
+                            const double* r = srow + (size_t)sv[u] * Kp + kofs;
+                            if (nk == 1) {
+                                d[u][0] = ldD<S>(r);
+                            } else {
+                                const double2 a = ldD2<S>(r);
+                                d[u][0] = a.x;
+                                d[u][1] = a.y;
+                                if (nk > 2) {
+                                    const double2 b = ldD2<S>(r + 2);
+                                    d[u][2] = b.x;
+                                    d[u][3] = b.y;
+                                }
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kBatch; ++u) {
+                        if (sv[u] < 0) continue;
+                        const double w = __dsub_rn(cv[u], __dmul_rn(lam, tv[u]));
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            if (kk >= nk || isinf(d[u][kk])) continue;
+                            const double cand = __dadd_rn(d[u][kk], w);
+                            if (cand < best && cand < ub) { best = cand; bs = sv[u]; bk = kofs + kk; }
+                        }
+                    }
+                }
+            } else {
+                for (int j = j0; j < j1; ++j) {
+                    const size_t e = (size_t)j * 32 + lane;
+                    const int sv = __ldg(src + e);
+                    if (sv < 0) continue;
+                    const double c = ld_stream(cst + e);
+                    double tt;
+                    if (TK == 0) tt = p.tconst;
+                    else if (TK == 1) tt = (double)__ldg(tstF + e);
+                    else tt = __ldg(tstD + e);
+                    const double w = __dsub_rn(c, __dmul_rn(lam, tt));
+                    const double* row = srow + (size_t)sv * Kp + kofs;
+                    for (int kk = 0; kk < nk; ++kk) {
+                        const double dd = ldD<S>(row + kk);
+                        if (isinf(dd)) continue;
+                        const double cand = __dadd_rn(dd, w);
+                        if (cand < best && cand < ub) { best = cand; bs = sv; bk = kofs + kk; }
                     }
                 }
             }
@@ -230,8 +314,8 @@ __device__ void relax_step(const BfParams& p, const Team& t, int l, int k, int e
                 } else {
                     const int* so = (inter && bs >= 0) ? porg : corg;
                     const int* sh = (inter && bs >= 0) ? phop : chop;
-                    o = __ldcg(so + (size_t)ps * Kp + pk);
-                    h = __ldcg(sh + (size_t)ps * Kp + pk) + 1;
+                    o = ldI<S>(so + (size_t)ps * Kp + pk);
+                    h = ldI<S>(sh + (size_t)ps * Kp + pk) + 1;
                 }
             }
             corg[(size_t)v * Kp + k] = o;
@@ -371,12 +455,22 @@ __device__ int dij_walk_end(const BfParams& p, int v) {
 // ---------------------------------------------------------------------------
 // The Bellman-Ford launch.  Every CTA of the grid belongs to one team.
 // ---------------------------------------------------------------------------
-template <class CT, int TK>
+template <class CT, int TK, bool S>
 __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
     Team t{(int)blockIdx.x, (int)gridDim.x, &p.ctl->barCount, &p.ctl->barGen, &p.ctl->error};
     const int n = p.n, K = p.K, Kp = p.Kp;
     const long long tid = t.thread(), nth = t.nthreads();
     const bool isLead = (blockIdx.x == 0 && threadIdx.x == 0);
+    if constexpr (S) {
+        // single-CTA team: distance, backup, origin and hop tables live in
+        // shared memory for the whole launch (layout as in global memory)
+        extern __shared__ double4 smemRaw[];
+        double* sm = reinterpret_cast<double*>(smemRaw);
+        p.dp = sm;
+        p.bak = sm + 2 * (size_t)n * Kp;
+        p.org = reinterpret_cast<int*>(p.bak + n);
+        p.hops = p.org + 2 * (size_t)n * Kp;
+    }
 
     // set-up (cost_time_ratio_solver.cpp:264-287): DP := inf, branch starts := 0
     for (long long i = tid; i < 2LL * n * Kp; i += nth) p.dp[i] = kInfD;
@@ -428,13 +522,13 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
     int sweep = 0;
     for (;;) {
         const int epoch = epochBase + sweep + 1;
-        for (long long i = tid; i < n; i += nth) p.bak[i] = __ldcg(p.dp + (size_t)i * Kp);
+        for (long long i = tid; i < n; i += nth) p.bak[i] = ldD<S>(p.dp + (size_t)i * Kp);
         if (!team_sync(t)) return;
         bool stop = false;
         for (int l = 0; l <= p.nY && !stop; ++l) {
             for (int k = 0; k < K; ++k) {
                 if (l == 0 && k == 0) continue;
-                relax_step<CT, TK>(p, t, l, k, epoch);
+                relax_step<CT, TK, S>(p, t, l, k, epoch);
                 if (!team_sync(t)) return;
             }
             if (l > 0 && l < p.nY && *(volatile int*)&p.layerFlag[l] != epoch) stop = true;
@@ -460,8 +554,8 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             const int* dOrg = p.org + (size_t)(p.nY & 1) * n * Kp;
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] != p.branchId) { p.lbOut[i] = kInfD; p.originOut[i] = -1; continue; }
-                const double lb = __ldcg(p.dp + (size_t)lastPar * n * Kp + (size_t)i * Kp + lastDepth);
-                int o = __ldcg(dOrg + (size_t)i * Kp);
+                const double lb = ldD<S>(p.dp + (size_t)lastPar * n * Kp + (size_t)i * Kp + lastDepth);
+                int o = ldI<S>(dOrg + (size_t)i * Kp);
                 if (o < 0 && !isinf((float)lb)) o = dij_walk_end(p, (int)i);
                 p.lbOut[i] = lb;
                 p.originOut[i] = o;
@@ -513,7 +607,7 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             const long long layerSpan = (long long)n * K;
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] == p.branchId) {
-                    const double cand = __ldcg(p.dp + (size_t)lastPar * n * Kp + (size_t)i * Kp + lastDepth);
+                    const double cand = ldD<S>(p.dp + (size_t)lastPar * n * Kp + (size_t)i * Kp + lastDepth);
                     const double b = p.bak[i];
                     if (cand < b) {
                         improved = 1;
@@ -532,8 +626,8 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
                     if (pe < 0 || lp != p.nY - 1) {
                         nx = kLapUnknown;
                     } else {
-                        nx = __ldcg(wOrg + (size_t)wv * Kp + kp);
-                        st = 1 + __ldcg(wHop + (size_t)wv * Kp + kp);
+                        nx = ldI<S>(wOrg + (size_t)wv * Kp + kp);
+                        st = 1 + ldI<S>(wHop + (size_t)wv * Kp + kp);
                     }
                 }
                 p.lapNext[i] = nx;
@@ -562,7 +656,7 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             for (long long i = tid; i < n; i += nth) {
                 int st = 0;
                 if (p.branchOf[i] == p.branchId) {
-                    const double d0 = __ldcg(p.dp + (size_t)i * Kp);
+                    const double d0 = ldD<S>(p.dp + (size_t)i * Kp);
                     if (d0 < 0) {
                         int v0 = -1;
                         long long steps = 0;
@@ -620,7 +714,7 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
                     for (int i = 0; i < n; ++i) {
                         const int st = __ldcg(p.candStat + i);
                         if (st == 0) continue;
-                        Key kk{__ldcg(p.dp + (size_t)i * Kp), i};
+                        Key kk{ldD<S>(p.dp + (size_t)i * Kp), i};
                         if (key_less(prev, kk) && key_less(kk, next)) next = kk;
                     }
                     if (next.i == 0x7fffffff) break;
@@ -717,28 +811,47 @@ __global__ void lookup_pairs_kernel(LookupArgs a) {
 }
 
 // Host-side launch helpers -------------------------------------------------
-cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
-                      cudaStream_t stream) {
-    void* args[] = {(void*)&p};
-    void* fn = nullptr;
-    if (costIsF32) {
-        if (timeKind == 0) fn = (void*)bf_kernel<float, 0>;
-        else if (timeKind == 1) fn = (void*)bf_kernel<float, 1>;
-        else fn = (void*)bf_kernel<float, 2>;
-    } else {
-        if (timeKind == 0) fn = (void*)bf_kernel<double, 0>;
-        else if (timeKind == 1) fn = (void*)bf_kernel<double, 1>;
-        else fn = (void*)bf_kernel<double, 2>;
+static const void* bf_fn(int costIsF32, int timeKind, bool sharedTables) {
+    if (sharedTables) {
+        if (costIsF32)
+            return timeKind == 0 ? (const void*)bf_kernel<float, 0, true>
+                                 : timeKind == 1 ? (const void*)bf_kernel<float, 1, true>
+                                                 : (const void*)bf_kernel<float, 2, true>;
+        return timeKind == 0 ? (const void*)bf_kernel<double, 0, true>
+                             : timeKind == 1 ? (const void*)bf_kernel<double, 1, true>
+                                             : (const void*)bf_kernel<double, 2, true>;
     }
-    if (cooperative) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, 0, stream);
-    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, 0, stream);
+    if (costIsF32)
+        return timeKind == 0 ? (const void*)bf_kernel<float, 0, false>
+                             : timeKind == 1 ? (const void*)bf_kernel<float, 1, false>
+                                             : (const void*)bf_kernel<float, 2, false>;
+    return timeKind == 0 ? (const void*)bf_kernel<double, 0, false>
+                         : timeKind == 1 ? (const void*)bf_kernel<double, 1, false>
+                                         : (const void*)bf_kernel<double, 2, false>;
+}
+
+// Bytes of shared memory a single-CTA launch needs to keep the distance,
+// backup, origin and hop tables on chip.
+size_t bf_shared_table_bytes(int n, int Kp) {
+    return (size_t)n * Kp * 2 * sizeof(double) + (size_t)n * sizeof(double) + (size_t)n * Kp * 4 * sizeof(int);
+}
+
+cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
+                      size_t sharedBytes, cudaStream_t stream) {
+    void* args[] = {(void*)&p};
+    const bool shared = sharedBytes > 0;
+    const void* fn = bf_fn(costIsF32, timeKind, shared);
+    if (shared) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sharedBytes);
+        if (e != cudaSuccess) return e;
+    }
+    if (cooperative) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, sharedBytes, stream);
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, sharedBytes, stream);
 }
 
 cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, int* blocksPerSm) {
-    const void* fn;
-    if (costIsF32) fn = timeKind == 0 ? (const void*)bf_kernel<float, 0> : timeKind == 1 ? (const void*)bf_kernel<float, 1> : (const void*)bf_kernel<float, 2>;
-    else fn = timeKind == 0 ? (const void*)bf_kernel<double, 0> : timeKind == 1 ? (const void*)bf_kernel<double, 1> : (const void*)bf_kernel<double, 2>;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, bf_fn(costIsF32, timeKind, false), threads, 0);
 }
 
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream) {

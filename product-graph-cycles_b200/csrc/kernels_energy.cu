@@ -263,21 +263,59 @@ __device__ __forceinline__ bool entry_valid(const SelectArgs& a, long long idx) 
     return l < a.nY && a.tedgeIntra[pos - a.interEntries] >= 0;
 }
 
+// Histogram of the next digit of the keys that match the current prefix.
+// Costs cluster in a few digit values (equal exponents, repeated integers),
+// so lanes holding the same digit are combined with __match_any_sync before
+// one of them updates the block's shared-memory counter.
 __global__ void select_hist_kernel(SelectArgs a) {
     extern __shared__ unsigned int sh[];
     const int nb = 1 << a.bits;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
     __syncthreads();
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        if (!entry_valid(a, idx)) continue;
-        const unsigned long long k = order_key(a.col[idx]);
-        if ((k & a.prefixMask) != a.prefix) continue;
-        atomicAdd(&sh[(k >> a.shift) & (unsigned long long)(nb - 1)], 1u);
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (long long base = gw * 32; base < a.total; base += warps * 32) {
+        const long long idx = base + lane;
+        unsigned bin = 0xffffffffu;
+        if (idx < a.total && entry_valid(a, idx)) {
+            const unsigned long long k = order_key(a.col[idx]);
+            if ((k & a.prefixMask) == a.prefix) bin = (unsigned)((k >> a.shift) & (unsigned long long)(nb - 1));
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, bin);
+        if (bin != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&sh[bin], (unsigned)__popc(peers));
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x)
         if (sh[i]) atomicAdd(a.hist + i, (unsigned long long)sh[i]);
+}
+
+// Copies the values whose key matches (prefix, prefixMask) to out[0..cap).
+__global__ void select_compact_kernel(SelectArgs a, double* out, unsigned long long* count, long long cap) {
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        if (!entry_valid(a, idx)) continue;
+        const double x = a.col[idx];
+        if ((order_key(x) & a.prefixMask) != a.prefix) continue;
+        const unsigned long long at = atomicAdd(count, 1ull);
+        if ((long long)at < cap) out[at] = x;
+    }
+}
+
+// Smallest key strictly greater than `above` (all bits); *out starts at ~0.
+__global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, unsigned long long* out) {
+    unsigned long long best = ~0ull;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        if (!entry_valid(a, idx)) continue;
+        const unsigned long long k = order_key(a.col[idx]);
+        if (k > above && k < best) best = k;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+        best = x < best ? x : best;
+    }
+    if ((threadIdx.x & 31) == 0 && best != ~0ull) atomicMin(out, best);
 }
 
 // x <- min(round(factor * x), clip), in place on the valid entries; also
@@ -402,6 +440,16 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
 }
 cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
     select_hist_kernel<<<grid_for(a.total, 512), 512, (1 << a.bits) * sizeof(unsigned), s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,
+                                  cudaStream_t s) {
+    select_compact_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a, out, count, cap);
+    return cudaGetLastError();
+}
+cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long above, unsigned long long* out,
+                                    cudaStream_t s) {
+    select_min_above_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a, above, out);
     return cudaGetLastError();
 }
 cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,

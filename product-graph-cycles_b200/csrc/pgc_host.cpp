@@ -19,6 +19,7 @@
 #include <limits>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <set>
 #include <sstream>
 #include <stdexcept>
@@ -48,6 +49,75 @@ struct Failure : std::runtime_error {
             throw Failure(PGC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));             \
     } while (0)
 
+// Process-wide caching allocator for device buffers.  Freed blocks are kept,
+// per device, and handed out again to requests of at least half their size,
+// so that creating and destroying generators (and re-solving graphs of
+// similar size) does not pay cudaMalloc/cudaFree every time.  Every handle
+// synchronises its stream before it returns memory here, so a cached block is
+// never still in use.  pgc_release_cached_memory() returns the cache to CUDA.
+class DevicePool {
+  public:
+    static DevicePool& get() {
+        static DevicePool* pool = new DevicePool();  // never destroyed: outlives all handles
+        return *pool;
+    }
+    void* allocate(size_t bytes) {
+        int dev = 0;
+        PGC_CUDA(cudaGetDevice(&dev));
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            auto& fl = free_[dev];
+            auto it = fl.lower_bound(bytes);
+            if (it != fl.end() && it->first <= 2 * bytes + (1 << 20)) {
+                void* p = it->second;
+                sizes_[p] = it->first;
+                fl.erase(it);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaErrorMemoryAllocation) {
+            (void)cudaGetLastError();
+            release_cached();
+            e = cudaMalloc(&p, bytes);
+        }
+        if (e != cudaSuccess) throw Failure(PGC_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        std::lock_guard<std::mutex> lock(mu_);
+        sizes_[p] = bytes;
+        devOf_[p] = dev;
+        return p;
+    }
+    void deallocate(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lock(mu_);
+        auto it = sizes_.find(p);
+        if (it == sizes_.end()) return;
+        free_[devOf_[p]].emplace(it->second, p);
+        sizes_.erase(it);
+    }
+    void release_cached() {
+        std::lock_guard<std::mutex> lock(mu_);
+        int cur = 0;
+        cudaGetDevice(&cur);
+        for (auto& d : free_) {
+            cudaSetDevice(d.first);
+            for (auto& b : d.second) {
+                cudaFree(b.second);
+                devOf_.erase(b.second);
+            }
+            d.second.clear();
+        }
+        cudaSetDevice(cur);
+    }
+
+  private:
+    std::mutex mu_;
+    std::map<int, std::multimap<size_t, void*>> free_;
+    std::map<void*, size_t> sizes_;
+    std::map<void*, int> devOf_;
+};
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -57,7 +127,7 @@ struct DBuf {
     DBuf& operator=(const DBuf&) = delete;
     ~DBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) DevicePool::get().deallocate(p);
         p = nullptr;
         n = 0;
     }
@@ -65,7 +135,7 @@ struct DBuf {
         if (count <= n && p) return;
         release();
         if (count == 0) count = 1;
-        PGC_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+        p = (T*)DevicePool::get().allocate(count * sizeof(T));
         n = count;
     }
     void upload(const T* src, size_t count, cudaStream_t s) {
@@ -150,7 +220,9 @@ class Graph {
     std::string costName = "vanilla", timeName = "";
 
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // stream all work is issued on
+    cudaStream_t ownStream = nullptr;  // the handle's own stream
+    bool templateReady = false;        // topology uploaded (it never changes)
 
     // generated state
     bool generated = false;
@@ -185,13 +257,16 @@ class Graph {
     Stats stats;
 
     ~Graph() {
-        if (stream) cudaStreamDestroy(stream);
+        // device buffers go back to the caching pool: no work may still use them
+        if (stream) cudaStreamSynchronize(stream);
+        if (ownStream) cudaStreamDestroy(ownStream);
     }
 
     long numNodes() const { return (long)T.n * T.nY; }
 
     // -------------------------------------------------------------------
     void generate();
+    void upload_template();
     void ensure_generated() {
         if (!generated) generate();
     }
@@ -218,6 +293,7 @@ class Graph {
         double tconst;
         int blocks, threads;
         bool coop;
+        size_t sharedBytes;  // > 0: single CTA keeping its tables in shared memory
     };
     Run prepare_run(int K, bool ratio);
     void ensure_workspace(int K, int blocks);
@@ -238,17 +314,13 @@ class Graph {
     void rows_for_edges(const std::vector<long long>& edges);
 };
 
-// ---------------------------------------------------------------------------
-// generate(): product_graph_generators.cpp:21-89
-// ---------------------------------------------------------------------------
-void Graph::generate() {
-    if (conj && !normalsGiven)
-        throw Failure(PGC_ERR_STATE, "cannot generate the conjugate product graph without normals (set_normals)");
+// The product-graph topology depends only on EX, EY and the two graph flags,
+// all fixed at construction; it is built and uploaded once.
+void Graph::upload_template() {
     const std::string err = build_template(EX.data(), nex, EY.data(), ney, nvx, conj, prune, T);
     if (!err.empty()) throw Failure(PGC_ERR_ARG, err);
     for (int64_t i = 0; i < 2 * ney; ++i)
         if (EY[(size_t)i] >= nvy) throw Failure(PGC_ERR_ARG, "EY refers to a vertex outside VY");
-
     cudaStream_t s = stream;
     for (int p = 0; p < 2; ++p) {
         dSp[p].upload(T.sp[p].data(), T.sp[p].size(), s);
@@ -266,6 +338,18 @@ void Graph::generate() {
     dVX.upload(VX.data(), VX.size(), s);
     dVY.upload(VY.data(), VY.size(), s);
     dFD.upload(FD.data(), FD.size(), s);
+    templateReady = true;
+}
+
+// ---------------------------------------------------------------------------
+// generate(): product_graph_generators.cpp:21-89
+// ---------------------------------------------------------------------------
+void Graph::generate() {
+    if (conj && !normalsGiven)
+        throw Failure(PGC_ERR_STATE, "cannot generate the conjugate product graph without normals (set_normals)");
+    cudaStream_t s = stream;
+    if (!templateReady) upload_template();
+    generated = false;
 
     const long long stride = T.layerStride();
     const long long total = (long long)(T.nY + 1) * stride;
@@ -359,57 +443,94 @@ double Graph::median_of_column(int col) {
     const long long total = (long long)(T.nY + 1) * stride;
     const long long count = (long long)T.nY * T.eBlock;
     if (count <= 0) throw Failure(PGC_ERR_STATE, "empty product graph");
-    const int bits = 11;
-    DBuf<unsigned long long> hist;
+    // Order statistics k (and k+1 for an even count) by MSD radix selection on
+    // the order-preserving 64-bit keys: 12-bit digits; as soon as the bucket
+    // holding rank k has at most kCompact members it is copied out and
+    // finished on the host.  If rank k is the largest of its bucket, rank k+1
+    // is the smallest key above the bucket (one reduction pass).
+    const int bits = 12;
+    const long long kCompact = 1 << 16;
+    DBuf<unsigned long long> hist, cnt;
+    DBuf<double> band;
     hist.alloc((size_t)1 << bits);
+    cnt.alloc(1);
     std::vector<unsigned long long> h((size_t)1 << bits);
-    auto select = [&](long long k) -> double {
-        unsigned long long prefix = 0, mask = 0;
-        int shift = 64;
-        long long rank = k;
-        while (shift > 0) {
-            const int b = std::min(bits, shift);
-            shift -= b;
-            SelectArgs a{};
-            a.col = e64[col].p;
-            a.total = total;
-            a.layerStride = stride;
-            a.interEntries = T.entries[INTER];
-            a.nY = T.nY;
-            a.tedgeInter = dTedge[INTER].p;
-            a.tedgeIntra = dTedge[INTRA].p;
-            a.prefix = prefix;
-            a.prefixMask = mask;
-            a.shift = shift;
-            a.bits = b;
-            a.hist = hist.p;
-            PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
-            PGC_CUDA(launch_select_hist(a, stream));
-            stats.launches++;
-            PGC_CUDA(cudaMemcpyAsync(h.data(), hist.p, sizeof(unsigned long long) << b, cudaMemcpyDeviceToHost,
-                                     stream));
-            PGC_CUDA(cudaStreamSynchronize(stream));
-            int digit = 0;
-            long long acc = 0;
-            for (; digit < (1 << b); ++digit) {
-                if (acc + (long long)h[(size_t)digit] > rank) break;
-                acc += (long long)h[(size_t)digit];
-            }
-            if (digit >= (1 << b)) throw Failure(PGC_ERR_INTERNAL, "median selection lost its rank");
-            rank -= acc;
-            prefix |= (unsigned long long)digit << shift;
-            mask |= (((unsigned long long)1 << b) - 1) << shift;
-        }
-        const unsigned long long u = (prefix >> 63) ? (prefix & 0x7fffffffffffffffULL) : ~prefix;
+    SelectArgs a{};
+    a.col = e64[col].p;
+    a.total = total;
+    a.layerStride = stride;
+    a.interEntries = T.entries[INTER];
+    a.nY = T.nY;
+    a.tedgeInter = dTedge[INTER].p;
+    a.tedgeIntra = dTedge[INTRA].p;
+    a.hist = hist.p;
+    auto key_to_double = [](unsigned long long key) {
+        const unsigned long long u = (key >> 63) ? (key & 0x7fffffffffffffffULL) : ~key;
         double x;
         std::memcpy(&x, &u, sizeof(x));
         return x;
     };
-    if (count % 2 == 0) {
-        const double a = select((count - 2) / 2), b = select((count - 2) / 2 + 1);
-        return (a + b) / 2.0;
+    const bool even = count % 2 == 0;
+    const long long k = even ? (count - 2) / 2 : count / 2;
+    unsigned long long prefix = 0, mask = 0;
+    int shift = 64;
+    long long rank = k, bucket = count;
+    while (shift > 0 && bucket > kCompact) {
+        const int b = std::min(bits, shift);
+        shift -= b;
+        a.prefix = prefix;
+        a.prefixMask = mask;
+        a.shift = shift;
+        a.bits = b;
+        PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
+        PGC_CUDA(launch_select_hist(a, stream));
+        stats.launches++;
+        PGC_CUDA(cudaMemcpyAsync(h.data(), hist.p, sizeof(unsigned long long) << b, cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaStreamSynchronize(stream));
+        int digit = 0;
+        long long acc = 0;
+        for (; digit < (1 << b); ++digit) {
+            if (acc + (long long)h[(size_t)digit] > rank) break;
+            acc += (long long)h[(size_t)digit];
+        }
+        if (digit >= (1 << b)) throw Failure(PGC_ERR_INTERNAL, "median selection lost its rank");
+        rank -= acc;
+        bucket = (long long)h[(size_t)digit];
+        prefix |= (unsigned long long)digit << shift;
+        mask |= (((unsigned long long)1 << b) - 1) << shift;
     }
-    return select(count / 2);
+    double xk, xk1 = 0;
+    unsigned long long bucketTop;  // largest key the bucket can hold
+    if (shift == 0) {
+        xk = key_to_double(prefix);  // every member of the bucket equals it
+        if (even && rank + 1 < bucket) xk1 = xk;
+        bucketTop = prefix;
+    } else {
+        band.alloc((size_t)bucket);
+        a.prefix = prefix;
+        a.prefixMask = mask;
+        PGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), stream));
+        PGC_CUDA(launch_select_compact(a, band.p, cnt.p, bucket, stream));
+        stats.launches++;
+        std::vector<double> vals((size_t)bucket);
+        PGC_CUDA(cudaMemcpyAsync(vals.data(), band.p, sizeof(double) * (size_t)bucket, cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaStreamSynchronize(stream));
+        std::sort(vals.begin(), vals.end());
+        xk = vals[(size_t)rank];
+        if (even && rank + 1 < bucket) xk1 = vals[(size_t)rank + 1];
+        bucketTop = prefix | ~mask;
+    }
+    if (!even) return xk;
+    if (rank + 1 >= bucket) {
+        unsigned long long best = ~0ull;
+        PGC_CUDA(cudaMemcpyAsync(cnt.p, &best, sizeof(best), cudaMemcpyHostToDevice, stream));
+        PGC_CUDA(launch_select_min_above(a, bucketTop, cnt.p, stream));
+        stats.launches++;
+        PGC_CUDA(cudaMemcpyAsync(&best, cnt.p, sizeof(best), cudaMemcpyDeviceToHost, stream));
+        PGC_CUDA(cudaStreamSynchronize(stream));
+        xk1 = key_to_double(best);
+    }
+    return (xk + xk1) / 2.0;
 }
 
 void Graph::rescale_column(int col, double scaling) {
@@ -496,6 +617,11 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     }
     r.blocks = blocks;
     r.coop = blocks > 1;
+    r.sharedBytes = 0;
+    if (blocks == 1 && env_int("PGC_BF_SHARED_TABLES", 1)) {
+        const size_t bytes = bf_shared_table_bytes(T.n, r.Kp);
+        if (bytes <= (size_t)env_int("PGC_BF_SHARED_MAX_BYTES", 200 * 1024)) r.sharedBytes = bytes;
+    }
     ensure_workspace(K, blocks);
     return r;
 }
@@ -605,7 +731,7 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     PGC_CUDA(cudaEventCreate(&e0));
     PGC_CUDA(cudaEventCreate(&e1));
     PGC_CUDA(cudaEventRecord(e0, stream));
-    PGC_CUDA(launch_bf(p, r.costF32, r.timeKind, r.blocks, r.threads, r.coop, stream));
+    PGC_CUDA(launch_bf(p, r.costF32, r.timeKind, r.blocks, r.threads, r.coop, r.sharedBytes, stream));
     PGC_CUDA(cudaEventRecord(e1, stream));
     stats.launches++;
     PGC_CUDA(cudaMemcpyAsync(&c, wCtl.p, sizeof(Control), cudaMemcpyDeviceToHost, stream));
@@ -1241,7 +1367,8 @@ int pgc_create(const double* VX, int64_t nvx, const int32_t* EX, int64_t nex, co
         g.reg = use_regularising_cost_term != 0;
         g.prune = prune_intralayer != 0;
         PGC_CUDA(cudaGetDevice(&g.device));
-        PGC_CUDA(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        PGC_CUDA(cudaStreamCreateWithFlags(&g.ownStream, cudaStreamNonBlocking));
+        g.stream = g.ownStream;
         *out = h.release();
     });
 }
@@ -1283,6 +1410,14 @@ int pgc_update_robust_loss_params(pgc_graph* h, double alpha, double c, double p
         g.rlAlpha = alpha;
         g.rlC = c;
         g.rlPwr = pwr;
+    });
+}
+
+int pgc_set_stream(pgc_graph* h, void* cuda_stream) {
+    return guarded([&] {
+        Graph& g = h->g;
+        PGC_CUDA(cudaStreamSynchronize(g.stream));
+        g.stream = cuda_stream ? (cudaStream_t)cuda_stream : g.ownStream;
     });
 }
 
@@ -1490,6 +1625,28 @@ int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_
                 for (int k = 0; k < 3; ++k) out[3 * i + k] /= len;
         }
     });
+}
+
+int pgc_graph_info(pgc_graph* h, int64_t* out8) {
+    return guarded([&] {
+        Graph& g = h->g;
+        PGC_CUDA(cudaSetDevice(g.device));
+        g.ensure_generated();
+        int64_t inter = 0, intra = 0;
+        for (int64_t t = 0; t < g.T.eBlock; ++t) (g.T.eNext[(size_t)t] ? inter : intra) += 1;
+        out8[0] = g.T.n;
+        out8[1] = g.T.nY;
+        out8[2] = g.T.eBlock;
+        out8[3] = inter;
+        out8[4] = intra;
+        out8[5] = g.T.entries[pgc::INTER];
+        out8[6] = g.T.entries[pgc::INTRA];
+        out8[7] = g.ncols;
+    });
+}
+
+int pgc_release_cached_memory(void) {
+    return guarded([&] { pgc::DevicePool::get().release_cached(); });
 }
 
 const char* pgc_last_error(void) { return pgc::g_lastError.c_str(); }

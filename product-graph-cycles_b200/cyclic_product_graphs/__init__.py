@@ -58,6 +58,8 @@ _lib.pgc_result_cycle_edges.argtypes = [_h, _lp, _i64, _lp]
 _lib.pgc_result_stats.argtypes = [_h, _lp]
 _lib.pgc_compute_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
 _lib.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
+_lib.pgc_graph_info.argtypes = [_h, _lp]
+_lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
 _lib.pgc_last_error.restype = ctypes.c_char_p
 _lib.pgc_version.restype = ctypes.c_char_p
 
@@ -186,6 +188,18 @@ class product_graph_generator:
         out = np.empty(cnt.value, dtype=np.int64)
         _check(_lib.pgc_result_cycle_edges(self._h, out.ctypes.data_as(_lp), cnt.value, ctypes.byref(cnt)))
         return out
+
+    def graph_info(self) -> dict:
+        """Sizes of the generated product graph (generates it if needed)."""
+        buf = (ctypes.c_int64 * 8)()
+        _check(_lib.pgc_graph_info(self._h, buf))
+        keys = ["nodes_per_layer", "layers", "edges_per_block", "inter_edges_per_layer", "intra_edges_per_layer",
+                "inter_slots_per_layer", "intra_slots_per_layer", "cost_columns"]
+        return dict(zip(keys, list(buf)))
+
+    def set_stream(self, cuda_stream: int | None):
+        """Issue all device work of this generator on `cuda_stream` (a cudaStream_t as int)."""
+        _check(_lib.pgc_set_stream(self._h, ctypes.c_void_p(cuda_stream) if cuda_stream else None))
 
     def last_stats(self) -> dict:
         buf = (ctypes.c_int64 * 8)()

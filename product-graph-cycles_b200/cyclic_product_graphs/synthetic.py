@@ -193,5 +193,8 @@ def make_pair(n_vertices: int = 642, n_curve: int = 60, feat_dim: int = 32, seed
                feat_diff=np.ascontiguousarray(fd), F=F, fX=fX, fY=fY, nearest=nearest)
     if with_normals:
         out["NX"] = vertex_normals(VX, F)
-        out["NY"] = normals_2d(VY, EY)
+        # normals_2d picks the plane by the first coordinate column whose sum is
+        # ~0; a curve around the origin would be misread, so detect the plane
+        # on a translated copy (edge vectors, hence normals, are unchanged)
+        out["NY"] = normals_2d(VY + np.array([10.0, 10.0, 0.0]), EY)
     return out
