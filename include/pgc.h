@@ -109,6 +109,14 @@ int pgc_result_cycle_edges(pgc_graph* g, int64_t* out, int64_t capacity, int64_t
  * branches, fallback_walks, device_ms_x1000, kernel_launches]. */
 int pgc_result_stats(pgc_graph* g, int64_t* out8);
 
+/* Profile of the last solve's Bellman-Ford launches (no reference
+ * counterpart).  SM cycles seen by one thread of the first CTA:
+ * [0] relaxation, [1] sweep bookkeeping, [2] step hand-offs and barriers,
+ * [3] sweep tail (wrap-around and cycle detection); [4] (layer, depth) steps
+ * run; team shape of the last launch: [5] CTAs, [6] threads per CTA,
+ * [7] wait-list entries over all CTAs. */
+int pgc_result_profile(pgc_graph* g, int64_t* out8);
+
 /* utils::normals2d (helper/utils.cpp:93-157, bindings.cpp:27): outward
  * vertex normals of an ordered closed curve lying in a coordinate plane.
  * V [nv x 3], E [ne x 2] with ne == nv; out [nv x 3]. */

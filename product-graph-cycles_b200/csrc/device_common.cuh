@@ -21,6 +21,7 @@ enum BfStatus : int {
     BF_ERR_BARRIER = -2,     // a grid barrier wait ran out of iterations
     BF_ERR_CYCLE_CAP = -3,   // the extracted cycle does not fit its buffer
     BF_ERR_WALK = -4,        // a predecessor walk left the valid index range
+    BF_ERR_CHUNK = -5,       // a slice has more in-edge entries than the scratch holds
 };
 
 // Lap-successor codes (see bf kernel): P[v] >= 0 is the next layer-0 node.
@@ -43,7 +44,10 @@ struct Control {
     long long candidates;  // candidates decided (for statistics)
     unsigned barCount;
     unsigned barGen;
-    int pad[6];
+    int pad[2];
+    // SM cycles seen by CTA 0's thread 0 (profiling counters): relaxation,
+    // sweep bookkeeping, step hand-offs / barriers, sweep tail
+    unsigned long long cycPhaseA, cycPhaseB, cycSync, cycTail;
     // minimum-cost outputs
     double firstLb;
     int firstV;
@@ -51,6 +55,15 @@ struct Control {
     double validLb;
     int validV;
     int anyFinite;
+};
+
+// One (node, depth) entry of a layer's DP rows: the path value and, for the
+// stored path, its origin (the layer-0 start node it leaves from, or a
+// kLap* code) and its length in predecessor steps back to that origin.
+struct __align__(16) DPE {
+    double v;
+    int o;
+    int h;
 };
 
 struct BfParams {
@@ -67,18 +80,23 @@ struct BfParams {
     const void* time;              // same layout, or nullptr for a constant time
     double tconst;
     // state
-    double* dp;                    // [2][n][Kp]
+    DPE* dp;                       // [2][n][Kp] distance + origin of every (node, depth) of two layers
     double* bak;                   // [n]
     int* pred;                     // [(nY+1)*K*n], expanded index layer*n*K + k*n + v
-    int* org;                      // [2][n][Kp] origin (layer-0 start node) of the stored path
-    int* hops;                     // [2][n][Kp] predecessor steps back to that origin
+    const int* ctaSlice;           // [ncta+1] slice range of every CTA (both parts)
+    const int* waitPtr;            // [ncta+1] CSR offsets into waitIdx
+    const int* waitIdx;            // CTAs a CTA hands steps off with (its graph neighbours)
+    unsigned* stepDone;            // [ncta * kStepDoneStride] last step each CTA completed
+    int flagSync;                  // 1: neighbour hand-offs between steps, 0: team barrier
+    int maxCtaSlices;              // most slices any CTA owns
+    int rowCap;                    // rows (of 32 entries) one step buffer holds
     int* lapNext;                  // [n]
     int* lapSteps;                 // [n]
     int* mark;                     // [n] visited marks for literal walks
     int* candStat;                 // [n] shortcut verdict per candidate (0 none, 1 cycle, 2 no cycle, 3 undecided)
     int* candV0;                   // [n] first repeated layer-0 node of a candidate's walk
     long long* candSteps;          // [n] predecessor steps that walk needs
-    int* layerFlag;                // [nY+1] epoch of the last sweep that improved the layer
+    int* layerFlag;                // [nY+1] stamp of the last sweep that improved the layer
     const int* branchOf;
     int branchId;
     double lambda, ub;
@@ -170,10 +188,27 @@ struct LookupArgs {
     double* tOut;
 };
 
-size_t bf_shared_table_bytes(int n, int Kp);
+constexpr int kStepDoneStride = 8;  // one 32-byte sector per CTA step counter
+// Most threads per Bellman-Ford CTA: 20 warps fit the kernel's registers
+// (about 100 per thread) on one SM without spilling the relaxation loop.
+constexpr int kBfThreads = 640;
+// Bytes of shared memory a single-CTA launch needs to keep its DP records
+// and backup row on chip (128-byte aligned).
+__host__ __device__ inline size_t bf_shared_table_bytes(int n, int Kp) {
+    const size_t b = (size_t)2 * n * Kp * sizeof(DPE) + (size_t)n * sizeof(double);
+    return (b + 127) & ~(size_t)127;
+}
+// Offset of the first step buffer after the staged row offsets (128-byte aligned).
+__host__ __device__ inline size_t bf_stage_offset(int maxCtaSlices) {
+    return ((size_t)2 * (maxCtaSlices + 1) * sizeof(int) + 127) & ~(size_t)127;
+}
+// Bytes of one step buffer: source index, cost and time of rowCap rows.
+__host__ __device__ inline size_t bf_stage_buffer_bytes(int rowCap, int costBytes, int timeBytes) {
+    return (size_t)rowCap * 32 * (4 + costBytes + timeBytes);
+}
 cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
-                      size_t sharedBytes, cudaStream_t stream);
-cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, int* blocksPerSm);
+                      bool sharedTables, size_t smemBytes, cudaStream_t stream);
+cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);

@@ -3,7 +3,7 @@
 // One launch runs one Bellman-Ford call of the reference
 // (mooreBellmanFordSubroutineCPU, cost_time_ratio_solver.cpp:251-542, and
 // dijkstra_solver.cpp:203-388) from its set-up to its verdict, so the host
-// only sees one launch per call instead of one per (layer, depth).
+// sees one launch per call instead of one per (layer, depth).
 //
 // Semantics kept exactly (the result must equal the reference's):
 //  * the DP table keeps the reference's row layout: layer l writes parity
@@ -17,12 +17,20 @@
 //  * predecessors are written only on improvement, so stale entries evolve as
 //    in the reference.
 //
+// Work split of one (layer, depth) step: every CTA owns a range of node
+// slices (32 nodes each) balanced by in-edge entries.  Phase A: the CTA's
+// threads take the in-edge entries of a chunk of slices independently --
+// source index, cost and time, then the source's DP record -- and leave each
+// entry's best candidate in shared memory, so a whole chunk costs two memory
+// latencies however large the in-degree.  Phase B: one thread per node folds
+// its entries in edge order (the reference's tie-break) and writes the node.
+//
 // Cycle detection: the reference walks predecessors from every negative
 // start node in ascending order of its value until a start node repeats.
-// Here each stored path also carries its origin (the layer-0 start node it
-// leaves from) and its length in predecessor steps, so one "lap" of the walk
-// (layer-0 node -> next layer-0 node) is a table lookup.  Each candidate is
-// decided with Brent's cycle-finding algorithm on that lap function; the
+// Here each DP record also carries its path's origin (the layer-0 start node
+// it leaves from) and its length in predecessor steps, so one "lap" of the
+// walk (layer-0 node -> next layer-0 node) is a table lookup.  Each candidate
+// is decided with Brent's cycle-finding algorithm on that lap function; the
 // candidate with the smallest (value, index) whose walk repeats within the
 // reference's step limit wins.  When a lap cannot be derived from the
 // current sweep (a stale predecessor), that candidate is re-walked literally.
@@ -36,15 +44,13 @@ namespace pgc {
 
 namespace {
 
-constexpr unsigned kSpinLimit = 1u << 24;  // ~2 s of polling with 100 ns sleeps
+constexpr unsigned kSpinLimit = 1u << 24;  // ~2 s of polling at most
 
 struct Team {
     int cta, ncta;
     unsigned* cnt;
     unsigned* gen;
     int* err;
-    __device__ int warp() const { return cta * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5); }
-    __device__ int nwarps() const { return ncta * (int)(blockDim.x >> 5); }
     __device__ long long thread() const { return (long long)cta * blockDim.x + threadIdx.x; }
     __device__ long long nthreads() const { return (long long)ncta * blockDim.x; }
 };
@@ -54,53 +60,65 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-
 __device__ __forceinline__ unsigned atom_add_acq_rel_u32(unsigned* p, unsigned v) {
     unsigned old;
     asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
 }
-__device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Team barrier.  One CTA: __syncthreads.  Several CTAs (cooperative launch,
-// all resident): after the CTA-wide barrier, thread 0 arrives on a global
-// counter with release semantics (cumulative over the CTA's writes); the last
-// arrival resets the counter and bumps the generation word with release
-// semantics; the others poll the generation with acquire loads, spinning
-// briefly and then backing off, for a bounded number of iterations after
-// which the error word is raised.  Returns false when the team must stop.
-__device__ bool team_sync(const Team& t) {
-    __shared__ int s_stop;
-    __syncthreads();
+// Team barrier that also ORs one flag over the team.  One CTA:
+// __syncthreads_or.  Several CTAs (cooperative launch, all resident): after
+// the CTA-wide barrier, thread 0 adds 1 (+ 1 << 16 if its CTA's flag is set)
+// to a global counter with acquire-release semantics (cumulative over the
+// CTA's writes).  The last arrival resets the counter and publishes the next
+// generation with the team's flag in bit 0 (release store); the others poll
+// the generation with acquire loads -- briefly spinning, then backing off --
+// for a bounded number of iterations.  A CTA whose wait runs out raises the
+// error word and gets ok = false; every other waiter checks the error word
+// while polling and gives up too, so every CTA ends within a bounded time.
+__device__ int team_sync_or(const Team& t, int flag, bool& ok) {
+    __shared__ int s_flag, s_ok;
+    const int any = __syncthreads_or(flag);
     if (threadIdx.x == 0) {
+        int res = any, good = 1;
         if (t.ncta > 1) {
             const unsigned g = ld_acquire_u32(t.gen);
-            const unsigned arrived = atom_add_acq_rel_u32(t.cnt, 1u);
-            if (arrived == (unsigned)t.ncta - 1) {
+            const unsigned add = 1u + (any ? (1u << 16) : 0u);
+            const unsigned old = atom_add_acq_rel_u32(t.cnt, add);
+            if ((old & 0xffffu) == (unsigned)t.ncta - 1) {
+                res = ((old + add) >> 16) != 0;
                 atomicExch(t.cnt, 0u);
-                red_add_release_u32(t.gen, 1u);
+                st_release_u32(t.gen, (((g >> 1) + 1) << 1) | (unsigned)res);
             } else {
-                unsigned spins = 0;
-                while (ld_acquire_u32(t.gen) == g) {
-                    if (++spins > kSpinLimit) {
+                unsigned spins = 0, cur;
+                while ((cur = ld_acquire_u32(t.gen)) == g) {
+                    ++spins;
+                    if (spins > kSpinLimit || ((spins & 63u) == 0 && *(volatile int*)t.err)) {
                         atomicExch(t.err, 1);
+                        good = 0;
                         break;
                     }
                     if (spins > 4096) __nanosleep(64);
                 }
+                res = (int)(cur & 1u);
             }
         }
-        s_stop = *(volatile int*)t.err;
+        s_flag = res;
+        s_ok = good;
     }
     __syncthreads();
-    return s_stop == 0;
+    ok = s_ok != 0;
+    return s_flag;
 }
 
-template <class T>
-__device__ __forceinline__ double ld_stream(const T* p) {
-    return (double)__ldg(p);
+__device__ __forceinline__ bool team_sync(const Team& t) {
+    bool ok;
+    team_sync_or(t, 0, ok);
+    return ok;
 }
 
 // Lexicographic (value, index) key.
@@ -151,178 +169,339 @@ __device__ __forceinline__ int original_index(int n, int K, int e) {
     return rem - depth * n + layer * n;
 }
 
-// Loads of the distance / origin tables: from shared memory when the whole
-// team is one CTA that keeps them there (S), else through L2 (other CTAs
-// write them during the launch, so L1 must not serve stale lines).
+// DP record loads: from shared memory when the whole team is one CTA that
+// keeps its tables there (S), else through L2 (other CTAs write the records
+// during the launch, so L1 must not serve stale lines).
 template <bool S>
-__device__ __forceinline__ double ldD(const double* p) {
-    if constexpr (S) return *p;
-    else return __ldcg(p);
+__device__ __forceinline__ DPE ldE(const DPE* p) {
+    double2 x;
+    if constexpr (S) x = *reinterpret_cast<const double2*>(p);
+    else x = __ldcg(reinterpret_cast<const double2*>(p));
+    DPE e;
+    e.v = x.x;
+    const long long b = __double_as_longlong(x.y);
+    e.o = (int)(unsigned)(b & 0xffffffffLL);
+    e.h = (int)(b >> 32);
+    return e;
 }
 template <bool S>
-__device__ __forceinline__ double2 ldD2(const double* p) {
-    if constexpr (S) return *reinterpret_cast<const double2*>(p);
-    else return __ldcg(reinterpret_cast<const double2*>(p));
+__device__ __forceinline__ double ldV(const DPE* p) {
+    if constexpr (S) return p->v;
+    else return __ldcg(&p->v);
 }
-template <bool S>
-__device__ __forceinline__ int ldI(const int* p) {
-    if constexpr (S) return *p;
-    else return __ldcg(p);
+__device__ __forceinline__ void stE(DPE* p, double v, int o, int h) {
+    double2 x;
+    x.x = v;
+    x.y = __longlong_as_double(((long long)h << 32) | (long long)(unsigned)o);
+    *reinterpret_cast<double2*>(p) = x;
 }
 
 // ---------------------------------------------------------------------------
-// One (layer, depth) step of the sweep.
+// Step staging.  The in-edge streams a CTA reads in one step -- source
+// indices, costs and times of the rows of its slices -- are contiguous and do
+// not depend on the DP values, so the CTA copies the next step's streams
+// into shared memory with bulk asynchronous copies (TMA, no multicast) while
+// the current step runs and hands off.  Two buffers alternate; each has an
+// mbarrier that completes when its copies have landed.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// One bounded wait for the phase with the given parity; true when it completed.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    for (unsigned spins = 0; spins < kSpinLimit; ++spins) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, P;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// Global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Shared-memory state of a CTA: its slices' row offsets per part (staged
+// once per launch) and the two step buffers.
+struct Stage {
+    const int* splInter;         // sp[s0 + i] of the interlayer part, i = 0..s1-s0
+    const int* splIntra;         // same for the intralayer part
+    char* buf0;
+    char* buf1;
+    unsigned long long* bar;     // [2]
+    int rowCap;                  // rows one buffer holds
+    unsigned phase;              // bit b: parity of buffer b's next completion
+    unsigned pending;            // bit b: copies issued into buffer b, not yet waited for
+    int costBytes, timeBytes;    // bytes per entry of the cost and time streams
+    __device__ const int* spl(int part) const { return part ? splIntra : splInter; }
+    __device__ char* buf(int b) const { return b ? buf1 : buf0; }
+};
+
+struct StepRef {
+    int l, k;
+};
+__device__ __forceinline__ bool step_empty(const BfParams& p, int l, int k) { return l == p.nY && k > 0; }
+
+// Stage step (l, k) into buffer b.  Every thread keeps the same bookkeeping;
+// thread 0 issues the copies.
+__device__ void stage_issue(const BfParams& p, Stage& st, int s0, int s1, int b, int l, int k) {
+    if (st.rowCap == 0 || step_empty(p, l, k)) return;
+    const int* spl = st.spl(k == 0 ? 0 : 1);
+    const int r0 = spl[0], r1 = spl[s1 - s0];
+    if (r1 <= r0) return;
+    st.pending |= 1u << b;
+    if (threadIdx.x != 0) return;
+    const size_t e0 = (size_t)r0 * 32, cnt = (size_t)(r1 - r0) * 32;
+    const int* src = k == 0 ? (l == p.nY ? p.srcDummy : p.srcInter) : p.srcIntra;
+    const size_t base = (size_t)l * (size_t)p.layerStride + (k == 0 ? 0 : (size_t)p.interEntries);
+    char* dst = st.buf(b);
+    const unsigned bs = (unsigned)(cnt * 4), bc = (unsigned)(cnt * st.costBytes), bt = (unsigned)(cnt * st.timeBytes);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(st.bar + b, bs + bc + bt);
+    bulk_load(dst, src + e0, bs, st.bar + b);
+    bulk_load(dst + (size_t)st.rowCap * 32 * 4, (const char*)p.cost + (base + e0) * st.costBytes, bc, st.bar + b);
+    if (bt)
+        bulk_load(dst + (size_t)st.rowCap * 32 * (4 + st.costBytes), (const char*)p.time + (base + e0) * st.timeBytes,
+                  bt, st.bar + b);
+}
+
+// Wait for buffer b if copies were issued into it (every thread).
+__device__ __forceinline__ bool stage_wait(Stage& st, int b) {
+    if (!((st.pending >> b) & 1u)) return true;
+    const bool ok = mbar_wait(st.bar + b, (st.phase >> b) & 1u);
+    st.phase ^= 1u << b;
+    st.pending &= ~(1u << b);
+    return ok;
+}
+
+// Before the CTA exits: no copy may still be writing its shared memory.
+__device__ __forceinline__ void stage_drain(Stage& st) {
+    stage_wait(st, 0);
+    stage_wait(st, 1);
+}
+
+// ---------------------------------------------------------------------------
+// One (layer, depth) step of the sweep over the CTA's slices [s0, s1), with
+// the step's streams staged in buffer `sb`.
 //
-// A warp owns a slice of 32 target nodes (lane = node).  The in-edges of the
-// slice are consumed in batches of kBatch slots: first every source index,
-// cost and time of the batch is loaded (independent, coalesced 128-byte
-// loads), then every source distance (one 16/32-byte vector gather per
-// source row), then the batch is folded into the running minimum in edge
-// order, so one batch costs about two memory latencies instead of two per
-// edge.
+// A warp owns a slice of 32 target nodes (lane = node).  The slice's in-edge
+// rows are visited in the reference's order -- ascending edge, then source
+// depth -- in batches of kGather / NK rows (NK source depths per edge, a
+// compile-time constant of the step kind): first every source value of the
+// batch is gathered (independent loads), then the batch is folded into the
+// running first minimum, so a batch costs one memory latency.  The fold keeps
+// thr = min(best, upper bound): a candidate is taken iff cand < thr, which
+// is the reference's (cand < best && cand < ub); an unreached source
+// (+inf) can never pass it.  The winner's origin and path length are read
+// once per node after the fold.  Returns whether this thread improved a node.
 // ---------------------------------------------------------------------------
-constexpr int kBatch = 4;
+constexpr int kGather = 12;
 
-template <class CT, int TK, bool S>
-__device__ void relax_step(const BfParams& p, const Team& t, int l, int k, int epoch) {
-    const int n = p.n, K = p.K, Kp = p.Kp;
-    const int par = l & 1;
-    double* cur = p.dp + (size_t)par * n * Kp;
-    const double* prv = p.dp + (size_t)(par ^ 1) * n * Kp;
-    int* corg = p.org + (size_t)par * n * Kp;
-    int* chop = p.hops + (size_t)par * n * Kp;
-    const int* porg = p.org + (size_t)(par ^ 1) * n * Kp;
-    const int* phop = p.hops + (size_t)(par ^ 1) * n * Kp;
-    const bool inter = (k == 0);
-    const bool empty = (l == p.nY && k > 0);  // the closing layer has no intralayer edges
-    const int* sp = inter ? p.spInter : p.spIntra;
-    const int* src = inter ? (l == p.nY ? p.srcDummy : p.srcInter) : p.srcIntra;
-    const size_t base = (size_t)l * (size_t)p.layerStride + (inter ? 0 : (size_t)p.interEntries);
-    const CT* cst = (const CT*)p.cost + base;
-    const float* tstF = (TK == 1) ? (const float*)p.time + base : nullptr;
-    const double* tstD = (TK == 2) ? (const double*)p.time + base : nullptr;
-    int* predRow = p.pred + (size_t)l * n * K + (size_t)k * n;
-    const int srcLayer = inter ? l - 1 : l;
-    const int nk = inter ? K : 1;            // source depths per edge
-    const int kofs = inter ? 0 : k - 1;      // first source depth
-    const double* srow = inter ? prv : cur;  // source rows
-    const int lane = threadIdx.x & 31;
-    const double lam = p.lambda, ub = p.ub;
-    bool any = false;
-    for (int s = t.warp(); s < p.nslices; s += t.nwarps()) {
-        const int v = s * 32 + lane;
-        const bool valid = v < n;
-        double best = kInfD;
-        if (l == 0 && valid) best = ldD<S>(cur + (size_t)v * Kp + k);
-        int bs = -1, bk = -1;
-        if (!empty) {
-            const int j0 = __ldg(sp + s), j1 = __ldg(sp + s + 1);
-            if (nk <= 4) {
-                for (int jb = j0; jb < j1; jb += kBatch) {
-                    int sv[kBatch];
-                    double cv[kBatch], tv[kBatch];
+struct StepView {
+    const int* src;     // source index per entry, from the step's first row
+    const void* cost;
+    const char* time;
+    const DPE* srow;    // DP records of the source layer
+    int Kp, kofs, nk;
+    double lam, tconst;
+};
+
+template <class CT, int TK>
+__device__ __forceinline__ double edge_weight(const StepView& v, int q) {
+    double t = v.tconst;
+    if (TK == 1) t = (double)reinterpret_cast<const float*>(v.time)[q];
+    else if (TK == 2) t = reinterpret_cast<const double*>(v.time)[q];
+    return __dsub_rn((double)reinterpret_cast<const CT*>(v.cost)[q], __dmul_rn(v.lam, t));
+}
+
+// Rows [row, j1) of one slice for lane `lane`; NK > 0 source depths per edge
+// known at compile time, NK == 0: v.nk depths, one gather at a time.
+template <class CT, int TK, bool S, int NK>
+__device__ __forceinline__ void fold_rows(const StepView& v, int lane, int row, int j1, double& best, double& thr,
+                                          int& bs, int& bk) {
+    if constexpr (NK > 0) {
+        constexpr int RB = kGather / NK > 0 ? kGather / NK : 1;
+        for (; row < j1; row += RB) {
+            int sv[RB];
+            double d[RB][NK];
 #pragma unroll
-                    for (int u = 0; u < kBatch; ++u) {
-                        sv[u] = -1;
-                        cv[u] = 0.0;
-                        tv[u] = p.tconst;
-                        if (jb + u < j1) {
-                            const size_t e = (size_t)(jb + u) * 32 + lane;
-                            sv[u] = __ldg(src + e);
-                            cv[u] = ld_stream(cst + e);
-                            if (TK == 1) tv[u] = (double)__ldg(tstF + e);
-                            else if (TK == 2) tv[u] = __ldg(tstD + e);
-                        }
-                    }
-                    double d[kBatch][4];
+            for (int r = 0; r < RB; ++r) {
+                sv[r] = row + r < j1 ? v.src[(row + r) * 32 + lane] : -1;
+                const DPE* rec = v.srow + (size_t)(sv[r] < 0 ? 0 : sv[r]) * v.Kp + v.kofs;
 #pragma unroll
-                    for (int u = 0; u < kBatch; ++u) {
-                        d[u][0] = d[u][1] = d[u][2] = d[u][3] = kInfD;
-                        if (sv[u] >= 0) {
-                            const double* r = srow + (size_t)sv[u] * Kp + kofs;
-                            if (nk == 1) {
-                                d[u][0] = ldD<S>(r);
-                            } else {
-                                const double2 a = ldD2<S>(r);
-                                d[u][0] = a.x;
-                                d[u][1] = a.y;
-                                if (nk > 2) {
-                                    const double2 b = ldD2<S>(r + 2);
-                                    d[u][2] = b.x;
-                                    d[u][3] = b.y;
-                                }
-                            }
-                        }
-                    }
+                for (int kk = 0; kk < NK; ++kk) d[r][kk] = sv[r] >= 0 ? ldV<S>(rec + kk) : kInfD;
+            }
 #pragma unroll
-                    for (int u = 0; u < kBatch; ++u) {
-                        if (sv[u] < 0) continue;
-                        const double w = __dsub_rn(cv[u], __dmul_rn(lam, tv[u]));
+            for (int r = 0; r < RB; ++r) {
+                if (sv[r] < 0) continue;
+                const double w = edge_weight<CT, TK>(v, (row + r) * 32 + lane);
 #pragma unroll
-                        for (int kk = 0; kk < 4; ++kk) {
-                            if (kk >= nk || isinf(d[u][kk])) continue;
-                            const double cand = __dadd_rn(d[u][kk], w);
-                            if (cand < best && cand < ub) { best = cand; bs = sv[u]; bk = kofs + kk; }
-                        }
-                    }
-                }
-            } else {
-                for (int j = j0; j < j1; ++j) {
-                    const size_t e = (size_t)j * 32 + lane;
-                    const int sv = __ldg(src + e);
-                    if (sv < 0) continue;
-                    const double c = ld_stream(cst + e);
-                    double tt;
-                    if (TK == 0) tt = p.tconst;
-                    else if (TK == 1) tt = (double)__ldg(tstF + e);
-                    else tt = __ldg(tstD + e);
-                    const double w = __dsub_rn(c, __dmul_rn(lam, tt));
-                    const double* row = srow + (size_t)sv * Kp + kofs;
-                    for (int kk = 0; kk < nk; ++kk) {
-                        const double dd = ldD<S>(row + kk);
-                        if (isinf(dd)) continue;
-                        const double cand = __dadd_rn(dd, w);
-                        if (cand < best && cand < ub) { best = cand; bs = sv; bk = kofs + kk; }
-                    }
+                for (int kk = 0; kk < NK; ++kk) {
+                    const double cand = __dadd_rn(d[r][kk], w);
+                    if (cand < thr) { best = cand; thr = cand; bs = sv[r]; bk = v.kofs + kk; }
                 }
             }
         }
-        if (valid) {
-            cur[(size_t)v * Kp + k] = best;
-            int o = kLapUnknown, h = 0;
-            int ps = -1, pk = -1;  // source (node, depth) of the stored predecessor
-            if (bs >= 0) {
-                predRow[v] = bs + srcLayer * n * K + bk * n;
-                any = true;
-                ps = bs;
-                pk = bk;
-            } else if (l == 0) {
-                // Layer 0 keeps an older value and its older predecessor.
-                const int pe = __ldcg(predRow + v);
-                if (pe < 0) {
-                    o = kLapEnd;
-                } else {
-                    ps = pe - (k - 1) * n;
-                    pk = k - 1;
-                    if (ps < 0 || ps >= n) { ps = -1; o = kLapUnknown; }
-                }
+    } else {
+        for (; row < j1; ++row) {
+            const int sv = v.src[row * 32 + lane];
+            if (sv < 0) continue;
+            const double w = edge_weight<CT, TK>(v, row * 32 + lane);
+            const DPE* rec = v.srow + (size_t)sv * v.Kp + v.kofs;
+            for (int kk = 0; kk < v.nk; ++kk) {
+                const double cand = __dadd_rn(ldV<S>(rec + kk), w);
+                if (cand < thr) { best = cand; thr = cand; bs = sv; bk = v.kofs + kk; }
             }
-            if (ps >= 0) {
-                if (srcLayer == 0 && pk == 0) {
+        }
+    }
+}
+
+template <class CT, int TK, bool S, int NK>
+__device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* spl, int s0, int s1, int l, int k) {
+    const int n = p.n, K = p.K, Kp = p.Kp;
+    DPE* cur = p.dp + (size_t)(l & 1) * n * Kp;
+    const bool empty = step_empty(p, l, k);
+    const int r0 = spl[0];
+    int* predRow = p.pred + (size_t)l * n * K + (size_t)k * n;
+    const int srcLayer = k == 0 ? l - 1 : l;
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const double ub = p.ub;
+    bool any = false;
+    for (int s = s0 + (int)(threadIdx.x >> 5); s < s1; s += nwarps) {
+        const int v = s * 32 + lane;
+        const bool valid = v < n;
+        DPE* me = cur + (size_t)v * Kp + k;
+        double best = (l == 0 && valid) ? ldV<S>(me) : kInfD;
+        double thr = best < ub ? best : ub;
+        int bs = -1, bk = -1;
+        if (!empty) fold_rows<CT, TK, S, NK>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, best, thr, bs, bk);
+        if (!valid) continue;
+        int o = kLapUnknown, h = 0;
+        if (bs >= 0) {
+            predRow[v] = bs + srcLayer * n * K + bk * n;
+            any = true;
+            if (srcLayer == 0 && bk == 0) {  // leaves a layer-0 start node
+                o = bs;
+                h = 1;
+            } else {
+                const DPE e = ldE<S>(sv.srow + (size_t)bs * Kp + bk);
+                o = e.o;
+                h = e.h + 1;
+            }
+        } else if (l == 0) {
+            // Layer 0 keeps an older value and its older predecessor.
+            const int pe = __ldcg(predRow + v);
+            if (pe < 0) {
+                o = kLapEnd;
+            } else {
+                const int ps = pe - (k - 1) * n;
+                if (ps < 0 || ps >= n) {
+                    o = kLapUnknown;
+                } else if (k - 1 == 0) {
                     o = ps;
                     h = 1;
                 } else {
-                    const int* so = (inter && bs >= 0) ? porg : corg;
-                    const int* sh = (inter && bs >= 0) ? phop : chop;
-                    o = ldI<S>(so + (size_t)ps * Kp + pk);
-                    h = ldI<S>(sh + (size_t)ps * Kp + pk) + 1;
+                    const DPE e = ldE<S>(cur + (size_t)ps * Kp + (k - 1));
+                    o = e.o;
+                    h = e.h + 1;
                 }
             }
-            corg[(size_t)v * Kp + k] = o;
-            chop[(size_t)v * Kp + k] = h;
         }
+        stE(me, best, o, h);
     }
-    if (__any_sync(0xffffffffu, any) && lane == 0) p.layerFlag[l] = epoch;
+    return any;
+}
+
+template <class CT, int TK, bool S>
+__device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, int s1, int l, int k) {
+    const int n = p.n, K = p.K, Kp = p.Kp;
+    const bool inter = (k == 0);
+    const int part = inter ? 0 : 1;
+    const int* spl = st.spl(part);
+    const int r0 = spl[0];
+    StepView v;
+    // the step's streams from row r0 on: staged in shared memory, or read in
+    // place when a step of this CTA does not fit a buffer (rowCap == 0)
+    if (st.rowCap > 0) {
+        char* b = st.buf(sb);
+        v.src = reinterpret_cast<const int*>(b);
+        v.cost = b + (size_t)st.rowCap * 32 * 4;
+        v.time = b + (size_t)st.rowCap * 32 * (4 + sizeof(CT));
+    } else {
+        const size_t off = (size_t)l * (size_t)p.layerStride + (inter ? 0 : (size_t)p.interEntries) + (size_t)r0 * 32;
+        v.src = (inter ? (l == p.nY ? p.srcDummy : p.srcInter) : p.srcIntra) + (size_t)r0 * 32;
+        v.cost = reinterpret_cast<const CT*>(p.cost) + off;
+        v.time = TK == 0 ? nullptr : reinterpret_cast<const char*>(p.time) + off * st.timeBytes;
+    }
+    v.srow = p.dp + (size_t)((inter ? l - 1 : l) & 1) * n * Kp;
+    v.Kp = Kp;
+    v.kofs = inter ? 0 : k - 1;
+    v.nk = inter ? K : 1;
+    v.lam = p.lambda;
+    v.tconst = p.tconst;
+    if (!inter) return relax_slices<CT, TK, S, 1>(p, v, spl, s0, s1, l, k);
+    switch (K) {
+        case 1: return relax_slices<CT, TK, S, 1>(p, v, spl, s0, s1, l, k);
+        case 2: return relax_slices<CT, TK, S, 2>(p, v, spl, s0, s1, l, k);
+        case 3: return relax_slices<CT, TK, S, 3>(p, v, spl, s0, s1, l, k);
+        case 4: return relax_slices<CT, TK, S, 4>(p, v, spl, s0, s1, l, k);
+        default: return relax_slices<CT, TK, S, 0>(p, v, spl, s0, s1, l, k);
+    }
+}
+
+// Dataflow hand-off between steps of a multi-CTA team.  Step `step` of this
+// CTA is complete; publish it, then wait until every CTA on this CTA's wait
+// list (the owners of the sources it reads and the readers of the rows it
+// overwrites next) has completed it too.  This replaces a grid-wide barrier:
+// a CTA waits only for its graph neighbours.  Returns false when a wait ran
+// out of iterations or another CTA raised the error word.
+__device__ bool step_handoff(const BfParams& p, const Team& t, unsigned step) {
+    __syncthreads();  // the CTA's writes of this step are done
+    if (threadIdx.x < 32) {
+        // release store: with the CTA barrier above it publishes every write
+        // of the CTA's threads in this step
+        if (threadIdx.x == 0) st_release_u32(p.stepDone + (size_t)t.cta * kStepDoneStride, step);
+        __syncwarp();
+        const int w0 = __ldg(p.waitPtr + t.cta), w1 = __ldg(p.waitPtr + t.cta + 1);
+        int good = 1;
+        for (int i0 = w0; i0 < w1 && good; i0 += 32) {
+            const int i = i0 + (int)threadIdx.x;
+            const unsigned* f = i < w1 ? p.stepDone + (size_t)__ldg(p.waitIdx + i) * kStepDoneStride : nullptr;
+            unsigned spins = 0;
+            for (;;) {
+                const bool ready = f == nullptr || (int)(ld_acquire_u32(f) - step) >= 0;
+                if (__all_sync(0xffffffffu, ready)) break;
+                ++spins;
+                if ((spins & 63u) == 0 && *(volatile int*)t.err) { good = 0; break; }
+                if (spins > kSpinLimit) {
+                    if (threadIdx.x == 0) atomicExch(t.err, 1);
+                    good = 0;
+                    break;
+                }
+                if (spins > 256) __nanosleep(32);
+            }
+        }
+        if (threadIdx.x == 0 && !good) atomicExch(t.err, 1);
+    }
+    __syncthreads();
+    return *(volatile int*)t.err == 0;
 }
 
 // Brent's cycle finding on the lap function starting at x0.
@@ -454,40 +633,73 @@ __device__ int dij_walk_end(const BfParams& p, int v) {
 
 // ---------------------------------------------------------------------------
 // The Bellman-Ford launch.  Every CTA of the grid belongs to one team.
+// Dynamic shared memory: [DP tables + backup row, if S][candidate scratch].
 // ---------------------------------------------------------------------------
 template <class CT, int TK, bool S>
-__global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
+__global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     Team t{(int)blockIdx.x, (int)gridDim.x, &p.ctl->barCount, &p.ctl->barGen, &p.ctl->error};
     const int n = p.n, K = p.K, Kp = p.Kp;
     const long long tid = t.thread(), nth = t.nthreads();
     const bool isLead = (blockIdx.x == 0 && threadIdx.x == 0);
+    extern __shared__ double4 smemRaw[];
+    char* smem = reinterpret_cast<char*>(smemRaw);
     if constexpr (S) {
-        // single-CTA team: distance, backup, origin and hop tables live in
-        // shared memory for the whole launch (layout as in global memory)
-        extern __shared__ double4 smemRaw[];
-        double* sm = reinterpret_cast<double*>(smemRaw);
-        p.dp = sm;
-        p.bak = sm + 2 * (size_t)n * Kp;
-        p.org = reinterpret_cast<int*>(p.bak + n);
-        p.hops = p.org + 2 * (size_t)n * Kp;
+        // single-CTA team: the DP records and the backup row live in shared
+        // memory for the whole launch (layout as in global memory)
+        p.dp = reinterpret_cast<DPE*>(smem);
+        p.bak = reinterpret_cast<double*>(smem + (size_t)2 * n * Kp * sizeof(DPE));
+        smem += bf_shared_table_bytes(n, Kp);
+    }
+    const int s0 = __ldg(p.ctaSlice + blockIdx.x), s1 = __ldg(p.ctaSlice + blockIdx.x + 1);
+    const bool handoff = t.ncta > 1 && p.flagSync;
+    if (handoff && threadIdx.x == 0) p.stepDone[(size_t)t.cta * kStepDoneStride] = 0;
+    // shared memory: [row offsets of both parts][step buffer 0][step buffer 1]
+    __shared__ unsigned long long stageBar[2];
+    Stage st;
+    {
+        int* spl0 = reinterpret_cast<int*>(smem);
+        int* spl1 = spl0 + p.maxCtaSlices + 1;
+        for (int i = threadIdx.x; i <= s1 - s0; i += blockDim.x) {
+            spl0[i] = __ldg(p.spInter + s0 + i);
+            spl1[i] = __ldg(p.spIntra + s0 + i);
+        }
+        st.splInter = spl0;
+        st.splIntra = spl1;
+        st.costBytes = sizeof(CT);
+        st.timeBytes = TK == 1 ? 4 : TK == 2 ? 8 : 0;
+        st.rowCap = p.rowCap;
+        const size_t bufBytes = bf_stage_buffer_bytes(p.rowCap, st.costBytes, st.timeBytes);
+        st.buf0 = smem + bf_stage_offset(p.maxCtaSlices);
+        st.buf1 = st.buf0 + bufBytes;
+        st.bar = stageBar;
+        st.phase = 0;
+        st.pending = 0;
+        if (threadIdx.x == 0) {
+            mbar_init(stageBar);
+            mbar_init(stageBar + 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
     }
 
     // set-up (cost_time_ratio_solver.cpp:264-287): DP := inf, branch starts := 0
-    for (long long i = tid; i < 2LL * n * Kp; i += nth) p.dp[i] = kInfD;
+    // (each record is written once, by one thread)
+    for (long long r = tid; r < 2LL * n * Kp; r += nth) {
+        const long long node = (r / Kp) % n;
+        const bool start = r < (long long)n * Kp && r % Kp == 0 && p.branchOf[node] == p.branchId;
+        stE(p.dp + r, start ? 0.0 : kInfD, kLapUnknown, 0);
+    }
     for (long long i = tid; i < n; i += nth) {
         p.bak[i] = kInfD;
-        if (p.branchOf[i] == p.branchId) {
-            p.dp[(size_t)i * Kp] = 0.0;
-            p.pred[i] = -1;
-        }
+        if (p.branchOf[i] == p.branchId) p.pred[i] = -1;
     }
     {
         // branch size and the last branch node (the reference's indexNodeInLayer)
-        Key kmax{0, -1};
-        int cnt = 0;
+        int last = -1, cnt = 0;
         for (long long i = tid; i < n; i += nth)
-            if (p.branchOf[i] == p.branchId) { ++cnt; kmax.i = (int)i; }
-        Key km{-(double)kmax.i, kmax.i < 0 ? 0x7fffffff : kmax.i};
+            if (p.branchOf[i] == p.branchId) { ++cnt; last = (int)i; }
+        Key km{-(double)last, last < 0 ? 0x7fffffff : last};
+        if (last < 0) km.v = 1.0;
         km = block_min(km, 0);
         if (threadIdx.x == 0) p.redIdx[blockIdx.x] = km.i;
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
@@ -520,20 +732,61 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
     const int lastPar = lastRow / K, lastDepth = lastRow % K;
     const long long numNodes = p.numNodes;
     int sweep = 0;
+    unsigned step = 0;
     for (;;) {
-        const int epoch = epochBase + sweep + 1;
-        for (long long i = tid; i < n; i += nth) p.bak[i] = ldD<S>(p.dp + (size_t)i * Kp);
-        if (!team_sync(t)) return;
-        bool stop = false;
-        for (int l = 0; l <= p.nY && !stop; ++l) {
+        // the first step of the sweep is staged while the backup row is copied
+        stage_issue(p, st, s0, s1, 0, K > 1 ? 0 : 1, K > 1 ? 1 : 0);
+        for (long long i = tid; i < n; i += nth) p.bak[i] = ldV<S>(p.dp + (size_t)i * Kp);
+        if (!team_sync(t)) { stage_drain(st); return; }
+        // Layers are relaxed in order; a CTA hands each step off to its
+        // graph neighbours only (one team barrier closes the sweep).  The
+        // reference stops a sweep at the first layer 1..nY-1 without an
+        // improved node; every later layer then stays unreached (all
+        // infinite, no predecessor written), so the layers run to the end and
+        // the stop is decided from the per-layer stamps after the sweep.
+        const int stamp = epochBase + sweep + 1;
+        const unsigned long long tRelax = isLead ? clock64() : 0;
+        unsigned long long cycRelax = 0, cycHand = 0;
+        int sb = 0;  // buffer of the current step
+        for (int l = 0; l <= p.nY; ++l) {
             for (int k = 0; k < K; ++k) {
                 if (l == 0 && k == 0) continue;
-                relax_step<CT, TK, S>(p, t, l, k, epoch);
-                if (!team_sync(t)) return;
+                const unsigned long long ta = isLead ? clock64() : 0;
+                if (!stage_wait(st, sb)) {
+                    atomicExch(t.err, 1);
+                    stage_drain(st);
+                    return;
+                }
+                const bool last = l == p.nY && k == K - 1;
+                if (!last) stage_issue(p, st, s0, s1, sb ^ 1, k + 1 < K ? l : l + 1, k + 1 < K ? k + 1 : 0);
+                const bool any = relax_step<CT, TK, S>(p, st, sb, s0, s1, l, k);
+                if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) p.layerFlag[l] = stamp;
+                const unsigned long long tb = isLead ? clock64() : 0;
+                ++step;
+                sb ^= 1;
+                const bool ok = (handoff && !last) ? step_handoff(p, t, step) : team_sync(t);
+                if (!ok) {
+                    stage_drain(st);
+                    return;
+                }
+                if (isLead) {
+                    const unsigned long long tc = clock64();
+                    cycRelax += tb - ta;
+                    cycHand += tc - tb;
+                }
             }
-            if (l > 0 && l < p.nY && *(volatile int*)&p.layerFlag[l] != epoch) stop = true;
         }
+        int stopHere = 0;
+        for (int l = 1 + (int)threadIdx.x; l < p.nY; l += blockDim.x)
+            if (*(volatile int*)(p.layerFlag + l) != stamp) stopHere = 1;
+        const bool stop = __syncthreads_or(stopHere) != 0;
         ++sweep;
+        const unsigned long long tTail = isLead ? clock64() : 0;
+        if (isLead) {
+            p.ctl->cycPhaseA += cycRelax;
+            p.ctl->cycSync += cycHand;
+            p.ctl->cycPhaseB += tTail - tRelax - cycRelax - cycHand;
+        }
         if (stop) {
             if (isLead) { p.ctl->status = BF_LAYER_UNREACHED; p.ctl->sweeps = sweep; p.ctl->epoch = epochBase + sweep; }
             return;
@@ -546,16 +799,17 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             }
             return;
         }
+        const DPE* lastRowBase = p.dp + (size_t)lastPar * n * Kp + lastDepth;
         if (p.mode == 2) {
             // minimum-cost verdict: lower bounds of the branch nodes, origin of
             // their closing path, first and first-valid candidates.
             Key first{kInfD, 0x7fffffff}, firstValid{kInfD, 0x7fffffff};
             int anyFinite = 0;
-            const int* dOrg = p.org + (size_t)(p.nY & 1) * n * Kp;
+            const DPE* dRow = p.dp + (size_t)(p.nY & 1) * n * Kp;
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] != p.branchId) { p.lbOut[i] = kInfD; p.originOut[i] = -1; continue; }
-                const double lb = ldD<S>(p.dp + (size_t)lastPar * n * Kp + (size_t)i * Kp + lastDepth);
-                int o = ldI<S>(dOrg + (size_t)i * Kp);
+                const double lb = ldV<S>(lastRowBase + (size_t)i * Kp);
+                int o = ldE<S>(dRow + (size_t)i * Kp).o;
                 if (o < 0 && !isinf((float)lb)) o = dij_walk_end(p, (int)i);
                 p.lbOut[i] = lb;
                 p.originOut[i] = o;
@@ -601,20 +855,19 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
         // wrap-around (cost_time_ratio_solver.cpp:399-417) and lap function
         {
             int improved = 0;
-            const int wPar = (p.nY - 1) & 1;
-            const int* wOrg = p.org + (size_t)wPar * n * Kp;
-            const int* wHop = p.hops + (size_t)wPar * n * Kp;
+            const DPE* wRow = p.dp + (size_t)((p.nY - 1) & 1) * n * Kp;
             const long long layerSpan = (long long)n * K;
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] == p.branchId) {
-                    const double cand = ldD<S>(p.dp + (size_t)lastPar * n * Kp + (size_t)i * Kp + lastDepth);
+                    const double cand = ldV<S>(lastRowBase + (size_t)i * Kp);
                     const double b = p.bak[i];
+                    DPE* d0 = p.dp + (size_t)i * Kp;
                     if (cand < b) {
                         improved = 1;
-                        p.dp[(size_t)i * Kp] = cand;
+                        d0->v = cand;
                         p.pred[i] = __ldcg(p.pred + (size_t)p.nY * layerSpan + i);
                     } else {
-                        p.dp[(size_t)i * Kp] = b;
+                        d0->v = b;
                     }
                 }
                 const int pe = p.pred[i];
@@ -626,27 +879,22 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
                     if (pe < 0 || lp != p.nY - 1) {
                         nx = kLapUnknown;
                     } else {
-                        nx = ldI<S>(wOrg + (size_t)wv * Kp + kp);
-                        st = 1 + ldI<S>(wHop + (size_t)wv * Kp + kp);
+                        const DPE w = ldE<S>(wRow + (size_t)wv * Kp + kp);
+                        nx = w.o;
+                        st = 1 + w.h;
                     }
                 }
                 p.lapNext[i] = nx;
                 p.lapSteps[i] = st;
             }
-            improved = __syncthreads_or(improved);
-            if (threadIdx.x == 0) p.redAux[blockIdx.x] = improved;
-        }
-        if (!team_sync(t)) return;
-        {
-            int improved = 0;
-            for (int c = 0; c < t.ncta; ++c) improved |= *(volatile int*)&p.redAux[c];
+            bool ok;
+            improved = team_sync_or(t, improved, ok);
+            if (!ok) return;
             if (!improved) {
                 if (isLead) { p.ctl->status = BF_WRAP_NO_IMPROVE; p.ctl->sweeps = sweep; p.ctl->epoch = epochBase + sweep; }
                 return;
             }
         }
-        // every CTA has read redAux before it is reused below
-        if (!team_sync(t)) return;
 
         // candidates (cost_time_ratio_solver.cpp:431-489)
         {
@@ -656,7 +904,7 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             for (long long i = tid; i < n; i += nth) {
                 int st = 0;
                 if (p.branchOf[i] == p.branchId) {
-                    const double d0 = ldD<S>(p.dp + (size_t)i * Kp);
+                    const double d0 = ldV<S>(p.dp + (size_t)i * Kp);
                     if (d0 < 0) {
                         int v0 = -1;
                         long long steps = 0;
@@ -688,6 +936,7 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             }
         }
         if (!team_sync(t)) return;
+        int finished = 0;
         if (isLead) {
             Key ok{kInfD, 0x7fffffff}, unk{kInfD, 0x7fffffff};
             long long dec = 0;
@@ -714,13 +963,18 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
                     for (int i = 0; i < n; ++i) {
                         const int st = __ldcg(p.candStat + i);
                         if (st == 0) continue;
-                        Key kk{ldD<S>(p.dp + (size_t)i * Kp), i};
+                        Key kk{ldV<S>(p.dp + (size_t)i * Kp), i};
                         if (key_less(prev, kk) && key_less(kk, next)) next = kk;
                     }
                     if (next.i == 0x7fffffff) break;
                     prev = next;
                     const int st = __ldcg(p.candStat + next.i);
-                    if (st == 1) { winner = next.i; v0 = __ldcg(p.candV0 + winner); steps = __ldcg(p.candSteps + winner); break; }
+                    if (st == 1) {
+                        winner = next.i;
+                        v0 = __ldcg(p.candV0 + winner);
+                        steps = __ldcg(p.candSteps + winner);
+                        break;
+                    }
                     if (st == 3) {
                         p.ctl->fallbackWalks++;
                         if (literal_walk(p, next.i, numNodes, &v0, &steps) == 1) { winner = next.i; break; }
@@ -737,9 +991,12 @@ __global__ void __launch_bounds__(512) bf_kernel(BfParams p) {
             }
             p.ctl->sweeps = sweep;
             p.ctl->epoch = epochBase + sweep;
+            finished = p.ctl->status != BF_RUNNING;
         }
-        if (!team_sync(t)) return;
-        if (*(volatile int*)&p.ctl->status != BF_RUNNING) return;
+        bool ok;
+        finished = team_sync_or(t, finished, ok);
+        if (isLead) atomicAdd(&p.ctl->cycTail, clock64() - tTail);
+        if (!ok || finished) return;
     }
 }
 
@@ -770,7 +1027,6 @@ __global__ void extract_path_kernel(BfParams p, int v) {
 // the target whose source matches (computeRatioForCycle's lookup,
 // cost_time_ratio_solver.cpp:103-122) and returns its edge id and the double
 // cost/time of that edge.  Target ids >= numNodes denote the closing layer.
-
 __global__ void lookup_pairs_kernel(LookupArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.count) return;
@@ -830,28 +1086,21 @@ static const void* bf_fn(int costIsF32, int timeKind, bool sharedTables) {
                                          : (const void*)bf_kernel<double, 2, false>;
 }
 
-// Bytes of shared memory a single-CTA launch needs to keep the distance,
-// backup, origin and hop tables on chip.
-size_t bf_shared_table_bytes(int n, int Kp) {
-    return (size_t)n * Kp * 2 * sizeof(double) + (size_t)n * sizeof(double) + (size_t)n * Kp * 4 * sizeof(int);
-}
-
 cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
-                      size_t sharedBytes, cudaStream_t stream) {
+                      bool sharedTables, size_t smemBytes, cudaStream_t stream) {
     void* args[] = {(void*)&p};
-    const bool shared = sharedBytes > 0;
-    const void* fn = bf_fn(costIsF32, timeKind, shared);
-    if (shared) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sharedBytes);
-        if (e != cudaSuccess) return e;
-    }
-    if (cooperative) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, sharedBytes, stream);
-    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, sharedBytes, stream);
+    const void* fn = bf_fn(costIsF32, timeKind, sharedTables);
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+    if (e != cudaSuccess) return e;
+    if (cooperative) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
 }
 
-cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, int* blocksPerSm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, bf_fn(costIsF32, timeKind, false), threads, 0);
+cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm) {
+    const void* fn = bf_fn(costIsF32, timeKind, false);
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, smemBytes);
 }
 
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream) {

@@ -206,6 +206,9 @@ struct Stats {
     long long bfCalls = 0, sweeps = 0, candidates = 0, lawlerIters = 0, branches = 0, fallbackWalks = 0;
     double deviceMs = 0;
     long long launches = 0;
+    unsigned long long cycA = 0, cycB = 0, cycSync = 0, cycTail = 0;
+    long long steps = 0;
+    long long ctas = 0, threads = 0, waitEntries = 0;  // team shape of the last launch
 };
 
 class Graph {
@@ -238,8 +241,13 @@ class Graph {
     bool f32Known[2] = {false, false};  // e32 state computed since the last energy change
 
     // solver workspace
-    DBuf<double> wDp, wBak, wRedVal, wLb, wCOut, wTOut;
-    DBuf<int> wPred, wOrg, wHops, wLapNext, wLapSteps, wMark, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
+    DBuf<DPE> wDp;
+    DBuf<double> wBak, wRedVal, wLb, wCOut, wTOut;
+    DBuf<int> wCtaSlice, wWaitPtr, wWaitIdx;
+    DBuf<unsigned> wStepDone;
+    int ctaSliceBlocks = -1;
+    long long waitEntries = 0;  // wait-list entries over all CTAs of the current partition
+    DBuf<int> wPred, wLapNext, wLapSteps, wMark, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
         wRedIdx, wRedAux, wOrigin, wPairS, wPairT, wCount;
     DBuf<long long> wCandSteps, wRedAux64, wEdgeOut;
     DBuf<float> wMean;
@@ -293,10 +301,15 @@ class Graph {
         double tconst;
         int blocks, threads;
         bool coop;
-        size_t sharedBytes;  // > 0: single CTA keeping its tables in shared memory
+        bool sharedTables;  // single CTA keeping its DP records in shared memory
+        int flagSync;       // neighbour hand-offs between steps (multi-CTA teams)
+        int maxCtaSlices;   // most slices any CTA owns
+        int rowCap;         // rows a step buffer holds (0: streams read in place)
+        size_t smemBytes;   // dynamic shared memory per CTA
     };
     Run prepare_run(int K, bool ratio);
     void ensure_workspace(int K, int blocks);
+    void upload_cta_slices(int blocks);
     void upload_branch(const std::vector<int>& branchOf);
     // Every solve starts from an unwritten predecessor table (-1), like the
     // reference's freshly allocated solver state.
@@ -594,36 +607,122 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
         r.time = nullptr;
         r.tconst = ratio ? 50000.0 : 0.0;
     }
-    r.threads = env_int("PGC_BF_THREADS", 512);
-    int blocks = env_int("PGC_BF_BLOCKS", 0);
-    const int warpsPerBlock = r.threads / 32;
-    const int needed = (T.nslices + warpsPerBlock - 1) / warpsPerBlock;
-    if (blocks <= 0) {
-        if (T.n <= env_int("PGC_BF_SINGLE_CTA_MAX_NODES", 8192)) {
-            blocks = 1;
-        } else {
-            int sms = 0, perSm = 0;
-            PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-            PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, &perSm));
-            blocks = sms * std::max(1, std::min(perSm, 1));
+    // Team shape.  A warp relaxes one slice (32 nodes) per step, so a step
+    // costs about one slice's batches of memory latency when every warp has
+    // at most one slice.  Small graphs: one CTA that keeps the DP records in
+    // shared memory.  Otherwise CTAs of up to kBfThreads threads, one per
+    // (threads / 32) slices, up to the number that can be co-resident.  Each
+    // CTA stages its next step's streams in two shared-memory buffers; when
+    // they cannot fit, it reads the streams in place.
+    int sms = 0, smemOptin = 0;
+    PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    PGC_CUDA(cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    const size_t smemCap = (size_t)std::max(0, smemOptin - 1024);  // static shared memory of the kernel
+    const int costBytes = r.costF32 ? 4 : 8, timeBytes = r.timeKind == 1 ? 4 : r.timeKind == 2 ? 8 : 0;
+    const bool stageOn = env_int("PGC_BF_STAGE", 1) != 0;
+    auto stage_need = [&](int blocks, int& maxSl, int& rowCap) -> size_t {
+        maxSl = 0;
+        rowCap = 0;
+        for (int c = 0; c < blocks; ++c) {
+            const int a = (int)((long long)c * T.nslices / blocks), b = (int)((long long)(c + 1) * T.nslices / blocks);
+            maxSl = std::max(maxSl, b - a);
+            for (int p = 0; p < 2; ++p) rowCap = std::max(rowCap, T.sp[p][(size_t)b] - T.sp[p][(size_t)a]);
         }
-    }
-    blocks = std::max(1, std::min(blocks, std::max(1, needed)));
+        rowCap = std::max(rowCap, 1);
+        return bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(rowCap, costBytes, timeBytes);
+    };
+    const size_t tables = bf_shared_table_bytes(T.n, r.Kp);
+    const int envBlocks = env_int("PGC_BF_BLOCKS", 0), envThreads = env_int("PGC_BF_THREADS", 0);
+    if (envThreads && (envThreads < 32 || envThreads > kBfThreads || envThreads % 32 != 0))
+        throw Failure(PGC_ERR_ARG, "PGC_BF_THREADS must be a multiple of 32 in [32, 640]");
+    int maxSl = 0, rowCap = 0;
+    int blocks = envBlocks;
+    if (blocks <= 0 && T.nslices <= env_int("PGC_BF_SINGLE_CTA_SLICES", 64) &&
+        env_int("PGC_BF_SHARED_TABLES", 1) && tables + stage_need(1, maxSl, rowCap) <= smemCap)
+        blocks = 1;
+    r.threads = envThreads ? envThreads : kBfThreads;
+    if (blocks == 1 && !envThreads) r.threads = std::min(kBfThreads, 32 * T.nslices);
+    if (blocks <= 0) blocks = (T.nslices + r.threads / 32 - 1) / (r.threads / 32);
+    blocks = std::max(1, std::min(blocks, T.nslices));
+    r.sharedTables = blocks == 1 && env_int("PGC_BF_SHARED_TABLES", 1) && tables <= smemCap;
     if (blocks > 1) {
-        int sms = 0, perSm = 0;
-        PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-        PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, &perSm));
-        blocks = std::min(blocks, sms * std::max(1, perSm));
+        int perSm = 0;
+        PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, 0, &perSm));
+        if (perSm < 1) throw Failure(PGC_ERR_CUDA, "the Bellman-Ford kernel cannot be resident with this block size");
+        blocks = std::min(blocks, sms * perSm);
+    }
+    const size_t fixed = r.sharedTables ? tables : 0;
+    size_t need = stage_need(blocks, maxSl, rowCap);
+    r.rowCap = rowCap;
+    if (!stageOn || fixed + need > smemCap) {
+        r.rowCap = 0;  // read the streams in place
+        need = bf_stage_offset(maxSl);
+    }
+    r.maxCtaSlices = maxSl;
+    r.smemBytes = fixed + need;
+    if (r.smemBytes > smemCap) throw Failure(PGC_ERR_ARG, "the product graph's DP tables do not fit shared memory");
+    if (blocks > 1) {
+        int perSm = 0;
+        PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, r.smemBytes, &perSm));
+        if (perSm < 1) throw Failure(PGC_ERR_CUDA, "the Bellman-Ford kernel cannot be resident with its shared memory");
+        if (blocks > sms * perSm) {
+            // fewer CTAs fit with this much shared memory: read in place
+            blocks = sms * perSm;
+            stage_need(blocks, maxSl, rowCap);
+            r.rowCap = 0;
+            r.maxCtaSlices = maxSl;
+            r.smemBytes = bf_stage_offset(maxSl);
+        }
     }
     r.blocks = blocks;
     r.coop = blocks > 1;
-    r.sharedBytes = 0;
-    if (blocks == 1 && env_int("PGC_BF_SHARED_TABLES", 1)) {
-        const size_t bytes = bf_shared_table_bytes(T.n, r.Kp);
-        if (bytes <= (size_t)env_int("PGC_BF_SHARED_MAX_BYTES", 200 * 1024)) r.sharedBytes = bytes;
-    }
+    r.flagSync = env_int("PGC_BF_FLAGS", 1) ? 1 : 0;
     ensure_workspace(K, blocks);
+    upload_cta_slices(blocks);
     return r;
+}
+
+// Slice range of every CTA (equal slice counts: a warp's step time depends on
+// its own slice only), and every CTA's wait list: the CTAs that own a source
+// of one of its in-edges (it reads their rows) or read one of its nodes
+// through an in-edge (they must be done before it overwrites a row).  The
+// product graph repeats one layer template, so one pass over the template
+// covers every layer; the closing layer's sources are a subset of the
+// interlayer ones.
+void Graph::upload_cta_slices(int blocks) {
+    if (ctaSliceBlocks == blocks) return;
+    std::vector<int> cut((size_t)blocks + 1);
+    for (int c = 0; c <= blocks; ++c) cut[(size_t)c] = (int)((long long)c * T.nslices / blocks);
+    std::vector<int> owner((size_t)T.nslices);
+    for (int c = 0; c < blocks; ++c)
+        for (int s = cut[(size_t)c]; s < cut[(size_t)c + 1]; ++s) owner[(size_t)s] = c;
+    std::vector<unsigned char> adj((size_t)blocks * blocks, 0);
+    for (int p = 0; p < 2; ++p) {
+        for (int s = 0; s < T.nslices; ++s) {
+            const int ct = owner[(size_t)s];
+            for (int j = T.sp[p][(size_t)s]; j < T.sp[p][(size_t)s + 1]; ++j)
+                for (int lane = 0; lane < 32; ++lane) {
+                    const int sv = T.src[p][(size_t)j * 32 + lane];
+                    if (sv < 0) continue;
+                    const int cs = owner[(size_t)(sv >> 5)];
+                    if (cs == ct) continue;
+                    adj[(size_t)ct * blocks + cs] = 1;
+                    adj[(size_t)cs * blocks + ct] = 1;
+                }
+        }
+    }
+    std::vector<int> ptr((size_t)blocks + 1, 0), idx;
+    for (int c = 0; c < blocks; ++c) {
+        for (int d = 0; d < blocks; ++d)
+            if (adj[(size_t)c * blocks + d]) idx.push_back(d);
+        ptr[(size_t)c + 1] = (int)idx.size();
+    }
+    wCtaSlice.upload(cut.data(), cut.size(), stream);
+    wWaitPtr.upload(ptr.data(), ptr.size(), stream);
+    if (idx.empty()) idx.push_back(0);  // keep a valid pointer; ptr says the lists are empty
+    wWaitIdx.upload(idx.data(), idx.size(), stream);
+    waitEntries = ptr.back();
+    ctaSliceBlocks = blocks;
 }
 
 void Graph::ensure_workspace(int K, int blocks) {
@@ -633,8 +732,6 @@ void Graph::ensure_workspace(int K, int blocks) {
     const size_t expanded = n * (size_t)(T.nY + 1) * (size_t)K;
     if (wsK != K || wPred.n < expanded) {
         wDp.alloc(2 * n * Kp);
-        wOrg.alloc(2 * n * Kp);
-        wHops.alloc(2 * n * Kp);
         wPred.alloc(expanded);
         PGC_CUDA(cudaMemsetAsync(wPred.p, 0xff, expanded * sizeof(int), stream));  // -1
         wsK = K;
@@ -660,6 +757,7 @@ void Graph::ensure_workspace(int K, int blocks) {
         ctlEpoch = 0;
     }
     wCtl.alloc(1);
+    wStepDone.alloc((size_t)blocks * kStepDoneStride);
     wRedVal.alloc(2 * (size_t)blocks);
     wRedIdx.alloc(2 * (size_t)blocks);
     wRedAux.alloc((size_t)blocks);
@@ -695,8 +793,13 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.dp = wDp.p;
     p.bak = wBak.p;
     p.pred = wPred.p;
-    p.org = wOrg.p;
-    p.hops = wHops.p;
+    p.ctaSlice = wCtaSlice.p;
+    p.waitPtr = wWaitPtr.p;
+    p.waitIdx = wWaitIdx.p;
+    p.stepDone = wStepDone.p;
+    p.flagSync = r.flagSync;
+    p.maxCtaSlices = r.maxCtaSlices;
+    p.rowCap = r.rowCap;
     p.lapNext = wLapNext.p;
     p.lapSteps = wLapSteps.p;
     p.mark = wMark.p;
@@ -731,7 +834,7 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     PGC_CUDA(cudaEventCreate(&e0));
     PGC_CUDA(cudaEventCreate(&e1));
     PGC_CUDA(cudaEventRecord(e0, stream));
-    PGC_CUDA(launch_bf(p, r.costF32, r.timeKind, r.blocks, r.threads, r.coop, r.sharedBytes, stream));
+    PGC_CUDA(launch_bf(p, r.costF32, r.timeKind, r.blocks, r.threads, r.coop, r.sharedTables, r.smemBytes, stream));
     PGC_CUDA(cudaEventRecord(e1, stream));
     stats.launches++;
     PGC_CUDA(cudaMemcpyAsync(&c, wCtl.p, sizeof(Control), cudaMemcpyDeviceToHost, stream));
@@ -747,10 +850,19 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     stats.sweeps += c.sweeps;
     stats.candidates += c.candidates;
     stats.fallbackWalks += c.fallbackWalks;
+    stats.cycA += c.cycPhaseA;
+    stats.cycB += c.cycPhaseB;
+    stats.cycSync += c.cycSync;
+    stats.cycTail += c.cycTail;
+    stats.steps += (long long)c.sweeps * ((long long)(T.nY + 1) * r.K - 1);
+    stats.ctas = r.blocks;
+    stats.threads = r.threads;
+    stats.waitEntries = r.blocks > 1 ? waitEntries : 0;
     if (c.error) throw Failure(PGC_ERR_TIMEOUT, "a grid barrier wait of the Bellman-Ford kernel ran out");
     if (c.status == BF_ERR_EMPTY_BRANCH) throw Failure(PGC_ERR_INTERNAL, "no nodes in branch");
     if (c.status == BF_ERR_CYCLE_CAP) throw Failure(PGC_ERR_INTERNAL, "cycle longer than its buffer");
     if (c.status == BF_ERR_WALK) throw Failure(PGC_ERR_INTERNAL, "predecessor walk left the node range");
+    if (c.status == BF_ERR_CHUNK) throw Failure(PGC_ERR_INTERNAL, "a slice exceeds the shared-memory scratch");
     if (c.status == BF_RUNNING) throw Failure(PGC_ERR_INTERNAL, "Bellman-Ford launch ended without a verdict");
     return c;
 }
@@ -1524,6 +1636,21 @@ int pgc_result_cycle_edges(pgc_graph* h, int64_t* out, int64_t capacity, int64_t
         const Graph& g = h->g;
         *count = (int64_t)g.resEdges.size();
         for (int64_t i = 0; i < *count && i < capacity; ++i) out[i] = g.resEdges[(size_t)i];
+    });
+}
+
+int pgc_result_profile(pgc_graph* h, int64_t* out8) {
+    return guarded([&] {
+        if (!out8) throw pgc::Failure(PGC_ERR_ARG, "null output");
+        const pgc::Stats& s = h->g.stats;
+        out8[0] = (int64_t)s.cycA;
+        out8[1] = (int64_t)s.cycB;
+        out8[2] = (int64_t)s.cycSync;
+        out8[3] = (int64_t)s.cycTail;
+        out8[4] = s.steps;
+        out8[5] = s.ctas;
+        out8[6] = s.threads;
+        out8[7] = s.waitEntries;
     });
 }
 

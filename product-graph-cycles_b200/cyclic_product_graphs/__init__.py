@@ -59,6 +59,7 @@ _lib.pgc_result_stats.argtypes = [_h, _lp]
 _lib.pgc_compute_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
 _lib.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
 _lib.pgc_graph_info.argtypes = [_h, _lp]
+_lib.pgc_result_profile.argtypes = [_h, _lp]
 _lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
 _lib.pgc_last_error.restype = ctypes.c_char_p
 _lib.pgc_version.restype = ctypes.c_char_p
@@ -188,6 +189,13 @@ class product_graph_generator:
         out = np.empty(cnt.value, dtype=np.int64)
         _check(_lib.pgc_result_cycle_edges(self._h, out.ctypes.data_as(_lp), cnt.value, ctypes.byref(cnt)))
         return out
+
+    def last_profile(self) -> dict:
+        """SM-cycle counters (one thread of CTA 0) and team shape of the last solve's Bellman-Ford launches."""
+        buf = (ctypes.c_int64 * 8)()
+        _check(_lib.pgc_result_profile(self._h, buf))
+        return dict(zip(["cycles_relax", "cycles_bookkeeping", "cycles_handoff", "cycles_sweep_tail", "steps",
+                         "ctas", "threads", "wait_entries"], list(buf)))
 
     def graph_info(self) -> dict:
         """Sizes of the generated product graph (generates it if needed)."""
