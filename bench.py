@@ -130,18 +130,20 @@ def _dist_env():
 
 
 def algorithmic_bytes_per_sweep(info, k, ratio_mode):
-    """HBM bytes one Bellman-Ford sweep must move (roofline).
+    """Bytes one Bellman-Ford sweep must move: (4 + 4c)(E_inter + (K-1) E_intra) + 8 K n (nY + 1).
 
-    Every real edge's cost (and time, in ratio mode with two cost columns)
-    is streamed once per sweep as float32; every (node, depth) of every layer
-    writes its int32 predecessor.  The in-edge template (one layer), the
-    distance rows and the origin rows are L2-resident and not counted.
+    Every interlayer edge is visited once per sweep and every intralayer edge
+    once per depth 1..K-1; a visit reads the int32 source index and c fp32
+    cost columns (c = 2 in ratio mode with a time column, else 1).  Every
+    (node, depth) of the nY + 1 layers writes an fp32-sized value and an
+    int32 predecessor.  Gathered source values are not counted.
     """
     L = info["layers"]
-    edges = L * (info["inter_edges_per_layer"] + info["intra_edges_per_layer"])
-    per_edge = 4 * (2 if (ratio_mode and info["cost_columns"] > 1) else 1)
-    preds = 4 * k * info["nodes_per_layer"] * (L + 1)
-    return edges * per_edge + preds
+    c = 2 if (ratio_mode and info["cost_columns"] > 1) else 1
+    e_inter = L * info["inter_edges_per_layer"]
+    e_intra = L * info["intra_edges_per_layer"]
+    nodes = info["nodes_per_layer"] * (L + 1)
+    return (4 + 4 * c) * (e_inter + (k - 1) * e_intra) + 8 * k * nodes
 
 
 def run_ours(args, world, rank):
