@@ -82,6 +82,17 @@ int pgc_generate(pgc_graph* g);
 int pgc_cost_vector_shape(pgc_graph* g, int64_t* rows, int64_t* cols);
 int pgc_get_cost_vector(pgc_graph* g, double* out);
 
+/* No reference counterpart.  pgc_get_cost_vector without any device
+ * allocation: the export kernel writes into a fixed device scratch (a
+ * file-scope array of 2^21 doubles, 16 MiB) that is then copied to `out`.
+ * Needs generated costs -- it never generates (PGC_ERR_STATE otherwise) --
+ * and rows x cols <= 2^21 (PGC_ERR_ARG otherwise).  Nothing is cleared
+ * first: the export writes every value.  The first call on a device takes
+ * the scratch address with cudaGetSymbolAddress (that device current); make
+ * it before any stream capture.  There is one scratch per device, so calls
+ * that overlap in time race on it. */
+int pgc_get_cost_vector_noalloc(pgc_graph* g, double* out);
+
 /* getProductSpace() -- product_graph_generators.cpp:173-178, bindings.cpp:39.
  * [rows x 4] (plain) or [rows x 6] (conjugate) int32 edge table. */
 int pgc_product_space_shape(pgc_graph* g, int64_t* rows, int64_t* cols);

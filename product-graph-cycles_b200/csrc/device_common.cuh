@@ -227,6 +227,10 @@ cudaError_t launch_to_f32(const double* col, float* col32, long long total, long
 cudaError_t launch_export(const double* col, double* out, int cols, int c, long long total, long long layerStride,
                           long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
                           cudaStream_t s);
+// Most values (rows x columns) the no-allocation cost export holds: 2^21
+// doubles, 16 MiB of device memory fixed at module load.
+constexpr long long kNoAllocExportValues = 1LL << 21;
+cudaError_t noalloc_export_scratch(double** ptr);
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s);

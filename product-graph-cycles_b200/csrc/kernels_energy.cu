@@ -472,6 +472,15 @@ cudaError_t launch_export(const double* col, double* out, int cols, int c, long 
                                                        eBlock, ti, tr);
     return cudaGetLastError();
 }
+// Fixed device scratch of the no-allocation cost export: a file-scope array,
+// so that export allocates nothing.  Its address is taken once per device
+// (cudaGetSymbolAddress with that device current).
+static __device__ __align__(256) double g_noallocExport[kNoAllocExportValues];
+
+cudaError_t noalloc_export_scratch(double** ptr) {
+    return cudaGetSymbolAddress(reinterpret_cast<void**>(ptr), g_noallocExport);
+}
+
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s) {

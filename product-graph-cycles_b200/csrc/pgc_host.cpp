@@ -289,6 +289,7 @@ class Graph {
 
     // cost export / product space
     void cost_vector(double* out);
+    void cost_vector_noalloc(double* out);
     void product_space(int32_t* out);
 
   private:
@@ -1375,6 +1376,47 @@ void Graph::cost_vector(double* out) {
     PGC_CUDA(cudaStreamSynchronize(stream));
 }
 
+// Device address of the no-allocation export scratch on `device`, taken
+// once per device with that device current.
+static double* noalloc_scratch_for(int device) {
+    static std::mutex mu;
+    static std::map<int, double*> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = addr.find(device);
+    if (it != addr.end()) return it->second;
+    double* p = nullptr;
+    const cudaError_t e = noalloc_export_scratch(&p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Failure(PGC_ERR_CUDA, std::string("cudaGetSymbolAddress of the export scratch failed: ") +
+                                        cudaGetErrorString(e));
+    }
+    addr[device] = p;
+    return p;
+}
+
+// cost_vector() through the fixed device scratch: no device allocation, no
+// generation.  Every one of the rows x columns values is written by the
+// export (each product-graph edge has exactly one stream entry), so nothing
+// needs clearing first.
+void Graph::cost_vector_noalloc(double* out) {
+    if (!generated) throw Failure(PGC_ERR_STATE, "the no-allocation export needs generated edge costs (call generate first)");
+    const long long rows = (long long)T.nY * T.eBlock;
+    const long long values = rows * ncols;
+    if (values > kNoAllocExportValues)
+        throw Failure(PGC_ERR_ARG, "cost vector has " + std::to_string(values) +
+                                       " values; the no-allocation export holds at most " +
+                                       std::to_string(kNoAllocExportValues));
+    double* scratch = noalloc_scratch_for(device);
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    for (int c = 0; c < ncols; ++c)
+        PGC_CUDA(launch_export(e64[c].p, scratch, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
+                               dTedge[INTER].p, dTedge[INTRA].p, stream));
+    PGC_CUDA(cudaMemcpyAsync(out, scratch, sizeof(double) * (size_t)values, cudaMemcpyDeviceToHost, stream));
+    PGC_CUDA(cudaStreamSynchronize(stream));
+}
+
 void Graph::product_space(int32_t* out) {
     ensure_generated();
     const long long rows = (long long)T.nY * T.eBlock;
@@ -1553,6 +1595,14 @@ int pgc_get_cost_vector(pgc_graph* h, double* out) {
     return guarded([&] {
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.cost_vector(out);
+    });
+}
+
+int pgc_get_cost_vector_noalloc(pgc_graph* h, double* out) {
+    return guarded([&] {
+        if (!h || !out) throw pgc::Failure(PGC_ERR_ARG, "null argument");
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.cost_vector_noalloc(out);
     });
 }
 
