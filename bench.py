@@ -129,6 +129,22 @@ def _dist_env():
     return world, rank, local
 
 
+def max_over_ranks(value, world, device):
+    """The largest `value` of all ranks (every rank gets it); `value` itself at one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(solves_per_rank, world, max_ms):
+    """Whole-job solves/s of `world` replicas that each ran `solves_per_rank` solves, timed as the max over ranks."""
+    return world * solves_per_rank / (max_ms / 1000.0)
+
+
 def algorithmic_bytes_per_sweep(info, k, ratio_mode):
     """Bytes one Bellman-Ford sweep must move: (4 + 4c)(E_inter + (K-1) E_intra) + 8 K n (nY + 1).
 
@@ -195,13 +211,9 @@ def run_ours(args, world, rank):
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), world, "cuda")
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1000.0)
+    value = replica_throughput(args.steps, world, total_ms)
 
     # roofline of the dominant kernel (the Bellman-Ford launch)
     peak, peak_kind = _peaks()

@@ -859,7 +859,7 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     stats.ctas = r.blocks;
     stats.threads = r.threads;
     stats.waitEntries = r.blocks > 1 ? waitEntries : 0;
-    if (c.error) throw Failure(PGC_ERR_TIMEOUT, "a grid barrier wait of the Bellman-Ford kernel ran out");
+    if (c.error) throw Failure(PGC_ERR_TIMEOUT, "a wait of the Bellman-Ford kernel (team barrier, step hand-off or staged copy) ran out");
     if (c.status == BF_ERR_EMPTY_BRANCH) throw Failure(PGC_ERR_INTERNAL, "no nodes in branch");
     if (c.status == BF_ERR_CYCLE_CAP) throw Failure(PGC_ERR_INTERNAL, "cycle longer than its buffer");
     if (c.status == BF_ERR_WALK) throw Failure(PGC_ERR_INTERNAL, "predecessor walk left the node range");
