@@ -82,15 +82,22 @@ int pgc_generate(pgc_graph* g);
 int pgc_cost_vector_shape(pgc_graph* g, int64_t* rows, int64_t* cols);
 int pgc_get_cost_vector(pgc_graph* g, double* out);
 
-/* No reference counterpart.  pgc_get_cost_vector without any device
- * allocation: the export kernel writes into a fixed device scratch (a
- * file-scope array of 2^21 doubles, 16 MiB) that is then copied to `out`.
- * Needs generated costs -- it never generates (PGC_ERR_STATE otherwise) --
- * and rows x cols <= 2^21 (PGC_ERR_ARG otherwise).  Nothing is cleared
- * first: the export writes every value.  The first call on a device takes
- * the scratch address with cudaGetSymbolAddress (that device current); make
- * it before any stream capture.  There is one scratch per device, so calls
- * that overlap in time race on it. */
+/* No counterpart in the reference.  pgc_get_cost_vector for callers that
+ * cannot let this library allocate device memory: processes whose GPU memory
+ * is already reserved by their own allocator (a PyTorch job's caching
+ * allocator, a serving engine that pre-reserves most of HBM), where a
+ * cudaMalloc would fail or make that allocator release memory, and loops that
+ * cannot afford the device-wide synchronization of cudaFree.  The export
+ * kernel writes into a fixed device scratch -- a file-scope array of 2^21
+ * doubles (16 MiB) that every GPU loading the library holds until exit --
+ * which is then copied to `out`.  Nothing is allocated and nothing is
+ * generated: the graph's costs must exist already (PGC_ERR_STATE otherwise)
+ * and rows x cols must be at most 2^21 (PGC_ERR_ARG otherwise).  Nothing
+ * needs clearing first: the export writes every value.  The first call on a
+ * device takes the scratch's device address (cudaGetSymbolAddress, that
+ * device current); make that first call before any stream capture.  Every
+ * call shares the one scratch of its device, so calls that overlap on the GPU
+ * race on it. */
 int pgc_get_cost_vector_noalloc(pgc_graph* g, double* out);
 
 /* getProductSpace() -- product_graph_generators.cpp:173-178, bindings.cpp:39.

@@ -230,7 +230,9 @@ cudaError_t launch_export(const double* col, double* out, int cols, int c, long 
 // Most values (rows x columns) the no-allocation cost export holds: 2^21
 // doubles, 16 MiB of device memory fixed at module load.
 constexpr long long kNoAllocExportValues = 1LL << 21;
-cudaError_t noalloc_export_scratch(double** ptr);
+// Device address of the no-allocation export scratch on `device` (which must
+// be current); taken with cudaGetSymbolAddress on the first call, then cached.
+cudaError_t noalloc_export_scratch(int device, double** ptr);
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s);

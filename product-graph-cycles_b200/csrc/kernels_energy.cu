@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <mutex>
 
 #include "device_common.cuh"
 
@@ -472,13 +474,35 @@ cudaError_t launch_export(const double* col, double* out, int cols, int c, long 
                                                        eBlock, ti, tr);
     return cudaGetLastError();
 }
-// Fixed device scratch of the no-allocation cost export: a file-scope array,
-// so that export allocates nothing.  Its address is taken once per device
-// (cudaGetSymbolAddress with that device current).
+// Fixed device scratch of the no-allocation cost export.  Some callers
+// cannot let this library allocate device memory: a process whose HBM is
+// already reserved by its own allocator (a PyTorch job's caching allocator, a
+// serving engine that pre-reserves most of the GPU) would see cudaMalloc fail
+// or force that allocator to give memory back, and cudaFree synchronizes the
+// whole device, stalling the caller's other streams.  For them the export
+// writes into this file-scope array instead: 2^21 doubles (16 MiB) that every
+// GPU loading the library holds until the process exits.
 static __device__ __align__(256) double g_noallocExport[kNoAllocExportValues];
 
-cudaError_t noalloc_export_scratch(double** ptr) {
-    return cudaGetSymbolAddress(reinterpret_cast<void**>(ptr), g_noallocExport);
+// In host code g_noallocExport names a host-side stand-in, not device memory,
+// so kernels are given the device address, taken here once per device with
+// that device current (the caller sets it) and cached.  The first call on a
+// device therefore does this set-up; it should come before any stream capture.
+cudaError_t noalloc_export_scratch(int device, double** ptr) {
+    static std::mutex mu;
+    static std::map<int, double*> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto it = addr.find(device);
+    if (it != addr.end()) {
+        *ptr = it->second;
+        return cudaSuccess;
+    }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocExport);
+    if (e != cudaSuccess) return e;
+    *ptr = static_cast<double*>(p);
+    addr[device] = *ptr;
+    return cudaSuccess;
 }
 
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,

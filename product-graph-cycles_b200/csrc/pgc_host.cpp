@@ -1376,22 +1376,15 @@ void Graph::cost_vector(double* out) {
     PGC_CUDA(cudaStreamSynchronize(stream));
 }
 
-// Device address of the no-allocation export scratch on `device`, taken
-// once per device with that device current.
+// Device address of the no-allocation export scratch on `device` (current).
 static double* noalloc_scratch_for(int device) {
-    static std::mutex mu;
-    static std::map<int, double*> addr;
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = addr.find(device);
-    if (it != addr.end()) return it->second;
     double* p = nullptr;
-    const cudaError_t e = noalloc_export_scratch(&p);
+    const cudaError_t e = noalloc_export_scratch(device, &p);
     if (e != cudaSuccess) {
         cudaGetLastError();
         throw Failure(PGC_ERR_CUDA, std::string("cudaGetSymbolAddress of the export scratch failed: ") +
                                         cudaGetErrorString(e));
     }
-    addr[device] = p;
     return p;
 }
 

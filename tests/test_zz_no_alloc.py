@@ -1,7 +1,12 @@
-"""pgc_get_cost_vector_noalloc (no reference counterpart) against the
-existing pgc_get_cost_vector, both called through the C ABI: two calls in a
-row must return the same matrix bit for bit, on plain and conjugate graphs,
-before and after a ratio solve has rescaled the costs in place."""
+"""pgc_get_cost_vector_noalloc, the cost export for callers that cannot let
+the library allocate device memory (their GPU memory is held by their own
+allocator, or they cannot afford cudaFree's device-wide synchronization). It
+has no counterpart in the reference. Called through the C ABI, two calls in a
+row must return the same matrix, bit for bit, as the allocating
+pgc_get_cost_vector. That holds on plain and conjugate graphs, before and
+after a ratio solve has rescaled the costs in place. Larger cost vectors than
+the 2^21-value scratch, and graphs whose costs were never generated, are
+refused."""
 import ctypes
 
 import numpy as np
