@@ -303,16 +303,18 @@ __device__ __forceinline__ void stage_drain(Stage& st) {
 //
 // A warp owns a slice of 32 target nodes (lane = node).  The slice's in-edge
 // rows are visited in the reference's order -- ascending edge, then source
-// depth -- in batches of kGather / NK rows (NK source depths per edge, a
-// compile-time constant of the step kind): first every source value of the
-// batch is gathered (independent loads), then the batch is folded into the
-// running first minimum, so a batch costs one memory latency.  The fold keeps
-// thr = min(best, upper bound): a candidate is taken iff cand < thr, which
-// is the reference's (cand < best && cand < ub); an unreached source
-// (+inf) can never pass it.  The winner's origin and path length are read
-// once per node after the fold.  Returns whether this thread improved a node.
+// depth -- in batches of up to min(kGather / NK, 8) rows (NK source depths
+// per edge, a compile-time constant of the step kind); the last batch has
+// exactly the rows that remain.  First every source value of the batch is
+// gathered (independent loads), then the batch is folded into the running
+// first minimum, so a batch costs one memory latency.  The fold keeps only
+// thr = min(best, upper bound) and the position of the last improvement: a
+// candidate is taken iff cand < thr, which is the reference's
+// (cand < best && cand < ub), and an unreached source (+inf) can never pass
+// it.  The winner's origin and path length are read once per node after the
+// fold.  Returns whether this thread improved a node.
 // ---------------------------------------------------------------------------
-constexpr int kGather = 12;
+constexpr int kGather = 16;
 
 struct StepView {
     const int* src;     // source index per entry, from the step's first row
@@ -333,32 +335,55 @@ __device__ __forceinline__ double edge_weight(const StepView& v, int q) {
 
 // Rows [row, j1) of one slice for lane `lane`; NK > 0 source depths per edge
 // known at compile time, NK == 0: v.nk depths, one gather at a time.
-template <class CT, int TK, bool S, int NK>
-__device__ __forceinline__ void fold_rows(const StepView& v, int lane, int row, int j1, double& best, double& thr,
-                                          int& bs, int& bk) {
-    if constexpr (NK > 0) {
-        constexpr int RB = kGather / NK > 0 ? kGather / NK : 1;
-        for (; row < j1; row += RB) {
-            int sv[RB];
-            double d[RB][NK];
+// One batch of exactly NR rows starting at `row`: every source value is
+// gathered first, then the batch is folded in edge order.  `win` records the
+// position of the last improvement (row * 8 + depth); thr is its value.
+template <class CT, int TK, bool S, int NK, int NR>
+__device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row, double& thr, int& win) {
+    int sv[NR];
+    double d[NR][NK];
 #pragma unroll
-            for (int r = 0; r < RB; ++r) {
-                sv[r] = row + r < j1 ? v.src[(row + r) * 32 + lane] : -1;
-                const DPE* rec = v.srow + (size_t)(sv[r] < 0 ? 0 : sv[r]) * v.Kp + v.kofs;
+    for (int r = 0; r < NR; ++r) {
+        sv[r] = v.src[(row + r) * 32 + lane];
+        const DPE* rec = v.srow + (size_t)(sv[r] < 0 ? 0 : sv[r]) * v.Kp + v.kofs;
 #pragma unroll
-                for (int kk = 0; kk < NK; ++kk) d[r][kk] = sv[r] >= 0 ? ldV<S>(rec + kk) : kInfD;
-            }
+        for (int kk = 0; kk < NK; ++kk) d[r][kk] = sv[r] >= 0 ? ldV<S>(rec + kk) : kInfD;
+    }
 #pragma unroll
-            for (int r = 0; r < RB; ++r) {
-                if (sv[r] < 0) continue;
-                const double w = edge_weight<CT, TK>(v, (row + r) * 32 + lane);
+    for (int r = 0; r < NR; ++r) {
+        if (sv[r] < 0) continue;
+        const double w = edge_weight<CT, TK>(v, (row + r) * 32 + lane);
 #pragma unroll
-                for (int kk = 0; kk < NK; ++kk) {
-                    const double cand = __dadd_rn(d[r][kk], w);
-                    if (cand < thr) { best = cand; thr = cand; bs = sv[r]; bk = v.kofs + kk; }
-                }
-            }
+        for (int kk = 0; kk < NK; ++kk) {
+            const double cand = __dadd_rn(d[r][kk], w);
+            if (cand < thr) { thr = cand; win = ((row + r) << 3) | kk; }
         }
+    }
+}
+
+// The last nr (1 <= nr <= NR) rows as one batch of exactly nr rows.  The row
+// count is the slice's, the same in every lane, so no lane runs row slots
+// that do not exist.
+template <class CT, int TK, bool S, int NK, int NR>
+__device__ __forceinline__ void fold_tail(const StepView& v, int lane, int row, int nr, double& thr, int& win) {
+    if constexpr (NR <= 1) {
+        fold_batch<CT, TK, S, NK, 1>(v, lane, row, thr, win);
+    } else {
+        if (nr == NR) fold_batch<CT, TK, S, NK, NR>(v, lane, row, thr, win);
+        else fold_tail<CT, TK, S, NK, NR - 1>(v, lane, row, nr, thr, win);
+    }
+}
+
+// Rows [row, j1) of one slice for lane `lane`.  Returns the position of the
+// winning candidate -- row * 8 + depth for NK > 0, row * nk + depth for the
+// run-time depth count (NK == 0) -- or -1; thr holds its value.
+template <class CT, int TK, bool S, int NK>
+__device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, int j1, double& thr) {
+    int win = -1;
+    if constexpr (NK > 0) {
+        constexpr int RB = kGather / NK < 1 ? 1 : kGather / NK > 8 ? 8 : kGather / NK;
+        for (; j1 - row >= RB; row += RB) fold_batch<CT, TK, S, NK, RB>(v, lane, row, thr, win);
+        if (row < j1) fold_tail<CT, TK, S, NK, RB>(v, lane, row, j1 - row, thr, win);
     } else {
         for (; row < j1; ++row) {
             const int sv = v.src[row * 32 + lane];
@@ -367,10 +392,11 @@ __device__ __forceinline__ void fold_rows(const StepView& v, int lane, int row, 
             const DPE* rec = v.srow + (size_t)sv * v.Kp + v.kofs;
             for (int kk = 0; kk < v.nk; ++kk) {
                 const double cand = __dadd_rn(ldV<S>(rec + kk), w);
-                if (cand < thr) { best = cand; thr = cand; bs = sv; bk = v.kofs + kk; }
+                if (cand < thr) { thr = cand; win = row * v.nk + kk; }
             }
         }
     }
+    return win;
 }
 
 template <class CT, int TK, bool S, int NK>
@@ -390,10 +416,17 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
         DPE* me = cur + (size_t)v * Kp + k;
         double best = (l == 0 && valid) ? ldV<S>(me) : kInfD;
         double thr = best < ub ? best : ub;
-        int bs = -1, bk = -1;
-        if (!empty) fold_rows<CT, TK, S, NK>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, best, thr, bs, bk);
+        int win = -1;
+        if (!empty) win = fold_rows<CT, TK, S, NK>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, thr);
         if (!valid) continue;
         int o = kLapUnknown, h = 0;
+        int bs = -1, bk = -1;
+        if (win >= 0) {
+            const int rw = NK > 0 ? (win >> 3) : win / sv.nk;
+            bk = sv.kofs + (NK > 0 ? (win & 7) : win % sv.nk);
+            bs = sv.src[rw * 32 + lane];
+            best = thr;
+        }
         if (bs >= 0) {
             predRow[v] = bs + srcLayer * n * K + bk * n;
             any = true;
