@@ -45,6 +45,11 @@ WORKLOADS = {
     "conj_2k_100_k3": (2000, 100, 64, True, False, False, "vanilla", "lengthnormalisation", 3),
 }
 DEFAULT_WORKLOAD = "single_pair_conj_5k_200_k3"
+# batched serving: many plain pairs of uneven size solved concurrently
+BATCHES = {
+    # name: (pairs, |VX| range, |VY| range (even), k choices, feature dim)
+    "batch_256_plain_1k8k": (256, (1000, 8000), (50, 250), (2, 3), 32),
+}
 
 
 def _peaks():
@@ -357,13 +362,184 @@ def run_reference(args):
     }
 
 
+def _batch_specs(name, seed):
+    import numpy as np
+
+    count, (v0, v1), (m0, m1), ks, dim = BATCHES[name]
+    rng = np.random.default_rng(seed)
+    return [dict(nv=int(rng.integers(v0, v1 + 1)), m=2 * int(rng.integers(m0 // 2, m1 // 2 + 1)),
+                 k=int(rng.choice(ks)), dim=dim, seed=seed * 100000 + i) for i in range(count)]
+
+
+def _batch_pair(spec):
+    sys.path.insert(0, os.path.join(ROOT, "product-graph-cycles_b200"))
+    from cyclic_product_graphs import synthetic
+
+    p = synthetic.make_pair(n_vertices=spec["nv"], n_curve=spec["m"], feat_dim=spec["dim"], seed=spec["seed"],
+                            with_normals=False)
+    return {k: p[k] for k in ("VX", "EX", "VY", "EY", "feat_diff")}
+
+
+def _batch_pairs(name, seed):
+    """The batch's seeded pairs, built in parallel host processes (spawned, before any GPU work)."""
+    import multiprocessing as mp
+
+    specs = _batch_specs(name, seed)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        pairs = pool.map(_batch_pair, specs, chunksize=4)
+    return specs, pairs
+
+
+def run_batch(args, world, rank):
+    """Batched serving: every step solves all pairs of the batch concurrently
+    (solve_batch: one stream and a one-CTA Bellman-Ford team per pair, costs
+    regenerated on the device first).  Also timed: the same pairs solved one
+    after the other with full-GPU teams (the plain per-pair GPU Lawler)."""
+    specs, pairs = _batch_pairs(args.workload, args.seed + rank)
+    import numpy as np
+    import torch
+
+    import cyclic_product_graphs as cpg
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dev = torch.cuda.current_device()
+
+    def make(i):
+        p = pairs[i]
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], False, False)
+        g.set_cost_time_ratio_mode("vanilla", "nomode")
+        g.set_max_depth_cost_time_ratio(specs[i]["k"])
+        return g
+
+    gens = [make(i) for i in range(len(pairs))]
+    for g in gens:
+        g.generate()
+    infos = [g.graph_info() for g in gens]
+
+    def step():
+        return cpg.solve_batch(gens, "lawlergpu", None, ctas_per_graph=1, regenerate=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    bytes_moved = 0
+    with ClockSampler(dev) as clocks:
+        for i in range(args.steps):
+            torch.cuda.synchronize()
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+            torch.cuda.synchronize()
+            for g, info, sp in zip(gens, infos, specs):
+                bytes_moved += algorithmic_bytes_per_sweep(info, sp["k"], True) * g.last_stats()["sweeps"]
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
+    solves = len(gens) * args.steps
+    value = replica_throughput(solves, world, total_ms)
+    peak, peak_kind = _peaks()
+    achieved = bytes_moved / (total_ms * 1e-3) / 1e9
+
+    # the plain per-pair GPU Lawler: the same pairs one after the other, full-GPU teams
+    seq_n = min(len(gens), 32)
+    for g in gens[:seq_n]:
+        g.generate()
+        g.solve_with_cost_time_ratio("lawlergpu")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for g in gens[:seq_n]:
+        g.generate()
+        g.solve_with_cost_time_ratio("lawlergpu")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_value = seq_n / (e0.elapsed_time(e1) / 1000.0)
+
+    # end to end from host arrays: handles built, batch solved, matchings back
+    h2d = sum(int(sum(np.asarray(p[k]).nbytes for k in p)) for p in pairs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fresh = [make(i) for i in range(len(pairs))]
+    results = cpg.solve_batch(fresh, "lawlergpu", None, ctas_per_graph=1)
+    e2e_s = time.perf_counter() - t0
+    d2h = sum(int(r[2].nbytes) + 8 for r in results)
+    del fresh
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (fp32 integer-valued cost streams)", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "pairs": len(gens), "vx_range": BATCHES[args.workload][1],
+                   "vy_range": BATCHES[args.workload][2], "k": BATCHES[args.workload][3],
+                   "edges_total": sum(i["layers"] * i["edges_per_block"] for i in infos),
+                   "parallelism": f"one stream + one CTA per pair, replicas x{world}",
+                   "l2": "inputs larger than L2 (all pairs' cost streams together)"},
+        "vs_plain_gpu_lawler": {"plain_solves_per_s": seq_value, "ratio": value / seq_value,
+                                "sample": f"first {seq_n} pairs solved one after the other, full-GPU teams"},
+        "e2e": {"value": world * len(pairs) / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": 1},
+        "gpu_launches": None,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_kernel (all pairs)",
+                     "note": "algorithmic bytes of every sweep of every pair / batch step time"},
+        "clocks": clocks.summary(),
+    }
+    launches = 0
+    for g in gens:
+        launches += g.last_stats()["kernel_launches"] + 1
+    line["gpu_launches"] = launches * args.steps
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = _batch_cpu_sample(specs, pairs)
+    return line
+
+
+def _batch_cpu_sample(specs, pairs, count=2):
+    """The oracle's lawlercpu on the first `count` pairs of the batch, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    t = 0.0
+    for spec, p in zip(specs[:count], pairs[:count]):
+        o = orc.OracleGenerator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], False, False)
+        o.set_cost_time_ratio_mode("vanilla", "nomode")
+        t0 = time.perf_counter()
+        o.generate()
+        o.solve_with_cost_time_ratio("lawlercpu", spec["k"])
+        t += time.perf_counter() - t0
+    return {"value": count / t, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"oracle generate + lawlercpu, OpenMP x{cores}, on the batch's first {count} pairs "
+                      f"({[(s['nv'], s['m'], s['k']) for s in specs[:count]]}), solved one after the other"}
+
+
+def run_reference_batch(args):
+    specs, pairs = _batch_pairs(args.workload, args.seed)
+    samples = []
+    for _ in range(max(0, args.warmup - 1)):
+        _batch_cpu_sample(specs, pairs, 1)
+    for i in range(args.steps):
+        samples.append(_batch_cpu_sample(specs[i % len(specs):], pairs[i % len(pairs):], 1)["value"])
+    value = statistics.median(samples)
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "pairs": len(specs)},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": "oracle generate + lawlercpu of one pair of the batch per step "
+                                       "(pairs 0..steps-1), median"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCHES), default=DEFAULT_WORKLOAD)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sweeps", type=int, default=3)
@@ -373,7 +549,8 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
+            fn = run_reference_batch if args.workload in BATCHES else run_reference
+            print(json.dumps(fn(args)), flush=True)
         return
 
     if world > 1:
@@ -383,7 +560,7 @@ def main():
 
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = run_ours(args, world, rank)
+    line = run_batch(args, world, rank) if args.workload in BATCHES else run_ours(args, world, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

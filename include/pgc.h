@@ -116,6 +116,24 @@ int pgc_solve_with_cost_time_ratio(pgc_graph* g, const char* solver_name, int ma
  * DijkstraSolver::run, dijkstra_solver.cpp:563-579. */
 int pgc_solve_with_minimum_cost(pgc_graph* g, const char* solver_name, int max_depth);
 
+/* No reference counterpart.  Most CTAs one Bellman-Ford launch of this graph
+ * may use (0, the default: as many as shorten a step).  A small team is
+ * slower per solve but leaves the rest of the GPU to other graphs. */
+int pgc_set_team_cap(pgc_graph* g, int max_ctas);
+
+/* No reference counterpart.  Solves `count` graphs concurrently: each one as
+ * pgc_solve_with_cost_time_ratio (solver "lawlercpu"/"lawlergpu") or
+ * pgc_solve_with_minimum_cost (any other name) would, on its own stream with
+ * a team of at most `ctas_per_graph` CTAs (0: one), driven by `workers` host
+ * threads (0: one per graph, at most 512; waiting threads sleep).  With
+ * `regenerate` != 0 each graph first recomputes its
+ * edge costs (pgc_generate).  Each graph's result is read afterwards with
+ * pgc_result*; status[i] receives its return code.  Returns PGC_OK when all
+ * succeeded, else the first failure's code (with its message).  The handles
+ * must be distinct. */
+int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver_name, int max_depth,
+                    int ctas_per_graph, int workers, int regenerate, int* status);
+
 /* The CTR_CYCLE_SOLVER_OUTPUT / DIJKSTRA_SOLVER_OUTPUT tuple
  * (cost_time_ratio_solver.hpp:70, dijkstra_solver.hpp:22) of the last solve. */
 int pgc_result(pgc_graph* g, int* passes_layers_just_once, float* final_objective, int64_t* rows, int64_t* cols);

@@ -1119,11 +1119,29 @@ static const void* bf_fn(int costIsF32, int timeKind, bool sharedTables) {
                                          : (const void*)bf_kernel<double, 2, false>;
 }
 
+// The dynamic shared-memory limit is an attribute of the kernel function,
+// shared by every host thread: it is always raised to the device's opt-in
+// maximum (the same value from every thread, so concurrent solves cannot
+// lower it under each other's launches); each launch then requests its own
+// size.
+static cudaError_t allow_max_dynamic_smem(const void* fn) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) {
+        cudaFuncAttributes a{};
+        e = cudaFuncGetAttributes(&a, fn);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+    }
+    return e;
+}
+
 cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
                       bool sharedTables, size_t smemBytes, cudaStream_t stream) {
     void* args[] = {(void*)&p};
     const void* fn = bf_fn(costIsF32, timeKind, sharedTables);
-    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+    const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
     if (cooperative) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
@@ -1131,7 +1149,7 @@ cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks
 
 cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm) {
     const void* fn = bf_fn(costIsF32, timeKind, false);
-    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes);
+    const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, smemBytes);
 }

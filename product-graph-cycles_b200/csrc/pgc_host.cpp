@@ -24,7 +24,9 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
+#include <atomic>
 
 #include "../../include/pgc.h"
 #include "branch_heap.hpp"
@@ -254,6 +256,7 @@ class Graph {
     DBuf<Control> wCtl;
     int wsK = -1;
     int ctlEpoch = 0, ctlWalkId = 0;
+    int teamCap = 0;  // most CTAs of a Bellman-Ford launch (0: as many as help)
     bool workspaceFresh = false;
 
     // last result
@@ -264,9 +267,35 @@ class Graph {
     std::vector<long long> resEdges;
     Stats stats;
 
+    // Waiting for the stream: a spin wait by default (lowest latency); while
+    // many graphs are solved at once by as many host threads, a blocking
+    // wait, so that waiting threads sleep instead of competing for cores.
+    bool blockingSync = false;
+    cudaEvent_t syncEvent = nullptr;
+    cudaEvent_t timeEvents[2] = {nullptr, nullptr};  // around each Bellman-Ford launch
+    cudaError_t sync_stream() {
+        if (!blockingSync) return cudaStreamSynchronize(stream);
+        cudaError_t e = cudaSuccess;
+        if (!syncEvent) e = cudaEventCreateWithFlags(&syncEvent, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(syncEvent, stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(syncEvent);
+        return e;
+    }
+
+    // Device -> pageable host copy.  The copy waits for the stream's earlier
+    // work inside the driver (a spin); in blocking mode that wait happens on
+    // the blocking event first.
+    void d2h(void* dst, const void* src, size_t bytes) {
+        if (blockingSync) PGC_CUDA(sync_stream());
+        PGC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+    }
+
     ~Graph() {
         // device buffers go back to the caching pool: no work may still use them
         if (stream) cudaStreamSynchronize(stream);
+        if (syncEvent) cudaEventDestroy(syncEvent);
+        for (cudaEvent_t e : timeEvents)
+            if (e) cudaEventDestroy(e);
         if (ownStream) cudaStreamDestroy(ownStream);
     }
 
@@ -443,7 +472,7 @@ void Graph::generate() {
         PGC_CUDA(launch_ho_energy(a, s));
         dQuat.release();
     }
-    PGC_CUDA(cudaStreamSynchronize(s));
+    PGC_CUDA(sync_stream());
     energy_changed();
     generated = true;
 }
@@ -499,8 +528,8 @@ double Graph::median_of_column(int col) {
         PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
         PGC_CUDA(launch_select_hist(a, stream));
         stats.launches++;
-        PGC_CUDA(cudaMemcpyAsync(h.data(), hist.p, sizeof(unsigned long long) << b, cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(h.data(), hist.p, sizeof(unsigned long long) << b);
+        PGC_CUDA(sync_stream());
         int digit = 0;
         long long acc = 0;
         for (; digit < (1 << b); ++digit) {
@@ -527,8 +556,8 @@ double Graph::median_of_column(int col) {
         PGC_CUDA(launch_select_compact(a, band.p, cnt.p, bucket, stream));
         stats.launches++;
         std::vector<double> vals((size_t)bucket);
-        PGC_CUDA(cudaMemcpyAsync(vals.data(), band.p, sizeof(double) * (size_t)bucket, cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(vals.data(), band.p, sizeof(double) * (size_t)bucket);
+        PGC_CUDA(sync_stream());
         std::sort(vals.begin(), vals.end());
         xk = vals[(size_t)rank];
         if (even && rank + 1 < bucket) xk1 = vals[(size_t)rank + 1];
@@ -540,8 +569,8 @@ double Graph::median_of_column(int col) {
         PGC_CUDA(cudaMemcpyAsync(cnt.p, &best, sizeof(best), cudaMemcpyHostToDevice, stream));
         PGC_CUDA(launch_select_min_above(a, bucketTop, cnt.p, stream));
         stats.launches++;
-        PGC_CUDA(cudaMemcpyAsync(&best, cnt.p, sizeof(best), cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(&best, cnt.p, sizeof(best));
+        PGC_CUDA(sync_stream());
         xk1 = key_to_double(best);
     }
     return (xk + xk1) / 2.0;
@@ -560,8 +589,8 @@ void Graph::rescale_column(int col, double scaling) {
                             dTedge[INTRA].p, factor, 100 * scaling, wCount.p, stream));
     stats.launches++;
     int exact = 0;
-    PGC_CUDA(cudaMemcpyAsync(&exact, wCount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+    d2h(&exact, wCount.p, sizeof(int));
+    PGC_CUDA(sync_stream());
     f32Valid[col] = exact != 0;
     f32Known[col] = true;
 }
@@ -578,8 +607,8 @@ void Graph::ensure_f32(int col) {
                            dTedge[INTRA].p, wCount.p, stream));
     stats.launches++;
     int exact = 0;
-    PGC_CUDA(cudaMemcpyAsync(&exact, wCount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+    d2h(&exact, wCount.p, sizeof(int));
+    PGC_CUDA(sync_stream());
     f32Valid[col] = exact != 0;
     f32Known[col] = true;
 }
@@ -644,8 +673,11 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     r.threads = envThreads ? envThreads : kBfThreads;
     if (blocks == 1 && !envThreads) r.threads = std::min(kBfThreads, 32 * T.nslices);
     if (blocks <= 0) blocks = (T.nslices + r.threads / 32 - 1) / (r.threads / 32);
+    if (teamCap > 0 && !envBlocks) blocks = std::min(blocks, teamCap);
     blocks = std::max(1, std::min(blocks, T.nslices));
-    r.sharedTables = blocks == 1 && env_int("PGC_BF_SHARED_TABLES", 1) && tables <= smemCap;
+    if (blocks == 1 && !envThreads) r.threads = std::min(kBfThreads, 32 * T.nslices);
+    r.sharedTables = blocks == 1 && env_int("PGC_BF_SHARED_TABLES", 1) &&
+                     tables + bf_stage_offset(T.nslices) <= smemCap;
     if (blocks > 1) {
         int perSm = 0;
         PGC_CUDA(bf_max_coop_blocks(r.costF32, r.timeKind, r.threads, 0, &perSm));
@@ -831,19 +863,19 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     c.epoch = ctlEpoch;
     c.walkId = ctlWalkId;
     PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
-    cudaEvent_t e0, e1;
-    PGC_CUDA(cudaEventCreate(&e0));
-    PGC_CUDA(cudaEventCreate(&e1));
+    if (!timeEvents[0]) {
+        PGC_CUDA(cudaEventCreate(&timeEvents[0]));
+        PGC_CUDA(cudaEventCreate(&timeEvents[1]));
+    }
+    cudaEvent_t e0 = timeEvents[0], e1 = timeEvents[1];
     PGC_CUDA(cudaEventRecord(e0, stream));
     PGC_CUDA(launch_bf(p, r.costF32, r.timeKind, r.blocks, r.threads, r.coop, r.sharedTables, r.smemBytes, stream));
     PGC_CUDA(cudaEventRecord(e1, stream));
     stats.launches++;
-    PGC_CUDA(cudaMemcpyAsync(&c, wCtl.p, sizeof(Control), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+    d2h(&c, wCtl.p, sizeof(Control));
+    PGC_CUDA(sync_stream());
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     stats.deviceMs += ms;
     ctlEpoch = c.epoch;
     ctlWalkId = c.walkId;
@@ -871,8 +903,8 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
 std::vector<int> Graph::read_cycle_buffer(int len) {
     std::vector<int> out((size_t)std::max(0, len));
     if (len > 0)
-        PGC_CUDA(cudaMemcpyAsync(out.data(), wCycle.p, sizeof(int) * (size_t)len, cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(out.data(), wCycle.p, sizeof(int) * (size_t)len);
+    PGC_CUDA(sync_stream());
     return out;
 }
 
@@ -913,10 +945,10 @@ void Graph::lookup_pairs(const std::vector<int>& src, const std::vector<int>& tr
     a.tOut = wTOut.p;
     PGC_CUDA(launch_lookup_pairs(a, stream));
     stats.launches++;
-    PGC_CUDA(cudaMemcpyAsync(edges.data(), wEdgeOut.p, m * sizeof(long long), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaMemcpyAsync(c.data(), wCOut.p, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaMemcpyAsync(t.data(), wTOut.p, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+    d2h(edges.data(), wEdgeOut.p, m * sizeof(long long));
+    d2h(c.data(), wCOut.p, m * sizeof(double));
+    d2h(t.data(), wTOut.p, m * sizeof(double));
+    PGC_CUDA(sync_stream());
 }
 
 void Graph::rows_for_edges(const std::vector<long long>& edges) {
@@ -998,9 +1030,9 @@ void Graph::solve_ratio(int K) {
         PGC_CUDA(launch_layer1_mean(e64[0].p, T.layerStride(), T.entries[INTER], n, T.nslices, dSp[INTER].p,
                                     dSp[INTRA].p, dSrc[INTER].p, dSrc[INTRA].p, wMean.p, wCandStat.p, stream));
         stats.launches++;
-        PGC_CUDA(cudaMemcpyAsync(mean.data(), wMean.p, sizeof(float) * n, cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaMemcpyAsync(cnt.data(), wCandStat.p, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(mean.data(), wMean.p, sizeof(float) * n);
+        d2h(cnt.data(), wCandStat.p, sizeof(int) * n);
+        PGC_CUDA(sync_stream());
         float bestCost = std::numeric_limits<float>::infinity();
         int bestV = 0;
         for (int v = 0; v < n; ++v)
@@ -1210,8 +1242,8 @@ void Graph::solve_min_cost(int K) {
         PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
         PGC_CUDA(launch_extract_path(p, v, stream));
         stats.launches++;
-        PGC_CUDA(cudaMemcpyAsync(&c, wCtl.p, sizeof(Control), cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(&c, wCtl.p, sizeof(Control));
+        PGC_CUDA(sync_stream());
         if (c.status < 0) throw Failure(PGC_ERR_INTERNAL, "minimum-cost path extraction failed");
         return read_cycle_buffer(c.cycleLen);
     };
@@ -1256,8 +1288,8 @@ void Graph::solve_min_cost(int K) {
     // branch (dijkstra_solver.cpp:87-174)
     auto branch = [&](int newId) {
         std::vector<double> lb((size_t)n);
-        PGC_CUDA(cudaMemcpyAsync(lb.data(), wLb.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
-        PGC_CUDA(cudaStreamSynchronize(stream));
+        d2h(lb.data(), wLb.p, sizeof(double) * n);
+        PGC_CUDA(sync_stream());
         lowerBounds.clear();
         for (int v = 0; v < n; ++v)
             if (branchOf[(size_t)v] == branchId) lowerBounds.push_back({lb[(size_t)v], v});
@@ -1373,7 +1405,7 @@ void Graph::cost_vector(double* out) {
         PGC_CUDA(launch_export(e64[c].p, tmp.p, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
                                dTedge[INTER].p, dTedge[INTRA].p, stream));
     PGC_CUDA(cudaMemcpyAsync(out, tmp.p, sizeof(double) * (size_t)(rows * ncols), cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+    PGC_CUDA(sync_stream());
 }
 
 // Device address of the no-allocation export scratch on `device` (current).
@@ -1407,7 +1439,7 @@ void Graph::cost_vector_noalloc(double* out) {
         PGC_CUDA(launch_export(e64[c].p, scratch, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
                                dTedge[INTER].p, dTedge[INTRA].p, stream));
     PGC_CUDA(cudaMemcpyAsync(out, scratch, sizeof(double) * (size_t)values, cudaMemcpyDeviceToHost, stream));
-    PGC_CUDA(cudaStreamSynchronize(stream));
+    PGC_CUDA(sync_stream());
 }
 
 void Graph::product_space(int32_t* out) {
@@ -1654,6 +1686,54 @@ int pgc_solve_with_minimum_cost(pgc_graph* h, const char* solver, int max_depth)
         }
         PGC_CUDA(cudaSetDevice(g.device));
         g.solve_min_cost(K);
+    });
+}
+
+int pgc_set_team_cap(pgc_graph* h, int max_ctas) {
+    return guarded([&] {
+        if (!h || max_ctas < 0) throw Failure(PGC_ERR_ARG, "max_ctas must be >= 0");
+        h->g.teamCap = max_ctas;
+    });
+}
+
+int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver, int max_depth, int ctas_per_graph,
+                    int workers, int regenerate, int* status) {
+    return guarded([&] {
+        if (count < 0 || (count > 0 && (!graphs || !status))) throw Failure(PGC_ERR_ARG, "null argument");
+        const std::string name = solver ? solver : "";
+        const bool ratio = name == "lawlercpu" || name == "lawlergpu";
+        if (workers <= 0) workers = (int)std::min<int64_t>(count, 512);
+        workers = (int)std::min<int64_t>(workers, count);
+        std::atomic<int64_t> next{0};
+        std::vector<std::string> errors((size_t)count);
+        auto work = [&] {
+            for (;;) {
+                const int64_t i = next.fetch_add(1);
+                if (i >= count) return;
+                pgc_graph* h = graphs[i];
+                if (!h) {
+                    status[i] = PGC_ERR_ARG;
+                    continue;
+                }
+                const int saved = h->g.teamCap;
+                h->g.teamCap = ctas_per_graph > 0 ? ctas_per_graph : 1;
+                h->g.blockingSync = true;
+                status[i] = regenerate ? pgc_generate(h) : PGC_OK;
+                if (status[i] == PGC_OK)
+                    status[i] = ratio ? pgc_solve_with_cost_time_ratio(h, solver, max_depth)
+                                      : pgc_solve_with_minimum_cost(h, solver, max_depth);
+                if (status[i] != PGC_OK) errors[(size_t)i] = pgc_last_error();
+                h->g.teamCap = saved;
+                h->g.blockingSync = false;
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int w = 1; w < workers; ++w) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        for (int64_t i = 0; i < count; ++i)
+            if (status[i] != PGC_OK)
+                throw Failure(status[i], "graph " + std::to_string(i) + " of the batch failed: " + errors[(size_t)i]);
     });
 }
 

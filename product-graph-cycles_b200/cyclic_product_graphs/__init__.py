@@ -21,7 +21,7 @@ import os
 import numpy as np
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
-           "compute_local_thickness_2d", "library_path", "PGCError"]
+           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -61,6 +61,9 @@ _lib.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
 _lib.pgc_graph_info.argtypes = [_h, _lp]
 _lib.pgc_result_profile.argtypes = [_h, _lp]
 _lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
+_lib.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
+_lib.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
 _lib.pgc_last_error.restype = ctypes.c_char_p
 _lib.pgc_version.restype = ctypes.c_char_p
 
@@ -205,6 +208,10 @@ class product_graph_generator:
                 "inter_slots_per_layer", "intra_slots_per_layer", "cost_columns"]
         return dict(zip(keys, list(buf)))
 
+    def set_team_cap(self, max_ctas: int):
+        """Most CTAs a Bellman-Ford launch of this graph may use (0: no limit)."""
+        _check(_lib.pgc_set_team_cap(self._h, int(max_ctas)))
+
     def set_stream(self, cuda_stream: int | None):
         """Issue all device work of this generator on `cuda_stream` (a cudaStream_t as int)."""
         _check(_lib.pgc_set_stream(self._h, ctypes.c_void_p(cuda_stream) if cuda_stream else None))
@@ -215,6 +222,28 @@ class product_graph_generator:
         keys = ["bf_calls", "sweeps", "candidates", "lawler_iters", "branches", "fallback_walks", "device_us",
                 "kernel_launches"]
         return dict(zip(keys, list(buf)))
+
+
+def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas_per_graph: int = 1,
+                workers: int = 0, regenerate: bool = False):
+    """Solve many generators concurrently (no counterpart in the reference).
+
+    Each generator is solved as ``solve_with_cost_time_ratio`` (solver
+    ``"lawlercpu"``/``"lawlergpu"``) or ``solve_with_minimum_cost`` (any other
+    name) would, on its own CUDA stream with a Bellman-Ford team of at most
+    ``ctas_per_graph`` CTAs, by ``workers`` native threads (0: one per
+    generator, at most 512); with
+    ``regenerate`` each first recomputes its edge costs.  Returns the list of
+    ``(passes_layers_just_once, final_objective, matching)`` triples.
+    """
+    gens = list(generators)
+    if len(set(id(g) for g in gens)) != len(gens):
+        raise ValueError("solve_batch needs distinct generators")
+    arr = (_h * len(gens))(*[g._h for g in gens])
+    status = (ctypes.c_int * len(gens))()
+    _check(_lib.pgc_solve_batch(arr, len(gens), str(solver_name).encode(), -1 if max_depth is None else int(max_depth),
+                                int(ctas_per_graph), int(workers), int(bool(regenerate)), status))
+    return [g._result() for g in gens]
 
 
 def compute_normals_2d(V, E) -> np.ndarray:
