@@ -116,6 +116,26 @@ int pgc_solve_with_cost_time_ratio(pgc_graph* g, const char* solver_name, int ma
  * DijkstraSolver::run, dijkstra_solver.cpp:563-579. */
 int pgc_solve_with_minimum_cost(pgc_graph* g, const char* solver_name, int max_depth);
 
+/* No reference counterpart.  Adjoint of the last solve's objective with
+ * respect to feat_diff, for the plain product graph: adds (accumulate != 0)
+ * or writes grad_objective * d objective / d feat_diff into the DEVICE
+ * buffer grad_feat_diff [|VX| x |VY|] f64 of the handle's device.  Ratio:
+ * d lambda* / d c_e = 1[e in cycle] / T(cycle) over the rescaled costs;
+ * minimum cost: 1[e in cycle].  The rescale factor is held fixed and its
+ * rounding passed straight through; the energy's adjoint scatters every
+ * cycle edge into the two feat_diff entries its cost reads.  PGC_ERR_STATE
+ * without a result, PGC_ERR_MODE for the conjugate graph. */
+int pgc_backward_feat_diff(pgc_graph* g, double grad_objective, double* grad_feat_diff, int accumulate);
+
+/* No reference counterpart (the oracle's setCostVector).  Sets the edge costs
+ * [rows x cols] (rows = nY * edges per layer block, in edge-id order, cols 1
+ * or 2) in place of generate(); solves then use (and rescale) them. */
+int pgc_set_cost_vector(pgc_graph* g, const double* costs, int64_t rows, int64_t cols);
+
+/* No reference counterpart.  Replaces feat_diff [|VX| x |VY|]; the next solve
+ * regenerates the costs.  Lets one handle serve many training steps. */
+int pgc_set_feat_diff(pgc_graph* g, const double* feat_diff, int64_t rows, int64_t cols);
+
 /* No reference counterpart.  Most CTAs one Bellman-Ford launch of this graph
  * may use (0, the default: as many as shorten a step).  A small team is
  * slower per solve but leaves the rest of the GPU to other graphs. */

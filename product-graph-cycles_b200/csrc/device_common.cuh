@@ -233,6 +233,11 @@ constexpr long long kNoAllocExportValues = 1LL << 21;
 // Device address of the no-allocation export scratch on `device` (which must
 // be current); taken with cudaGetSymbolAddress on the first call, then cached.
 cudaError_t noalloc_export_scratch(int device, double** ptr);
+cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
+                                        double coef, double* grad, cudaStream_t s);
+cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,
+                          long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
+                          cudaStream_t s);
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s);

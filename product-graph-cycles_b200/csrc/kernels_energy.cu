@@ -73,6 +73,52 @@ __global__ void plain_energy_kernel(EnergyArgs a) {
     }
 }
 
+// Adjoint of plain_energy_kernel for the edges of a cycle: scatters
+// coef * d(cost)/d(feat_diff) of every listed product edge into grad
+// (|VX| x |VY|, row-major).  cost = 0.5 (fd[x0,y0] + fd[x1,y1]) li, or
+// fd[x0,y0] + fd[x1,y1] in the ("feature", "lengthnormalisation") mode,
+// whose time column li does not depend on feat_diff.  An edge listed twice
+// contributes twice.
+__global__ void plain_energy_backward_kernel(EnergyArgs a, const long long* edges, int count, long long eBlock,
+                                             double coef, double* grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long e = edges[i];
+    if (e < 0) return;
+    const int b = (int)(e / eBlock), t = (int)(e - (long long)b * eBlock);
+    if (b >= a.nY) return;
+    const int y0 = a.EY[2 * b];
+    const int y1 = a.eY[t] == 0 ? y0 : a.EY[2 * b + 1];
+    const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1];
+    const double li = a.lineIntegral ? line_integral(a, y0, y1, x0, x1) : 1.0;
+    const double d = a.lengthMode ? coef : coef * 0.5 * li;
+    atomicAdd(grad + (long long)x0 * a.nvy + y0, d);
+    atomicAdd(grad + (long long)x1 * a.nvy + y1, d);
+}
+
+// Inverse of export_kernel: column c of a [rows x cols] edge-ordered matrix
+// into the per-layer stream (empty slots get NaN).
+__global__ void import_kernel(const double* in, double* col, int cols, int c, long long total, long long layerStride,
+                              long long interEntries, int nY, long long eBlock, const int* tedgeInter,
+                              const int* tedgeIntra) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long l = idx / layerStride;
+        const long long pos = idx - l * layerStride;
+        long long block;
+        int t;
+        if (pos < interEntries) {
+            t = l < 1 ? -1 : tedgeInter[pos];
+            block = l - 1;
+        } else {
+            t = l >= nY ? -1 : tedgeIntra[pos - interEntries];
+            block = l;
+        }
+        col[idx] = t < 0 ? nan : in[(block * eBlock + t) * cols + c];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // SO(3) frame alignment (higherOrderDeformationEnergy.cpp:16-53, :95-134).
 // The reference takes R = U diag(1,1,det(UV^T)) V^T from the SVD of X^T Y.
@@ -505,6 +551,19 @@ cudaError_t noalloc_export_scratch(int device, double** ptr) {
     return cudaSuccess;
 }
 
+cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
+                                        double coef, double* grad, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    plain_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, grad);
+    return cudaGetLastError();
+}
+cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,
+                          long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
+                          cudaStream_t s) {
+    import_kernel<<<grid_for(total, 256), 256, 0, s>>>(in, col, cols, c, total, layerStride, interEntries, nY, eBlock,
+                                                       ti, tr);
+    return cudaGetLastError();
+}
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s) {

@@ -310,6 +310,20 @@ class Graph {
     void energy_changed() {
         f32Known[0] = f32Known[1] = false;
     }
+    EnergyArgs energy_args() const;
+
+    // What the adjoint of the last solve needs: the product of the rescale
+    // factors applied to each cost column since its costs were last set, the
+    // kind of the last result (0 none, 1 ratio, 2 minimum cost) and, for a
+    // ratio, the time sum T of its cycle.
+    double colScale[2] = {1.0, 1.0};
+    int adjKind = 0;
+    double adjT = 0;
+    DBuf<long long> wAdjEdges;
+    DBuf<double> wImport;
+    void backward_feat_diff(double grad, double* gradFd, bool accumulate);
+    void set_cost_vector(const double* in, int64_t rows, int64_t cols);
+    void set_feat_diff(const double* fd, int64_t rows, int64_t cols);
 
     // -------------------------------------------------------------------
     void solve_ratio(int K);
@@ -384,6 +398,30 @@ void Graph::upload_template() {
     templateReady = true;
 }
 
+// Graph-dependent fields of the energy kernels' arguments.
+EnergyArgs Graph::energy_args() const {
+    EnergyArgs a{};
+    a.n = T.n;
+    a.nY = T.nY;
+    a.nvx = (int)nvx;
+    a.nvy = (int)nvy;
+    a.interEntries = T.entries[INTER];
+    a.layerStride = T.layerStride();
+    a.total = (long long)(T.nY + 1) * a.layerStride;
+    a.tedgeInter = dTedge[INTER].p;
+    a.tedgeIntra = dTedge[INTRA].p;
+    a.eX = dEXcols.p;
+    a.eY = dEYpat.p;
+    a.eSrc = dESrc.p;
+    a.eTrgt = dETrgt.p;
+    a.eNext = dENext.p;
+    a.EY = dEY.p;
+    a.VX = dVX.p;
+    a.VY = dVY.p;
+    a.FD = dFD.p;
+    return a;
+}
+
 // ---------------------------------------------------------------------------
 // generate(): product_graph_generators.cpp:21-89
 // ---------------------------------------------------------------------------
@@ -396,25 +434,7 @@ void Graph::generate() {
 
     const long long stride = T.layerStride();
     const long long total = (long long)(T.nY + 1) * stride;
-    EnergyArgs a{};
-    a.n = T.n;
-    a.nY = T.nY;
-    a.nvx = (int)nvx;
-    a.nvy = (int)nvy;
-    a.interEntries = T.entries[INTER];
-    a.layerStride = stride;
-    a.total = total;
-    a.tedgeInter = dTedge[INTER].p;
-    a.tedgeIntra = dTedge[INTRA].p;
-    a.eX = dEXcols.p;
-    a.eY = dEYpat.p;
-    a.eSrc = dESrc.p;
-    a.eTrgt = dETrgt.p;
-    a.eNext = dENext.p;
-    a.EY = dEY.p;
-    a.VX = dVX.p;
-    a.VY = dVY.p;
-    a.FD = dFD.p;
+    EnergyArgs a = energy_args();
     if (!conj) {
         // deformationEnergy.cpp:97-103: two columns only for ("feature", "lengthnormalisation")
         const bool lengthMode = costName == "feature" && timeName == "lengthnormalisation";
@@ -474,6 +494,8 @@ void Graph::generate() {
     }
     PGC_CUDA(sync_stream());
     energy_changed();
+    colScale[0] = colScale[1] = 1.0;
+    adjKind = 0;
     generated = true;
 }
 
@@ -593,6 +615,7 @@ void Graph::rescale_column(int col, double scaling) {
     PGC_CUDA(sync_stream());
     f32Valid[col] = exact != 0;
     f32Known[col] = true;
+    colScale[col] *= factor;
 }
 
 void Graph::ensure_f32(int col) {
@@ -1167,6 +1190,9 @@ void Graph::solve_ratio(int K) {
     resPasses = true;
     resObjective = (float)fin.ratio;
     rows_for_edges(negativeCycle.edges);
+    adjKind = 1;
+    adjT = 0;
+    for (double t : negativeCycle.t) adjT += t;
     (void)wall0;
 }
 
@@ -1392,6 +1418,7 @@ void Graph::solve_min_cost(int K) {
     resPasses = loops < 2;
     resObjective = (float)upperBound;
     rows_for_edges(found);
+    adjKind = 2;
 }
 
 void Graph::cost_vector(double* out) {
@@ -1440,6 +1467,60 @@ void Graph::cost_vector_noalloc(double* out) {
                                dTedge[INTER].p, dTedge[INTRA].p, stream));
     PGC_CUDA(cudaMemcpyAsync(out, scratch, sizeof(double) * (size_t)values, cudaMemcpyDeviceToHost, stream));
     PGC_CUDA(sync_stream());
+}
+
+// Adjoint of the last solve's objective with respect to feat_diff (plain
+// graph).  Ratio: lambda* = C / T over the cycle's rescaled costs, so
+// d lambda* / d c_e = 1[e in cycle] / T; minimum cost: d / d c_e = 1[e in
+// cycle].  The rescale is taken with its factor fixed and its rounding passed
+// straight through (d c_scaled / d c = product of the factors applied), and
+// the energy's adjoint scatters into feat_diff (plain_energy_backward_kernel).
+void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
+    if (conj) throw Failure(PGC_ERR_MODE, "the feat_diff adjoint covers the plain product graph");
+    if (adjKind == 0 || !generated) throw Failure(PGC_ERR_STATE, "no ratio or minimum-cost result to differentiate");
+    double coef = grad * colScale[0];
+    if (adjKind == 1) coef /= adjT;
+    if (!accumulate) PGC_CUDA(cudaMemsetAsync(gradFd, 0, sizeof(double) * (size_t)(nvx * nvy), stream));
+    EnergyArgs a = energy_args();
+    a.lengthMode = costName == "feature" && timeName == "lengthnormalisation";
+    a.lineIntegral = reg || a.lengthMode;
+    wAdjEdges.upload(resEdges.data(), resEdges.size(), stream);
+    PGC_CUDA(launch_plain_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coef, gradFd, stream));
+    stats.launches++;
+    PGC_CUDA(sync_stream());
+}
+
+// The edge costs set directly ([rows x cols] in edge-id order), in place of
+// generate(); the next solve uses them as they are (and rescales them).
+void Graph::set_cost_vector(const double* in, int64_t rows, int64_t cols) {
+    if (!templateReady) upload_template();
+    if (rows != (int64_t)T.nY * T.eBlock || cols < 1 || cols > 2)
+        throw Failure(PGC_ERR_ARG, "cost vector must be [" + std::to_string((long long)T.nY * T.eBlock) +
+                                       " x 1|2], got [" + std::to_string(rows) + " x " + std::to_string(cols) + "]");
+    const long long stride = T.layerStride();
+    const long long total = (long long)(T.nY + 1) * stride;
+    wImport.upload(in, (size_t)(rows * cols), stream);
+    ncols = (int)cols;
+    for (int c = 0; c < ncols; ++c) {
+        e64[c].alloc((size_t)total);
+        PGC_CUDA(launch_import(wImport.p, e64[c].p, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
+                               dTedge[INTER].p, dTedge[INTRA].p, stream));
+    }
+    PGC_CUDA(sync_stream());
+    wImport.release();
+    energy_changed();
+    colScale[0] = colScale[1] = 1.0;
+    adjKind = 0;
+    generated = true;
+}
+
+// A new feature-difference matrix; the next solve regenerates the costs.
+void Graph::set_feat_diff(const double* fd, int64_t rows, int64_t cols) {
+    if (rows != nvx || cols != nvy) throw Failure(PGC_ERR_ARG, "feat_diff must be |VX| x |VY|");
+    FD.assign(fd, fd + rows * cols);
+    if (templateReady) dFD.upload(FD.data(), FD.size(), stream);
+    generated = false;
+    adjKind = 0;
 }
 
 void Graph::product_space(int32_t* out) {
@@ -1660,6 +1741,7 @@ int pgc_solve_with_cost_time_ratio(pgc_graph* h, const char* solver, int max_dep
             g.resCols = 1;
             g.resMatching.assign(4, 0);
             g.resEdges.clear();
+            g.adjKind = 0;
             return;
         }
         if (name != "lawlercpu" && name != "lawlergpu")
@@ -1682,10 +1764,35 @@ int pgc_solve_with_minimum_cost(pgc_graph* h, const char* solver, int max_depth)
             g.resCols = 1;
             g.resMatching.assign(4, 0);
             g.resEdges.clear();
+            g.adjKind = 0;
             return;
         }
         PGC_CUDA(cudaSetDevice(g.device));
         g.solve_min_cost(K);
+    });
+}
+
+int pgc_backward_feat_diff(pgc_graph* h, double grad_objective, double* grad_feat_diff, int accumulate) {
+    return guarded([&] {
+        if (!h || !grad_feat_diff) throw Failure(PGC_ERR_ARG, "null argument");
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.backward_feat_diff(grad_objective, grad_feat_diff, accumulate != 0);
+    });
+}
+
+int pgc_set_cost_vector(pgc_graph* h, const double* costs, int64_t rows, int64_t cols) {
+    return guarded([&] {
+        if (!h || !costs) throw Failure(PGC_ERR_ARG, "null argument");
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.set_cost_vector(costs, rows, cols);
+    });
+}
+
+int pgc_set_feat_diff(pgc_graph* h, const double* feat_diff, int64_t rows, int64_t cols) {
+    return guarded([&] {
+        if (!h || !feat_diff) throw Failure(PGC_ERR_ARG, "null argument");
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.set_feat_diff(feat_diff, rows, cols);
     });
 }
 

@@ -62,6 +62,9 @@ _lib.pgc_graph_info.argtypes = [_h, _lp]
 _lib.pgc_result_profile.argtypes = [_h, _lp]
 _lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
 _lib.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
+_lib.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
+_lib.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
+_lib.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
 _lib.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                  ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
 _lib.pgc_last_error.restype = ctypes.c_char_p
@@ -207,6 +210,25 @@ class product_graph_generator:
         keys = ["nodes_per_layer", "layers", "edges_per_block", "inter_edges_per_layer", "intra_edges_per_layer",
                 "inter_slots_per_layer", "intra_slots_per_layer", "cost_columns"]
         return dict(zip(keys, list(buf)))
+
+    def set_cost_vector(self, E):
+        """Set the edge costs [rows x 1|2] (edge-id order) in place of generate()."""
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        if E.ndim == 1:
+            E = E.reshape(-1, 1)
+        _check(_lib.pgc_set_cost_vector(self._h, E.ctypes.data_as(_dp), E.shape[0], E.shape[1]))
+
+    def set_feat_diff(self, feat_diff):
+        """Replace feat_diff (|VX| x |VY|); the next solve regenerates the costs."""
+        FD = np.ascontiguousarray(feat_diff, dtype=np.float64)
+        if FD.ndim != 2:
+            raise ValueError("feat_diff must be a 2-d matrix")
+        _check(_lib.pgc_set_feat_diff(self._h, FD.ctypes.data_as(_dp), FD.shape[0], FD.shape[1]))
+
+    def backward_feat_diff(self, grad_objective: float, grad_feat_diff_ptr: int, accumulate: bool = False):
+        """grad_objective * d(last objective)/d(feat_diff) into a device buffer (|VX| x |VY| float64)."""
+        _check(_lib.pgc_backward_feat_diff(self._h, float(grad_objective), ctypes.c_void_p(int(grad_feat_diff_ptr)),
+                                           int(bool(accumulate))))
 
     def set_team_cap(self, max_ctas: int):
         """Most CTAs a Bellman-Ford launch of this graph may use (0: no limit)."""

@@ -1,0 +1,122 @@
+"""Differentiable cycle objectives for PyTorch (no counterpart in the reference).
+
+The forward passes are the library's solves; the backward passes are the
+library's hand-written adjoint kernel (``pgc_backward_feat_diff``):
+
+* ratio: lambda* = C(C*) / T(C*) over the rescaled costs of the optimal
+  cycle C*, so d lambda*/d c_e = 1[e in C*] / T; the rescale factor is held
+  fixed and its rounding passed straight through;
+* minimum cost: d cost*/d c_e = 1[e in C*];
+
+and the plain energy's adjoint scatters every cycle edge into the two
+feat_diff entries it reads.  torch carries the gradient on from feat_diff
+(e.g. to learnable features).  ``BlackboxMinCostCycle`` implements blackbox
+interpolation (Vlastelica et al., ICLR 2020) over the edge costs: its
+backward solves again at w + tau * dL/dy and returns -(y(w) - y(w')) / tau.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import solve_batch
+
+
+def _as_host(fd: torch.Tensor) -> np.ndarray:
+    return fd.detach().to(device="cpu", dtype=torch.float64).contiguous().numpy()
+
+
+def _adjoint(gen, grad_out: torch.Tensor, like: torch.Tensor) -> torch.Tensor:
+    grad = torch.empty(like.shape, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    gen.backward_feat_diff(float(grad_out), grad.data_ptr())
+    return grad.to(device=like.device, dtype=like.dtype)
+
+
+class RatioCycleObjective(torch.autograd.Function):
+    """lambda*(feat_diff) of ``gen`` (a plain product_graph_generator whose
+    geometry and modes are set) by ``solve_with_cost_time_ratio``."""
+
+    @staticmethod
+    def forward(ctx, feat_diff, gen, max_depth=None):
+        gen.set_feat_diff(_as_host(feat_diff))
+        _, objective, _ = gen.solve_with_cost_time_ratio("lawlergpu", max_depth)
+        ctx.gen = gen
+        ctx.save_for_backward(feat_diff)
+        return torch.tensor(objective, dtype=feat_diff.dtype, device=feat_diff.device)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (feat_diff,) = ctx.saved_tensors
+        return _adjoint(ctx.gen, grad_out, feat_diff), None, None
+
+
+class MinCostCycleObjective(torch.autograd.Function):
+    """Cost of the minimum-cost cycle of ``gen`` as a function of feat_diff."""
+
+    @staticmethod
+    def forward(ctx, feat_diff, gen, max_depth=None):
+        gen.set_feat_diff(_as_host(feat_diff))
+        _, objective, _ = gen.solve_with_minimum_cost("dijkstragpu", max_depth)
+        ctx.gen = gen
+        ctx.save_for_backward(feat_diff)
+        return torch.tensor(objective, dtype=feat_diff.dtype, device=feat_diff.device)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (feat_diff,) = ctx.saved_tensors
+        return _adjoint(ctx.gen, grad_out, feat_diff), None, None
+
+
+class _BatchedRatio(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, gens, max_depth, *feat_diffs):
+        for g, fd in zip(gens, feat_diffs):
+            g.set_feat_diff(_as_host(fd))
+        results = solve_batch(gens, "lawlergpu", max_depth)
+        ctx.gens = gens
+        ctx.save_for_backward(*feat_diffs)
+        like = feat_diffs[0]
+        return torch.tensor([r[1] for r in results], dtype=like.dtype, device=like.device)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        fds = ctx.saved_tensors
+        return (None, None) + tuple(_adjoint(g, grad_out[i], fd) for i, (g, fd) in enumerate(zip(ctx.gens, fds)))
+
+
+def ratio_cycle_objectives(gens, feat_diffs, max_depth=None) -> torch.Tensor:
+    """lambda* of many pairs at once (one batched solve), differentiable in every feat_diff."""
+    return _BatchedRatio.apply(list(gens), max_depth, *feat_diffs)
+
+
+def cycle_indicator(gen, rows: int) -> np.ndarray:
+    """y[e] = how often product edge e is on the last returned cycle."""
+    y = np.zeros(rows, dtype=np.float64)
+    np.add.at(y, gen.last_cycle_edges(), 1.0)
+    return y
+
+
+class BlackboxMinCostCycle(torch.autograd.Function):
+    """y(w): the edge indicator of the minimum-cost cycle for edge costs w
+    ([rows] in edge-id order, set with ``set_cost_vector``).  Backward by
+    blackbox interpolation with step ``tau``: w' = w + tau * dL/dy,
+    dL/dw = -(y(w) - y(w')) / tau."""
+
+    @staticmethod
+    def forward(ctx, w, gen, tau=10.0, max_depth=None):
+        wh = _as_host(w)
+        gen.set_cost_vector(wh)
+        gen.solve_with_minimum_cost("dijkstragpu", max_depth)
+        y = cycle_indicator(gen, wh.shape[0])
+        ctx.gen, ctx.tau, ctx.max_depth, ctx.w, ctx.y = gen, float(tau), max_depth, wh, y
+        return torch.from_numpy(y).to(device=w.device, dtype=w.dtype)
+
+    @staticmethod
+    def backward(ctx, grad_y):
+        w2 = ctx.w + ctx.tau * _as_host(grad_y)
+        ctx.gen.set_cost_vector(w2)
+        ctx.gen.solve_with_minimum_cost("dijkstragpu", ctx.max_depth)
+        y2 = cycle_indicator(ctx.gen, w2.shape[0])
+        g = -(ctx.y - y2) / ctx.tau
+        return torch.from_numpy(g).to(device=grad_y.device, dtype=grad_y.dtype), None, None, None
