@@ -50,6 +50,11 @@ BATCHES = {
     # name: (pairs, |VX| range, |VY| range (even), k choices, feature dim)
     "batch_256_plain_1k8k": (256, (1000, 8000), (50, 250), (2, 3), 32),
 }
+# differentiation: forward (batched ratio solves) + backward (adjoint kernel) to learnable features
+FWDBWD = {
+    # name: (pairs, |VX|, |VY|, k, feature dim)
+    "fwdbwd_32_plain_2k_100_k2": (32, 2000, 100, 2, 64),
+}
 
 
 def _peaks():
@@ -533,13 +538,157 @@ def run_reference_batch(args):
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _fwdbwd_pairs(name, seed):
+    count, nv, m, k, dim = FWDBWD[name]
+    specs = [dict(nv=nv, m=m, k=k, dim=dim, seed=seed * 100000 + i) for i in range(count)]
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        pairs = pool.map(_fwdbwd_pair, specs)
+    return specs, pairs
+
+
+def _fwdbwd_pair(spec):
+    sys.path.insert(0, os.path.join(ROOT, "product-graph-cycles_b200"))
+    from cyclic_product_graphs import synthetic
+
+    p = synthetic.make_pair(n_vertices=spec["nv"], n_curve=spec["m"], feat_dim=spec["dim"], seed=spec["seed"],
+                            with_normals=False)
+    return {k: p[k] for k in ("VX", "EX", "VY", "EY", "feat_diff", "fX", "fY")}
+
+
+def run_fwdbwd(args, world, rank):
+    """Forward + backward: feat_diff = ||f_X - f_Y|| from learnable float32
+    features (torch), lambda* of every pair by one batched ratio solve, and
+    d(sum lambda*)/d features through the adjoint kernel and torch.  Also
+    timed: the same pairs one after the other with full-GPU teams (the plain
+    per-pair GPU Lawler, forward + backward)."""
+    specs, pairs = _fwdbwd_pairs(args.workload, args.seed + rank)
+    import numpy as np
+    import torch
+
+    import cyclic_product_graphs as cpg
+    from cyclic_product_graphs.autograd import RatioCycleObjective, ratio_cycle_objectives
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dev = torch.cuda.current_device()
+    k = specs[0]["k"]
+
+    def make(p):
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], False, False)
+        g.set_cost_time_ratio_mode("vanilla", "nomode")
+        return g
+
+    gens = [make(p) for p in pairs]
+    fX = [torch.tensor(p["fX"], device="cuda", requires_grad=True) for p in pairs]
+    fY = [torch.tensor(p["fY"], device="cuda", requires_grad=True) for p in pairs]
+
+    def step():
+        fds = [torch.cdist(a, b).double() for a, b in zip(fX, fY)]
+        lam = ratio_cycle_objectives(gens, fds, k)
+        lam.sum().backward()
+        return lam
+
+    def step_plain():
+        for g, a, b in zip(gens, fX, fY):
+            g.set_team_cap(0)
+            RatioCycleObjective.apply(torch.cdist(a, b).double(), g, k).backward()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(dev) as clocks:
+        for i in range(args.steps):
+            torch.cuda.synchronize()
+            ev[i][0].record(stream)
+            lam = step()
+            ev[i][1].record(stream)
+            torch.cuda.synchronize()
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
+    value = replica_throughput(len(gens) * args.steps, world, total_ms)
+    grads_ok = all(t.grad is not None and bool(torch.isfinite(t.grad).all()) for t in fX)
+
+    step_plain()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    step_plain()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_value = len(gens) / (e0.elapsed_time(e1) / 1000.0)
+
+    # end to end: host features -> device, fresh handles, forward + backward, gradients back to the host
+    h2d = sum(int(p[k2].nbytes) for p in pairs for k2 in ("VX", "EX", "VY", "EY", "fX", "fY"))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fresh = [make(p) for p in pairs]
+    ax = [torch.from_numpy(p["fX"]).pin_memory().to("cuda", non_blocking=True).requires_grad_(True) for p in pairs]
+    by = [torch.from_numpy(p["fY"]).pin_memory().to("cuda", non_blocking=True) for p in pairs]
+    lam_e = ratio_cycle_objectives(fresh, [torch.cdist(a, b).double() for a, b in zip(ax, by)], k)
+    lam_e.sum().backward()
+    host_grads = [a.grad.cpu() for a in ax]
+    e2e_s = time.perf_counter() - t0
+    d2h = sum(int(gr.numel() * gr.element_size()) for gr in host_grads) + 8 * len(pairs)
+
+    return {
+        "metric": METRIC, "value": value, "unit": "fwd+bwd pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 solve / fp32 features", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "pairs": len(gens), "vx": FWDBWD[args.workload][1],
+                   "vy": FWDBWD[args.workload][2], "k": k, "feature_dim": FWDBWD[args.workload][4],
+                   "parallelism": f"one stream + one CTA per pair, replicas x{world}",
+                   "l2": "per-pair streams of all pairs exceed L2"},
+        "vs_plain_gpu_lawler": {"plain_pairs_per_s": plain_value, "ratio": value / plain_value,
+                                "sample": "the same pairs, forward + backward one after the other, full-GPU teams"},
+        "e2e": {"value": world * len(pairs) / e2e_s, "unit": "fwd+bwd pairs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": 1},
+        "gradients_finite": grads_ok,
+        "mean_objective": float(lam.detach().mean()),
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+
+
+def run_reference_fwdbwd(args):
+    """The oracle's lawlercpu (forward) on one pair per step; the reference has no backward."""
+    specs, pairs = _fwdbwd_pairs(args.workload, args.seed)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    orc.set_threads(os.cpu_count() or 1)
+    samples = []
+    for i in range(args.warmup + args.steps):
+        p = pairs[i % len(pairs)]
+        o = orc.OracleGenerator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], False, False)
+        o.set_cost_time_ratio_mode("vanilla", "nomode")
+        t0 = time.perf_counter()
+        o.generate()
+        o.solve_with_cost_time_ratio("lawlercpu", specs[0]["k"])
+        if i >= args.warmup:
+            samples.append(time.perf_counter() - t0)
+    value = 1.0 / statistics.median(samples)
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "fwd+bwd pairs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload},
+            "cpu_baseline": {"value": value, "unit": "fwd+bwd pairs/s", "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": "oracle generate + lawlercpu of one pair per step (forward only: the "
+                                       "reference has no backward), median"},
+            "e2e": {"value": value, "unit": "fwd+bwd pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCHES), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(FWDBWD),
+                    default=DEFAULT_WORKLOAD)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sweeps", type=int, default=3)
@@ -549,7 +698,8 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            fn = run_reference_batch if args.workload in BATCHES else run_reference
+            fn = run_reference_batch if args.workload in BATCHES else run_reference_fwdbwd \
+                if args.workload in FWDBWD else run_reference
             print(json.dumps(fn(args)), flush=True)
         return
 
@@ -560,7 +710,12 @@ def main():
 
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = run_batch(args, world, rank) if args.workload in BATCHES else run_ours(args, world, rank)
+    if args.workload in BATCHES:
+        line = run_batch(args, world, rank)
+    elif args.workload in FWDBWD:
+        line = run_fwdbwd(args, world, rank)
+    else:
+        line = run_ours(args, world, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
