@@ -10,10 +10,26 @@
 
 #include <algorithm>
 #include <climits>
+#include <thread>
 
 namespace pgc {
 
 namespace {
+
+// Runs f(begin, end) over [0, n) split across the host's cores.
+template <class F>
+void parallel_for(int64_t n, F f) {
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 16), n / 2048));
+    if (parts <= 1) {
+        f((int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int64_t i = 1; i < parts; ++i) th.emplace_back(f, n * i / parts, n * (i + 1) / parts);
+    f((int64_t)0, n / parts);
+    for (auto& t : th) t.join();
+}
 
 struct EdgeOut {
     int src, trgt;
@@ -22,91 +38,146 @@ struct EdgeOut {
     int8_t y;
 };
 
-void emit(LayerTemplate& T, const EdgeOut& e) {
-    T.eSrc.push_back(e.src);
-    T.eTrgt.push_back(e.trgt);
-    T.eNext.push_back(e.next);
-    T.eX.push_back(e.x0);
-    T.eX.push_back(e.x1);
-    T.eX.push_back(e.x2);
-    T.eY.push_back(e.y);
-}
+// Writes template edges from position `at` on; the arrays are sized once
+// for the known count.
+struct Emitter {
+    LayerTemplate& T;
+    size_t at = 0;
+    Emitter(LayerTemplate& t, size_t count) : T(t) {
+        T.eSrc.resize(count);
+        T.eTrgt.resize(count);
+        T.eNext.resize(count);
+        T.eX.resize(3 * count);
+        T.eY.resize(count);
+    }
+    Emitter(LayerTemplate& t, size_t count, size_t from) : T(t), at(from) { (void)count; }
+    void operator()(const EdgeOut& e) {
+        T.eSrc[at] = e.src;
+        T.eTrgt[at] = e.trgt;
+        T.eNext[at] = e.next;
+        T.eX[3 * at] = e.x0;
+        T.eX[3 * at + 1] = e.x1;
+        T.eX[3 * at + 2] = e.x2;
+        T.eY[at] = e.y;
+        ++at;
+    }
+};
 
 void build_plain(const int* EX, int64_t nEX, LayerTemplate& T) {
+    Emitter emit(T, (size_t)(nEX * (T.prune ? 1 : 2) + T.nvx));
     for (int64_t j = 0; j < nEX; ++j) {
         const int a = EX[2 * j], b = EX[2 * j + 1];
-        if (!T.prune) emit(T, {a, b, 0, a, b, 0, Y_SS});
-        emit(T, {a, b, 1, a, b, 0, Y_SM});
+        if (!T.prune) emit({a, b, 0, a, b, 0, Y_SS});
+        emit({a, b, 1, a, b, 0, Y_SM});
     }
-    for (int x = 0; x < T.nvx; ++x) emit(T, {x, x, 1, x, x, 0, Y_SM});
+    for (int x = 0; x < T.nvx; ++x) emit({x, x, 1, x, x, 0, Y_SM});
 }
 
 void build_conj(const int* EX, int64_t nEX, LayerTemplate& T) {
-    std::vector<std::vector<int>> out((size_t)T.nvx);
-    for (int64_t e = 0; e < nEX; ++e) out[(size_t)EX[2 * e]].push_back((int)e);
+    // outgoing edges of every vertex in ascending edge id (CSR)
+    std::vector<int> outPtr((size_t)T.nvx + 1, 0), out((size_t)nEX);
+    for (int64_t e = 0; e < nEX; ++e) ++outPtr[(size_t)EX[2 * e] + 1];
+    for (int v = 0; v < T.nvx; ++v) outPtr[(size_t)v + 1] += outPtr[(size_t)v];
+    {
+        std::vector<int> fill(outPtr.begin(), outPtr.end() - 1);
+        for (int64_t e = 0; e < nEX; ++e) out[(size_t)fill[(size_t)EX[2 * e]]++] = (int)e;
+    }
+    // turns (j, it): edge it leaves the head of edge j and does not return to
+    // its tail.  Every edge j emits a fixed number of template edges per
+    // turn, so the offsets of all j are known up front and ranges of j are
+    // written in parallel.
+    std::vector<int64_t> turns((size_t)nEX + 1, 0);
+    parallel_for(nEX, [&](int64_t j0, int64_t j1) {
+        for (int64_t j = j0; j < j1; ++j) {
+            const int s3 = EX[2 * j], m3 = EX[2 * j + 1];
+            int c = 0;
+            for (int q = outPtr[(size_t)m3]; q < outPtr[(size_t)m3 + 1]; ++q)
+                if (EX[2 * out[(size_t)q] + 1] != s3) ++c;
+            turns[(size_t)j + 1] = c;
+        }
+    });
+    for (int64_t j = 0; j < nEX; ++j) turns[(size_t)j + 1] += turns[(size_t)j];
+    const int64_t allTurns = turns[(size_t)nEX];
+    const int perA = T.prune ? 0 : 2, perB = T.prune ? 2 : 3;
+    const size_t count = (size_t)((perA + perB) * allTurns + 2 * nEX);
+    Emitter sized(T, count);
     const int off2d = (int)nEX;
     const int off3d = T.prune ? off2d : 2 * (int)nEX;
-    if (!T.prune) {
-        for (int j = 0; j < (int)nEX; ++j) {
+    const size_t baseB = (size_t)(perA * allTurns);
+    parallel_for(nEX, [&](int64_t j0, int64_t j1) {
+        Emitter emitA(T, count, (size_t)(perA * turns[(size_t)j0]));
+        Emitter emitB(T, count, baseB + (size_t)(perB * turns[(size_t)j0] + 2 * j0));
+        for (int j = (int)j0; j < (int)j1; ++j) {
             const int s3 = EX[2 * j], m3 = EX[2 * j + 1];
-            for (int it : out[(size_t)m3]) {
+            for (int q = outPtr[(size_t)m3]; q < outPtr[(size_t)m3 + 1]; ++q) {
+                const int it = out[(size_t)q];
                 const int t3 = EX[2 * it + 1];
                 if (t3 == s3) continue;
-                emit(T, {off2d + j, off2d + it, 0, s3, m3, t3, Y_SSS});
-                emit(T, {off2d + j, it, 0, s3, m3, t3, Y_SSM});
+                if (!T.prune) {
+                    emitA({off2d + j, off2d + it, 0, s3, m3, t3, Y_SSS});
+                    emitA({off2d + j, it, 0, s3, m3, t3, Y_SSM});
+                }
+                emitB({j, it, 1, s3, m3, t3, Y_SMT});
+                if (!T.prune) emitB({j, off2d + it, 1, s3, m3, t3, Y_SMM});
+                emitB({off3d + j, it, 1, m3, m3, t3, Y_SMT});
             }
+            emitB({j, off3d + j, 1, s3, m3, m3, Y_SMT});
+            emitB({off3d + j, off3d + j, 1, m3, m3, m3, Y_SMT});
         }
-    }
-    for (int j = 0; j < (int)nEX; ++j) {
-        const int s3 = EX[2 * j], m3 = EX[2 * j + 1];
-        for (int it : out[(size_t)m3]) {
-            const int t3 = EX[2 * it + 1];
-            if (t3 == s3) continue;
-            emit(T, {j, it, 1, s3, m3, t3, Y_SMT});
-            if (!T.prune) emit(T, {j, off2d + it, 1, s3, m3, t3, Y_SMM});
-            emit(T, {off3d + j, it, 1, m3, m3, t3, Y_SMT});
-        }
-        emit(T, {j, off3d + j, 1, s3, m3, m3, Y_SMT});
-        emit(T, {off3d + j, off3d + j, 1, m3, m3, m3, Y_SMT});
-    }
+    });
 }
 
 void build_sell(LayerTemplate& T) {
     T.nslices = (T.n + 31) / 32;
-    for (int p = 0; p < 2; ++p) {
-        std::vector<std::vector<int>> lists((size_t)T.n);
-        for (int64_t t = 0; t < T.eBlock; ++t) {
-            const int part = T.eNext[(size_t)t] ? INTER : INTRA;
-            if (part != p) continue;
-            lists[(size_t)T.eTrgt[(size_t)t]].push_back((int)t);
+    const size_t n = (size_t)T.n;
+    T.ePos.assign((size_t)T.eBlock, -1);
+    auto part = [&](int p) {
+        // in-edges of every target in ascending template edge id (counting sort, stable)
+        std::vector<int> ptr(n + 1, 0), list;
+        for (int64_t t = 0; t < T.eBlock; ++t)
+            if ((T.eNext[(size_t)t] ? INTER : INTRA) == p) ++ptr[(size_t)T.eTrgt[(size_t)t] + 1];
+        for (size_t v = 0; v < n; ++v) ptr[v + 1] += ptr[v];
+        list.resize((size_t)ptr[n]);
+        {
+            std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+            for (int64_t t = 0; t < T.eBlock; ++t)
+                if ((T.eNext[(size_t)t] ? INTER : INTRA) == p) list[(size_t)fill[(size_t)T.eTrgt[(size_t)t]]++] = (int)t;
         }
         std::vector<int>& sp = T.sp[p];
         sp.assign((size_t)T.nslices + 1, 0);
         for (int s = 0; s < T.nslices; ++s) {
-            size_t w = 0;
+            int w = 0;
             for (int i = 0; i < 32; ++i) {
-                const int v = 32 * s + i;
-                if (v < T.n) w = std::max(w, lists[(size_t)v].size());
+                const size_t v = (size_t)(32 * s + i);
+                if (v < n) w = std::max(w, ptr[v + 1] - ptr[v]);
             }
-            sp[(size_t)s + 1] = sp[(size_t)s] + (int)w;
+            sp[(size_t)s + 1] = sp[(size_t)s] + w;
         }
         T.entries[p] = (int64_t)sp.back() * 32;
-        T.src[p].assign((size_t)T.entries[p], -1);
-        T.tedge[p].assign((size_t)T.entries[p], -1);
-        for (int s = 0; s < T.nslices; ++s) {
-            for (int i = 0; i < 32; ++i) {
-                const int v = 32 * s + i;
-                if (v >= T.n) continue;
-                const auto& L = lists[(size_t)v];
-                for (size_t j = 0; j < L.size(); ++j) {
-                    const size_t at = ((size_t)sp[(size_t)s] + j) * 32 + (size_t)i;
-                    T.src[p][at] = T.eSrc[(size_t)L[j]];
-                    T.tedge[p][at] = L[j];
-                    T.ePos[(size_t)L[j]] = (int)at | (p << 30);
+        T.src[p].resize((size_t)T.entries[p]);
+        T.tedge[p].resize((size_t)T.entries[p]);
+        parallel_for(T.nslices, [&](int64_t s0, int64_t s1) {
+            for (int64_t s = s0; s < s1; ++s) {
+                const size_t r0 = (size_t)sp[(size_t)s] * 32, r1 = (size_t)sp[(size_t)s + 1] * 32;
+                std::fill(T.src[p].begin() + r0, T.src[p].begin() + r1, -1);
+                std::fill(T.tedge[p].begin() + r0, T.tedge[p].begin() + r1, -1);
+                for (int i = 0; i < 32; ++i) {
+                    const size_t v = (size_t)(32 * s + i);
+                    if (v >= n) continue;
+                    for (int j = 0; j < ptr[v + 1] - ptr[v]; ++j) {
+                        const int t = list[(size_t)(ptr[v] + j)];
+                        const size_t at = r0 + (size_t)j * 32 + (size_t)i;
+                        T.src[p][at] = T.eSrc[(size_t)t];
+                        T.tedge[p][at] = t;
+                        T.ePos[(size_t)t] = (int)at | (p << 30);
+                    }
                 }
             }
-        }
-    }
+        });
+    };
+    std::thread other(part, 1);
+    part(0);
+    other.join();
     // The closing layer takes the INTER edges of block nY-1 whose global
     // source id is strictly greater than n (cost_time_ratio_solver.cpp:56);
     // with two layers that drops the edges leaving node 0 of layer 1.
@@ -145,7 +216,6 @@ std::string build_template(const int* EX, int64_t nEX, const int* EY, int64_t nE
         build_plain(EX, nEX, T);
     }
     T.eBlock = (int64_t)T.eSrc.size();
-    T.ePos.assign((size_t)T.eBlock, -1);
     build_sell(T);
     (void)EY;
     return "";

@@ -314,7 +314,7 @@ __device__ __forceinline__ void stage_drain(Stage& st) {
 // it.  The winner's origin and path length are read once per node after the
 // fold.  Returns whether this thread improved a node.
 // ---------------------------------------------------------------------------
-constexpr int kGather = 16;
+constexpr int kGather = 20;
 
 struct StepView {
     const int* src;     // source index per entry, from the step's first row
