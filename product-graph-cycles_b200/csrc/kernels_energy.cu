@@ -304,35 +304,61 @@ __device__ __forceinline__ unsigned long long order_key(double x) {
 }
 
 
-__device__ __forceinline__ bool entry_valid(const SelectArgs& a, long long idx) {
-    const long long l = idx / a.layerStride;
-    const long long pos = idx - l * a.layerStride;
-    if (pos < a.interEntries) return l >= 1 && a.tedgeInter[pos] >= 0;
-    return l < a.nY && a.tedgeIntra[pos - a.interEntries] >= 0;
+// Visits the per-layer streams in work items of consecutive positions of one
+// layer (one division per item, not per entry): f(idx, valid, inRange) for
+// every position; `valid` marks a real edge (l >= 1 for interlayer entries,
+// l < nY for intralayer ones, template edge >= 0).  Positions are visited
+// warp-aligned, so every lane of a warp makes the same calls (warp
+// collectives inside f are allowed); lanes past the item's end get
+// inRange = false.
+template <class F>
+__device__ __forceinline__ void for_stream_entries(long long layerStride, long long interEntries, int nY,
+                                                   const int* ti, const int* tr, F f) {
+    const long long chunk = 8LL * blockDim.x;
+    const long long perLayer = (layerStride + chunk - 1) / chunk;
+    const long long items = perLayer * (nY + 1);
+    const int lane = threadIdx.x & 31;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const long long l = it / perLayer;
+        const long long p0 = (it - l * perLayer) * chunk;
+        const long long p1 = p0 + chunk < layerStride ? p0 + chunk : layerStride;
+        for (long long pos = p0 + threadIdx.x; pos - lane < p1; pos += blockDim.x) {
+            const bool inRange = pos < p1;
+            bool valid = false;
+            if (inRange) {
+                const int t = pos < interEntries ? (l >= 1 ? ti[pos] : -1) : (l < nY ? tr[pos - interEntries] : -1);
+                valid = t >= 0;
+            }
+            f(l * layerStride + pos, valid, inRange);
+        }
+    }
 }
 
 // Histogram of the next digit of the keys that match the current prefix.
 // Costs cluster in a few digit values (equal exponents, repeated integers),
 // so lanes holding the same digit are combined with __match_any_sync before
-// one of them updates the block's shared-memory counter.
+// one of them updates the block's shared-memory counter.  A small persistent
+// grid keeps the final flush of the block histograms short.
 __global__ void select_hist_kernel(SelectArgs a) {
     extern __shared__ unsigned int sh[];
     const int nb = 1 << a.bits;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    for (long long base = gw * 32; base < a.total; base += warps * 32) {
-        const long long idx = base + lane;
-        unsigned bin = 0xffffffffu;
-        if (idx < a.total && entry_valid(a, idx)) {
-            const unsigned long long k = order_key(a.col[idx]);
-            if ((k & a.prefixMask) == a.prefix) bin = (unsigned)((k >> a.shift) & (unsigned long long)(nb - 1));
-        }
-        const unsigned peers = __match_any_sync(0xffffffffu, bin);
-        if (bin != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&sh[bin], (unsigned)__popc(peers));
-    }
+    for_stream_entries(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                       [&](long long idx, bool valid, bool inRange) {
+                           // the value is loaded whether or not the slot is an
+                           // edge (empty slots hold NaN), so both loads overlap
+                           const double x = inRange ? a.col[idx] : 0.0;
+                           unsigned bin = 0xffffffffu;
+                           if (valid) {
+                               const unsigned long long k = order_key(x);
+                               if ((k & a.prefixMask) == a.prefix)
+                                   bin = (unsigned)((k >> a.shift) & (unsigned long long)(nb - 1));
+                           }
+                           const unsigned peers = __match_any_sync(0xffffffffu, bin);
+                           if (bin != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&sh[bin], (unsigned)__popc(peers));
+                       });
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x)
         if (sh[i]) atomicAdd(a.hist + i, (unsigned long long)sh[i]);
@@ -340,25 +366,25 @@ __global__ void select_hist_kernel(SelectArgs a) {
 
 // Copies the values whose key matches (prefix, prefixMask) to out[0..cap).
 __global__ void select_compact_kernel(SelectArgs a, double* out, unsigned long long* count, long long cap) {
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        if (!entry_valid(a, idx)) continue;
-        const double x = a.col[idx];
-        if ((order_key(x) & a.prefixMask) != a.prefix) continue;
-        const unsigned long long at = atomicAdd(count, 1ull);
-        if ((long long)at < cap) out[at] = x;
-    }
+    for_stream_entries(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                       [&](long long idx, bool valid, bool inRange) {
+                           const double x = inRange ? a.col[idx] : 0.0;
+                           if (!valid || (order_key(x) & a.prefixMask) != a.prefix) return;
+                           const unsigned long long at = atomicAdd(count, 1ull);
+                           if ((long long)at < cap) out[at] = x;
+                       });
 }
 
 // Smallest key strictly greater than `above` (all bits); *out starts at ~0.
 __global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, unsigned long long* out) {
     unsigned long long best = ~0ull;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        if (!entry_valid(a, idx)) continue;
-        const unsigned long long k = order_key(a.col[idx]);
-        if (k > above && k < best) best = k;
-    }
+    for_stream_entries(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                       [&](long long idx, bool valid, bool inRange) {
+                           const double x = inRange ? a.col[idx] : 0.0;
+                           if (!valid) return;
+                           const unsigned long long k = order_key(x);
+                           if (k > above && k < best) best = k;
+                       });
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
         best = x < best ? x : best;
@@ -371,50 +397,41 @@ __global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, 
 __global__ void rescale_kernel(double* col, float* col32, long long total, long long layerStride,
                                long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
                                double factor, double clip, int* exact) {
-    SelectArgs a{};
-    a.layerStride = layerStride;
-    a.interEntries = interEntries;
-    a.nY = nY;
-    a.tedgeInter = tedgeInter;
-    a.tedgeIntra = tedgeIntra;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        if (!entry_valid(a, idx)) {
-            if (col32) col32[idx] = __int_as_float(0x7fc00000);
-            continue;
-        }
-        double x = round(factor * col[idx]);
-        if (x > clip) x = clip;
-        col[idx] = x;
-        const float f = (float)x;
-        if (col32) col32[idx] = f;
-        if ((double)f != x) *exact = 0;
-    }
+    (void)total;
+    for_stream_entries(layerStride, interEntries, nY, tedgeInter, tedgeIntra,
+                       [&](long long idx, bool valid, bool inRange) {
+                           if (!inRange) return;
+                           const double v = col[idx];
+                           if (!valid) {
+                               if (col32) col32[idx] = __int_as_float(0x7fc00000);
+                               return;
+                           }
+                           double x = round(factor * v);
+                           if (x > clip) x = clip;
+                           col[idx] = x;
+                           const float f = (float)x;
+                           if (col32) col32[idx] = f;
+                           if ((double)f != x) *exact = 0;
+                       });
 }
-
 __global__ void to_f32_kernel(const double* col, float* col32, long long total, long long layerStride,
                               long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
                               int* exact) {
-    SelectArgs a{};
-    a.layerStride = layerStride;
-    a.interEntries = interEntries;
-    a.nY = nY;
-    a.tedgeInter = tedgeInter;
-    a.tedgeIntra = tedgeIntra;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        if (!entry_valid(a, idx)) {
-            col32[idx] = __int_as_float(0x7fc00000);
-            continue;
-        }
-        const double x = col[idx];
-        const float f = (float)x;
-        col32[idx] = f;
-        if ((double)f != x) *exact = 0;
-    }
+    (void)total;
+    for_stream_entries(layerStride, interEntries, nY, tedgeInter, tedgeIntra,
+                       [&](long long idx, bool valid, bool inRange) {
+                           if (!inRange) return;
+                           const double x = col[idx];
+                           if (!valid) {
+                               col32[idx] = __int_as_float(0x7fc00000);
+                               return;
+                           }
+                           const float f = (float)x;
+                           col32[idx] = f;
+                           if ((double)f != x) *exact = 0;
+                       });
 }
 
-// Scatter a stream column to edge-id order: out[e * cols + c].
 __global__ void export_kernel(const double* col, double* out, int cols, int c, long long total,
                               long long layerStride, long long interEntries, int nY, long long eBlock,
                               const int* tedgeInter, const int* tedgeIntra) {
@@ -467,6 +484,19 @@ __global__ void layer1_mean_kernel(const double* cost, long long layerStride, lo
 }
 
 // Host wrappers -------------------------------------------------------------
+// Persistent grid of a stream pass: as many CTAs as can be resident at once
+// (one full wave; a partial second wave would double the pass).
+template <class K>
+static int stream_grid(K kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) {
+        cudaGetLastError();
+        return 148;
+    }
+    return sms * per;
+}
+
 static int grid_for(long long total, int threads) {
     long long b = (total + threads - 1) / threads;
     if (b > 148LL * 32) b = 148LL * 32;
@@ -487,29 +517,30 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
-    select_hist_kernel<<<grid_for(a.total, 512), 512, (1 << a.bits) * sizeof(unsigned), s>>>(a);
+    select_hist_kernel<<<stream_grid(select_hist_kernel, 512, (1 << a.bits) * sizeof(unsigned)), 512,
+                         (1 << a.bits) * sizeof(unsigned), s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,
                                   cudaStream_t s) {
-    select_compact_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a, out, count, cap);
+    select_compact_kernel<<<stream_grid(select_compact_kernel, 256, 0), 256, 0, s>>>(a, out, count, cap);
     return cudaGetLastError();
 }
 cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long above, unsigned long long* out,
                                     cudaStream_t s) {
-    select_min_above_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a, above, out);
+    select_min_above_kernel<<<stream_grid(select_min_above_kernel, 256, 0), 256, 0, s>>>(a, above, out);
     return cudaGetLastError();
 }
 cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
                            int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
                            cudaStream_t s) {
-    rescale_kernel<<<grid_for(total, 256), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
+    rescale_kernel<<<stream_grid(rescale_kernel, 256, 0), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
                                                         factor, clip, exact);
     return cudaGetLastError();
 }
 cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,
                           long long interEntries, int nY, const int* ti, const int* tr, int* exact, cudaStream_t s) {
-    to_f32_kernel<<<grid_for(total, 256), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
+    to_f32_kernel<<<stream_grid(to_f32_kernel, 256, 0), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
                                                        exact);
     return cudaGetLastError();
 }
