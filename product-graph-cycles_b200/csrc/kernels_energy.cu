@@ -23,21 +23,6 @@ namespace pgc {
 
 enum HoMode { NOMODE = 0, VANILLA, FEATURE, LENGTH, SO3_PLAIN, SO3_ROBUST, PENALISE_DEGENERATE };
 
-__device__ __forceinline__ bool entry_edge(const EnergyArgs& a, long long idx, int& block, int& tedge) {
-    const long long l = idx / a.layerStride;
-    const long long pos = idx - l * a.layerStride;
-    if (pos < a.interEntries) {
-        if (l < 1) return false;
-        tedge = a.tedgeInter[pos];
-        block = (int)(l - 1);
-    } else {
-        if (l >= a.nY) return false;
-        tedge = a.tedgeIntra[pos - a.interEntries];
-        block = (int)l;
-    }
-    return tedge >= 0;
-}
-
 __device__ __forceinline__ double line_integral(const EnergyArgs& a, int y0, int y1, int x0, int x1) {
     double li = 0.0;
     for (int j = 0; j < 3; ++j) {
@@ -49,28 +34,62 @@ __device__ __forceinline__ double line_integral(const EnergyArgs& a, int y0, int
     return sqrt(li);
 }
 
-__global__ void plain_energy_kernel(EnergyArgs a) {
-    const double nan = __longlong_as_double(0x7ff8000000000000LL);
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int b, t;
-        if (!entry_edge(a, idx, b, t)) {
-            a.out0[idx] = nan;
-            if (a.out1) a.out1[idx] = nan;
-            continue;
-        }
-        const int y0 = a.EY[2 * b];
-        const int y1 = a.eY[t] == 0 ? y0 : a.EY[2 * b + 1];
-        const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1];
-        const double li = a.lineIntegral ? line_integral(a, y0, y1, x0, x1) : 1.0;
-        const double fd = a.FD[(long long)x0 * a.nvy + y0] + a.FD[(long long)x1 * a.nvy + y1];
-        if (a.lengthMode) {
-            a.out0[idx] = fd;
-            a.out1[idx] = li;
-        } else {
-            a.out0[idx] = 0.5 * fd * li;
+// Visits the per-layer streams in work items of consecutive positions of one
+// layer (one division per item, not per entry): f(idx, valid, inRange) for
+// every position; `valid` marks a real edge (l >= 1 for interlayer entries,
+// l < nY for intralayer ones, template edge >= 0).  Positions are visited
+// warp-aligned, so every lane of a warp makes the same calls (warp
+// collectives inside f are allowed); lanes past the item's end get
+// inRange = false.
+template <class F>
+__device__ __forceinline__ void for_stream_layers(long long layerStride, long long interEntries, int nY,
+                                                  const int* ti, const int* tr, F f) {
+    const long long chunk = 8LL * blockDim.x;
+    const long long perLayer = (layerStride + chunk - 1) / chunk;
+    const long long items = perLayer * (nY + 1);
+    const int lane = threadIdx.x & 31;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const long long l = it / perLayer;
+        const long long p0 = (it - l * perLayer) * chunk;
+        const long long p1 = p0 + chunk < layerStride ? p0 + chunk : layerStride;
+        for (long long pos = p0 + threadIdx.x; pos - lane < p1; pos += blockDim.x) {
+            const bool inRange = pos < p1;
+            int t = -1;
+            if (inRange) t = pos < interEntries ? (l >= 1 ? ti[pos] : -1) : (l < nY ? tr[pos - interEntries] : -1);
+            f(l * layerStride + pos, (int)l, pos, t, inRange);
         }
     }
+}
+template <class F>
+__device__ __forceinline__ void for_stream_entries(long long layerStride, long long interEntries, int nY,
+                                                   const int* ti, const int* tr, F f) {
+    for_stream_layers(layerStride, interEntries, nY, ti, tr,
+                      [&](long long idx, int, long long, int t, bool inRange) { f(idx, t >= 0, inRange); });
+}
+
+__global__ void plain_energy_kernel(EnergyArgs a) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for_stream_layers(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                      [&](long long idx, int l, long long pos, int t, bool inRange) {
+                          if (!inRange) return;
+                          if (t < 0) {
+                              a.out0[idx] = nan;
+                              if (a.out1) a.out1[idx] = nan;
+                              return;
+                          }
+                          const int b = pos < a.interEntries ? l - 1 : l;
+                          const int y0 = a.EY[2 * b];
+                          const int y1 = a.eY[t] == 0 ? y0 : a.EY[2 * b + 1];
+                          const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1];
+                          const double li = a.lineIntegral ? line_integral(a, y0, y1, x0, x1) : 1.0;
+                          const double fd = a.FD[(long long)x0 * a.nvy + y0] + a.FD[(long long)x1 * a.nvy + y1];
+                          if (a.lengthMode) {
+                              a.out0[idx] = fd;
+                              a.out1[idx] = li;
+                          } else {
+                              a.out0[idx] = 0.5 * fd * li;
+                          }
+                      });
 }
 
 // Adjoint of plain_energy_kernel for the edges of a cycle: scatters
@@ -235,14 +254,18 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     const double twoPi = 2 * 3.14159265358979323846;
     const bool needLi = (a.costMode == LENGTH || a.timeMode == LENGTH);
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < a.total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int b, t;
-        if (!entry_edge(a, idx, b, t)) {
+    // Without quaternions every SO(3) distance is 0: its robust loss is the
+    // same number for every edge, computed once per thread by the same code.
+    const double rl0 = robust_loss(a, 0.0);
+    for_stream_layers(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                      [&](long long idx, int l, long long pos, int t, bool inRange) {
+        if (!inRange) return;
+        if (t < 0) {
             a.out0[idx] = nan;
             if (a.out1) a.out1[idx] = nan;
-            continue;
+            return;
         }
+        const int b = pos < a.interEntries ? l - 1 : l;
         const int s2 = a.EY[2 * b], m2 = a.EY[2 * b + 1], t2 = a.EY[2 * ((b + 1) % a.nY) + 1];
         int y0, y1, y2;
         switch (a.eY[t]) {
@@ -258,20 +281,21 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
             const long long q1 = (long long)((b + a.eNext[t]) % a.nY) * a.n + a.eTrgt[t];
             so3 = so3_distance(a.quat[q0], a.quat[q1]);
         }
+        const double rl = a.quat ? robust_loss(a, so3) : rl0;
         const double fd = a.FD[(long long)x2 * a.nvy + y2];
         const double li = needLi ? line_integral(a, y0, y1, x0, x1) : 0.0;
         const bool degenerate = (y2 == y1 || x2 == x1);
         const int cm = a.costMode, tm = a.timeMode;
         double c0 = 0, c1 = 0;
         if (cm == VANILLA && tm == VANILLA) {
-            c0 = robust_loss(a, so3) + fd;
+            c0 = rl + fd;
         } else if (cm == VANILLA && tm == LENGTH) {
-            c0 = robust_loss(a, so3) + fd;
+            c0 = rl + fd;
             c1 = li;
         } else if (cm == LENGTH && tm == VANILLA) {
             c0 = li;
         } else if (cm == VANILLA && tm == PENALISE_DEGENERATE) {
-            c0 = robust_loss(a, so3) + fd;
+            c0 = rl + fd;
             c1 = degenerate ? 0.1 : 1;
         } else if (cm == PENALISE_DEGENERATE && tm == VANILLA) {
             c0 = degenerate ? 0.1 : 1;
@@ -280,9 +304,9 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
             c1 = fmax(0.0, twoPi - so3);
         } else if (cm == FEATURE && tm == SO3_ROBUST) {
             c0 = fd;
-            c1 = fmax(0.0, a.maxSO3 - robust_loss(a, so3));
+            c1 = fmax(0.0, a.maxSO3 - rl);
         } else if (cm == SO3_ROBUST && tm == FEATURE) {
-            c0 = robust_loss(a, so3);
+            c0 = rl;
             c1 = fmax(0.0, a.maxFd - fd);
         } else {  // SO3_PLAIN, FEATURE
             c0 = so3;
@@ -290,7 +314,7 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
         }
         a.out0[idx] = c0;
         if (a.out1) a.out1[idx] = c1;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -303,36 +327,6 @@ __device__ __forceinline__ unsigned long long order_key(double x) {
     return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
 }
 
-
-// Visits the per-layer streams in work items of consecutive positions of one
-// layer (one division per item, not per entry): f(idx, valid, inRange) for
-// every position; `valid` marks a real edge (l >= 1 for interlayer entries,
-// l < nY for intralayer ones, template edge >= 0).  Positions are visited
-// warp-aligned, so every lane of a warp makes the same calls (warp
-// collectives inside f are allowed); lanes past the item's end get
-// inRange = false.
-template <class F>
-__device__ __forceinline__ void for_stream_entries(long long layerStride, long long interEntries, int nY,
-                                                   const int* ti, const int* tr, F f) {
-    const long long chunk = 8LL * blockDim.x;
-    const long long perLayer = (layerStride + chunk - 1) / chunk;
-    const long long items = perLayer * (nY + 1);
-    const int lane = threadIdx.x & 31;
-    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
-        const long long l = it / perLayer;
-        const long long p0 = (it - l * perLayer) * chunk;
-        const long long p1 = p0 + chunk < layerStride ? p0 + chunk : layerStride;
-        for (long long pos = p0 + threadIdx.x; pos - lane < p1; pos += blockDim.x) {
-            const bool inRange = pos < p1;
-            bool valid = false;
-            if (inRange) {
-                const int t = pos < interEntries ? (l >= 1 ? ti[pos] : -1) : (l < nY ? tr[pos - interEntries] : -1);
-                valid = t >= 0;
-            }
-            f(l * layerStride + pos, valid, inRange);
-        }
-    }
-}
 
 // Histogram of the next digit of the keys that match the current prefix.
 // Costs cluster in a few digit values (equal exponents, repeated integers),
@@ -505,11 +499,11 @@ static int grid_for(long long total, int threads) {
 }
 
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s) {
-    plain_energy_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a);
+    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, 0), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
-    ho_energy_kernel<<<grid_for(a.total, 256), 256, 0, s>>>(a);
+    ho_energy_kernel<<<stream_grid(ho_energy_kernel, 256, 0), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
