@@ -57,15 +57,6 @@ struct Control {
     int anyFinite;
 };
 
-// One (node, depth) entry of a layer's DP rows: the path value and, for the
-// stored path, its origin (the layer-0 start node it leaves from, or a
-// kLap* code) and its length in predecessor steps back to that origin.
-struct __align__(16) DPE {
-    double v;
-    int o;
-    int h;
-};
-
 struct BfParams {
     // graph
     int n, nY, K, Kp, nslices;
@@ -80,7 +71,8 @@ struct BfParams {
     const void* time;              // same layout, or nullptr for a constant time
     double tconst;
     // state
-    DPE* dp;                       // [2][n][Kp] distance + origin of every (node, depth) of two layers
+    double* dv;                    // [2][n][Kp] path value of every (node, depth) of two layers
+    int2* doh;                     // [2][n][Kp] its path's origin (layer-0 start node or kLap* code) and length
     double* bak;                   // [n]
     int* pred;                     // [(nY+1)*K*n], expanded index layer*n*K + k*n + v
     const int* ctaSlice;           // [ncta+1] slice range of every CTA (both parts)
@@ -195,7 +187,7 @@ constexpr int kBfThreads = 640;
 // Bytes of shared memory a single-CTA launch needs to keep its DP records
 // and backup row on chip (128-byte aligned).
 __host__ __device__ inline size_t bf_shared_table_bytes(int n, int Kp) {
-    const size_t b = (size_t)2 * n * Kp * sizeof(DPE) + (size_t)n * sizeof(double);
+    const size_t b = (size_t)2 * n * Kp * (sizeof(double) + sizeof(int2)) + (size_t)n * sizeof(double);
     return (b + 127) & ~(size_t)127;
 }
 // Offset of the first step buffer after the staged row offsets (128-byte aligned).

@@ -169,31 +169,62 @@ __device__ __forceinline__ int original_index(int n, int K, int e) {
     return rem - depth * n + layer * n;
 }
 
-// DP record loads: from shared memory when the whole team is one CTA that
-// keeps its tables there (S), else through L2 (other CTAs write the records
-// during the launch, so L1 must not serve stale lines).
+// DP record access by record index parity * n * Kp + node * Kp + depth: the
+// value lives in p.dv, the path origin and length in p.doh.  Loads come from
+// shared memory when the whole team is one CTA that keeps its tables there
+// (S), else through L2 (other CTAs write the records during the launch, so
+// L1 must not serve stale lines).
+struct DpRec {
+    double v;
+    int o, h;
+};
 template <bool S>
-__device__ __forceinline__ DPE ldE(const DPE* p) {
-    double2 x;
-    if constexpr (S) x = *reinterpret_cast<const double2*>(p);
-    else x = __ldcg(reinterpret_cast<const double2*>(p));
-    DPE e;
-    e.v = x.x;
-    const long long b = __double_as_longlong(x.y);
-    e.o = (int)(unsigned)(b & 0xffffffffLL);
-    e.h = (int)(b >> 32);
-    return e;
+__device__ __forceinline__ double ldV(const BfParams& p, size_t r) {
+    if constexpr (S) return p.dv[r];
+    else return __ldcg(p.dv + r);
 }
 template <bool S>
-__device__ __forceinline__ double ldV(const DPE* p) {
-    if constexpr (S) return p->v;
-    else return __ldcg(&p->v);
+__device__ __forceinline__ DpRec ldE(const BfParams& p, size_t r) {
+    int2 oh;
+    if constexpr (S) oh = p.doh[r];
+    else oh = __ldcg(p.doh + r);
+    return DpRec{ldV<S>(p, r), oh.x, oh.y};
 }
-__device__ __forceinline__ void stE(DPE* p, double v, int o, int h) {
-    double2 x;
-    x.x = v;
-    x.y = __longlong_as_double(((long long)h << 32) | (long long)(unsigned)o);
-    *reinterpret_cast<double2*>(p) = x;
+__device__ __forceinline__ void stE(const BfParams& p, size_t r, double v, int o, int h) {
+    p.dv[r] = v;
+    p.doh[r] = make_int2(o, h);
+}
+
+// The NK values of consecutive depths starting at `rec` (a node's row of
+// Kp values: 16-byte aligned for Kp = 2, 32-byte aligned for Kp = 4) in one
+// vector load: 8, 16 or 32 bytes, one sector of L2 per source.  NK = 3 reads
+// the row's fourth value too and ignores it.
+template <bool S, int NK>
+__device__ __forceinline__ void ld_row(const double* rec, double (&d)[NK]) {
+    if constexpr (NK == 1) {
+        d[0] = S ? rec[0] : __ldcg(rec);
+    } else if constexpr (NK == 2) {
+        const double2 x = S ? *reinterpret_cast<const double2*>(rec) : __ldcg(reinterpret_cast<const double2*>(rec));
+        d[0] = x.x;
+        d[1] = x.y;
+    } else {
+        static_assert(NK <= 4, "a node row holds at most four depths here");
+        double a, b, c, e;
+        if constexpr (S) {
+            const double2 x = reinterpret_cast<const double2*>(rec)[0], y = reinterpret_cast<const double2*>(rec)[1];
+            a = x.x; b = x.y; c = y.x; e = y.y;
+        } else {
+            asm volatile("ld.global.cg.v4.f64 {%0, %1, %2, %3}, [%4];"
+                         : "=d"(a), "=d"(b), "=d"(c), "=d"(e)
+                         : "l"(rec)
+                         : "memory");
+        }
+        d[0] = a;
+        d[1] = b;
+        d[2] = c;
+        if constexpr (NK == 4) d[3] = e;
+        else (void)e;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -320,7 +351,8 @@ struct StepView {
     const int* src;     // source index per entry, from the step's first row
     const void* cost;
     const char* time;
-    const DPE* srow;    // DP records of the source layer
+    const double* srcv; // DP values of the source layer (its record 0)
+    size_t sbase;       // record index of the source layer's record 0
     int Kp, kofs, nk;
     double lam, tconst;
 };
@@ -345,9 +377,12 @@ __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row,
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
         sv[r] = v.src[(row + r) * 32 + lane];
-        const DPE* rec = v.srow + (size_t)(sv[r] < 0 ? 0 : sv[r]) * v.Kp + v.kofs;
+        if (sv[r] >= 0) {
+            ld_row<S, NK>(v.srcv + (size_t)sv[r] * v.Kp + v.kofs, d[r]);
+        } else {
 #pragma unroll
-        for (int kk = 0; kk < NK; ++kk) d[r][kk] = sv[r] >= 0 ? ldV<S>(rec + kk) : kInfD;
+            for (int kk = 0; kk < NK; ++kk) d[r][kk] = kInfD;
+        }
     }
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
@@ -389,9 +424,9 @@ __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, i
             const int sv = v.src[row * 32 + lane];
             if (sv < 0) continue;
             const double w = edge_weight<CT, TK>(v, row * 32 + lane);
-            const DPE* rec = v.srow + (size_t)sv * v.Kp + v.kofs;
+            const double* rec = v.srcv + (size_t)sv * v.Kp + v.kofs;
             for (int kk = 0; kk < v.nk; ++kk) {
-                const double cand = __dadd_rn(ldV<S>(rec + kk), w);
+                const double cand = __dadd_rn(S ? rec[kk] : __ldcg(rec + kk), w);
                 if (cand < thr) { thr = cand; win = row * v.nk + kk; }
             }
         }
@@ -402,7 +437,7 @@ __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, i
 template <class CT, int TK, bool S, int NK>
 __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* spl, int s0, int s1, int l, int k) {
     const int n = p.n, K = p.K, Kp = p.Kp;
-    DPE* cur = p.dp + (size_t)(l & 1) * n * Kp;
+    const size_t cur = (size_t)(l & 1) * n * Kp;
     const bool empty = step_empty(p, l, k);
     const int r0 = spl[0];
     int* predRow = p.pred + (size_t)l * n * K + (size_t)k * n;
@@ -413,8 +448,8 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
     for (int s = s0 + (int)(threadIdx.x >> 5); s < s1; s += nwarps) {
         const int v = s * 32 + lane;
         const bool valid = v < n;
-        DPE* me = cur + (size_t)v * Kp + k;
-        double best = (l == 0 && valid) ? ldV<S>(me) : kInfD;
+        const size_t me = cur + (size_t)v * Kp + k;
+        double best = (l == 0 && valid) ? ldV<S>(p, me) : kInfD;
         double thr = best < ub ? best : ub;
         int win = -1;
         if (!empty) win = fold_rows<CT, TK, S, NK>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, thr);
@@ -434,7 +469,7 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
                 o = bs;
                 h = 1;
             } else {
-                const DPE e = ldE<S>(sv.srow + (size_t)bs * Kp + bk);
+                const DpRec e = ldE<S>(p, sv.sbase + (size_t)bs * Kp + bk);
                 o = e.o;
                 h = e.h + 1;
             }
@@ -451,13 +486,13 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
                     o = ps;
                     h = 1;
                 } else {
-                    const DPE e = ldE<S>(cur + (size_t)ps * Kp + (k - 1));
+                    const DpRec e = ldE<S>(p, cur + (size_t)ps * Kp + (k - 1));
                     o = e.o;
                     h = e.h + 1;
                 }
             }
         }
-        stE(me, best, o, h);
+        stE(p, me, best, o, h);
     }
     return any;
 }
@@ -483,7 +518,8 @@ __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, i
         v.cost = reinterpret_cast<const CT*>(p.cost) + off;
         v.time = TK == 0 ? nullptr : reinterpret_cast<const char*>(p.time) + off * st.timeBytes;
     }
-    v.srow = p.dp + (size_t)((inter ? l - 1 : l) & 1) * n * Kp;
+    v.sbase = (size_t)((inter ? l - 1 : l) & 1) * n * Kp;
+    v.srcv = p.dv + v.sbase;
     v.Kp = Kp;
     v.kofs = inter ? 0 : k - 1;
     v.nk = inter ? K : 1;
@@ -679,8 +715,9 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     if constexpr (S) {
         // single-CTA team: the DP records and the backup row live in shared
         // memory for the whole launch (layout as in global memory)
-        p.dp = reinterpret_cast<DPE*>(smem);
-        p.bak = reinterpret_cast<double*>(smem + (size_t)2 * n * Kp * sizeof(DPE));
+        p.dv = reinterpret_cast<double*>(smem);
+        p.doh = reinterpret_cast<int2*>(smem + (size_t)2 * n * Kp * sizeof(double));
+        p.bak = reinterpret_cast<double*>(smem + (size_t)2 * n * Kp * (sizeof(double) + sizeof(int2)));
         smem += bf_shared_table_bytes(n, Kp);
     }
     const int s0 = __ldg(p.ctaSlice + blockIdx.x), s1 = __ldg(p.ctaSlice + blockIdx.x + 1);
@@ -720,7 +757,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     for (long long r = tid; r < 2LL * n * Kp; r += nth) {
         const long long node = (r / Kp) % n;
         const bool start = r < (long long)n * Kp && r % Kp == 0 && p.branchOf[node] == p.branchId;
-        stE(p.dp + r, start ? 0.0 : kInfD, kLapUnknown, 0);
+        stE(p, (size_t)r, start ? 0.0 : kInfD, kLapUnknown, 0);
     }
     for (long long i = tid; i < n; i += nth) {
         p.bak[i] = kInfD;
@@ -769,7 +806,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     for (;;) {
         // the first step of the sweep is staged while the backup row is copied
         stage_issue(p, st, s0, s1, 0, K > 1 ? 0 : 1, K > 1 ? 1 : 0);
-        for (long long i = tid; i < n; i += nth) p.bak[i] = ldV<S>(p.dp + (size_t)i * Kp);
+        for (long long i = tid; i < n; i += nth) p.bak[i] = ldV<S>(p, (size_t)i * Kp);
         if (!team_sync(t)) { stage_drain(st); return; }
         // Layers are relaxed in order; a CTA hands each step off to its
         // graph neighbours only (one team barrier closes the sweep).  The
@@ -832,17 +869,17 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             }
             return;
         }
-        const DPE* lastRowBase = p.dp + (size_t)lastPar * n * Kp + lastDepth;
+        const size_t lastRowBase = (size_t)lastPar * n * Kp + lastDepth;
         if (p.mode == 2) {
             // minimum-cost verdict: lower bounds of the branch nodes, origin of
             // their closing path, first and first-valid candidates.
             Key first{kInfD, 0x7fffffff}, firstValid{kInfD, 0x7fffffff};
             int anyFinite = 0;
-            const DPE* dRow = p.dp + (size_t)(p.nY & 1) * n * Kp;
+            const size_t dRow = (size_t)(p.nY & 1) * n * Kp;
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] != p.branchId) { p.lbOut[i] = kInfD; p.originOut[i] = -1; continue; }
-                const double lb = ldV<S>(lastRowBase + (size_t)i * Kp);
-                int o = ldE<S>(dRow + (size_t)i * Kp).o;
+                const double lb = ldV<S>(p, lastRowBase + (size_t)i * Kp);
+                int o = ldE<S>(p, dRow + (size_t)i * Kp).o;
                 if (o < 0 && !isinf((float)lb)) o = dij_walk_end(p, (int)i);
                 p.lbOut[i] = lb;
                 p.originOut[i] = o;
@@ -888,19 +925,19 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         // wrap-around (cost_time_ratio_solver.cpp:399-417) and lap function
         {
             int improved = 0;
-            const DPE* wRow = p.dp + (size_t)((p.nY - 1) & 1) * n * Kp;
+            const size_t wRow = (size_t)((p.nY - 1) & 1) * n * Kp;
             const long long layerSpan = (long long)n * K;
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] == p.branchId) {
-                    const double cand = ldV<S>(lastRowBase + (size_t)i * Kp);
+                    const double cand = ldV<S>(p, lastRowBase + (size_t)i * Kp);
                     const double b = p.bak[i];
-                    DPE* d0 = p.dp + (size_t)i * Kp;
+                    double* d0 = p.dv + (size_t)i * Kp;
                     if (cand < b) {
                         improved = 1;
-                        d0->v = cand;
+                        *d0 = cand;
                         p.pred[i] = __ldcg(p.pred + (size_t)p.nY * layerSpan + i);
                     } else {
-                        d0->v = b;
+                        *d0 = b;
                     }
                 }
                 const int pe = p.pred[i];
@@ -912,7 +949,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     if (pe < 0 || lp != p.nY - 1) {
                         nx = kLapUnknown;
                     } else {
-                        const DPE w = ldE<S>(wRow + (size_t)wv * Kp + kp);
+                        const DpRec w = ldE<S>(p, wRow + (size_t)wv * Kp + kp);
                         nx = w.o;
                         st = 1 + w.h;
                     }
@@ -937,7 +974,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             for (long long i = tid; i < n; i += nth) {
                 int st = 0;
                 if (p.branchOf[i] == p.branchId) {
-                    const double d0 = ldV<S>(p.dp + (size_t)i * Kp);
+                    const double d0 = ldV<S>(p, (size_t)i * Kp);
                     if (d0 < 0) {
                         int v0 = -1;
                         long long steps = 0;
@@ -996,7 +1033,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     for (int i = 0; i < n; ++i) {
                         const int st = __ldcg(p.candStat + i);
                         if (st == 0) continue;
-                        Key kk{ldV<S>(p.dp + (size_t)i * Kp), i};
+                        Key kk{ldV<S>(p, (size_t)i * Kp), i};
                         if (key_less(prev, kk) && key_less(kk, next)) next = kk;
                     }
                     if (next.i == 0x7fffffff) break;

@@ -243,7 +243,8 @@ class Graph {
     bool f32Known[2] = {false, false};  // e32 state computed since the last energy change
 
     // solver workspace
-    DBuf<DPE> wDp;
+    DBuf<double> wDv;
+    DBuf<int2> wDoh;
     DBuf<double> wBak, wRedVal, wLb, wCOut, wTOut;
     DBuf<int> wCtaSlice, wWaitPtr, wWaitIdx;
     DBuf<unsigned> wStepDone;
@@ -787,7 +788,8 @@ void Graph::ensure_workspace(int K, int blocks) {
     while (Kp < K) Kp <<= 1;
     const size_t expanded = n * (size_t)(T.nY + 1) * (size_t)K;
     if (wsK != K || wPred.n < expanded) {
-        wDp.alloc(2 * n * Kp);
+        wDv.alloc(2 * n * Kp);
+        wDoh.alloc(2 * n * Kp);
         wPred.alloc(expanded);
         PGC_CUDA(cudaMemsetAsync(wPred.p, 0xff, expanded * sizeof(int), stream));  // -1
         wsK = K;
@@ -846,7 +848,8 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.cost = r.cost;
     p.time = r.time;
     p.tconst = r.tconst;
-    p.dp = wDp.p;
+    p.dv = wDv.p;
+    p.doh = wDoh.p;
     p.bak = wBak.p;
     p.pred = wPred.p;
     p.ctaSlice = wCtaSlice.p;
