@@ -88,6 +88,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.at_end = False
 
     def __enter__(self):
         try:
@@ -111,6 +112,16 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if not self.lines:
+            # a timed region shorter than the sampling period: one query at
+            # its end, while the clocks still reflect the load
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10)
+                self.lines += [x.strip() for x in out.stdout.splitlines() if x.strip()]
+                self.at_end = True
+            except Exception:
+                pass
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -129,7 +140,10 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if self.at_end:
+            out["note"] = "timed region shorter than the 200 ms sampling period: sampled at its end"
+        return out
 
 
 def _dist_env():
