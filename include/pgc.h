@@ -145,7 +145,11 @@ int pgc_set_team_cap(pgc_graph* g, int max_ctas);
  * pgc_solve_with_cost_time_ratio (solver "lawlercpu"/"lawlergpu") or
  * pgc_solve_with_minimum_cost (any other name) would, on its own stream with
  * a team of at most `ctas_per_graph` CTAs (0: one), driven by `workers` host
- * threads (0: one per graph, at most 512; waiting threads sleep).  With
+ * threads (0: 32; waiting threads sleep).  Graphs run side by side only as
+ * far as the device has host work queues: start the process with
+ * CUDA_DEVICE_MAX_CONNECTIONS=32 (the Python package sets it as a default
+ * before CUDA starts); with the CUDA default of 8, streams share queues and
+ * the batch runs about 3x slower.  With
  * `regenerate` != 0 each graph first recomputes its
  * edge costs (pgc_generate).  Each graph's result is read afterwards with
  * pgc_result*; status[i] receives its return code.  Returns PGC_OK when all

@@ -483,12 +483,13 @@ __global__ void layer1_mean_kernel(const double* cost, long long layerStride, lo
 template <class K>
 static int stream_grid(K kernel, int threads, size_t smem) {
     int dev = 0, sms = 0, per = 0;
+    int grid = 148;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1)
         cudaGetLastError();
-        return 148;
-    }
-    return sms * per;
+    else
+        grid = sms * per;
+    return grid;
 }
 
 static int grid_for(long long total, int threads) {

@@ -1812,7 +1812,7 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
         if (count < 0 || (count > 0 && (!graphs || !status))) throw Failure(PGC_ERR_ARG, "null argument");
         const std::string name = solver ? solver : "";
         const bool ratio = name == "lawlercpu" || name == "lawlergpu";
-        if (workers <= 0) workers = (int)std::min<int64_t>(count, 512);
+        if (workers <= 0) workers = 32;
         workers = (int)std::min<int64_t>(workers, count);
         std::atomic<int64_t> next{0};
         std::vector<std::string> errors((size_t)count);

@@ -20,6 +20,13 @@ import os
 
 import numpy as np
 
+# Batched solves run one CUDA stream per graph; the device runs them side by
+# side only as far as it has host work queues, 8 by default.  32 (the most)
+# triples batched throughput.  The driver reads this when the process's CUDA
+# context is created, so it takes effect only if nothing has used CUDA yet;
+# a value the user set is kept.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
            "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch"]
 
@@ -124,7 +131,7 @@ class product_graph_generator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:  # at interpreter exit the module may already be torn down
             _lib.pgc_destroy(h)
             self._h = None
 
@@ -253,8 +260,7 @@ def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas
     Each generator is solved as ``solve_with_cost_time_ratio`` (solver
     ``"lawlercpu"``/``"lawlergpu"``) or ``solve_with_minimum_cost`` (any other
     name) would, on its own CUDA stream with a Bellman-Ford team of at most
-    ``ctas_per_graph`` CTAs, by ``workers`` native threads (0: one per
-    generator, at most 512); with
+    ``ctas_per_graph`` CTAs, by ``workers`` native threads (0: 32); with
     ``regenerate`` each first recomputes its edge costs.  Returns the list of
     ``(passes_layers_just_once, final_objective, matching)`` triples.
     """
