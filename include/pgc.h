@@ -144,8 +144,9 @@ int pgc_set_team_cap(pgc_graph* g, int max_ctas);
 /* No reference counterpart.  Solves `count` graphs concurrently: each one as
  * pgc_solve_with_cost_time_ratio (solver "lawlercpu"/"lawlergpu") or
  * pgc_solve_with_minimum_cost (any other name) would, on its own stream with
- * a team of at most `ctas_per_graph` CTAs (0: one), driven by `workers` host
- * threads (0: 32; waiting threads sleep).  Graphs run side by side only as
+ * a team of at most `ctas_per_graph` CTAs (0: SMs / min(count, 32), so the
+ * teams the device runs side by side cover its SMs), driven by `workers`
+ * host threads (0: 64; waiting threads sleep).  Graphs run side by side only as
  * far as the device has host work queues: start the process with
  * CUDA_DEVICE_MAX_CONNECTIONS=32 (the Python package sets it as a default
  * before CUDA starts); with the CUDA default of 8, streams share queues and

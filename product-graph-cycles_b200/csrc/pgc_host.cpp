@@ -1812,7 +1812,15 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
         if (count < 0 || (count > 0 && (!graphs || !status))) throw Failure(PGC_ERR_ARG, "null argument");
         const std::string name = solver ? solver : "";
         const bool ratio = name == "lawlercpu" || name == "lawlergpu";
-        if (workers <= 0) workers = 32;
+        if (workers <= 0) workers = 64;
+        if (ctas_per_graph <= 0) {
+            // the device runs at most 32 kernels side by side (host work
+            // queues): teams that together cover the SMs keep them all busy
+            int dev = 0, sms = 0;
+            PGC_CUDA(cudaGetDevice(&dev));
+            PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            ctas_per_graph = std::max(1, sms / (int)std::max<int64_t>(1, std::min<int64_t>(count, 32)));
+        }
         workers = (int)std::min<int64_t>(workers, count);
         std::atomic<int64_t> next{0};
         std::vector<std::string> errors((size_t)count);
@@ -1826,7 +1834,7 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
                     continue;
                 }
                 const int saved = h->g.teamCap;
-                h->g.teamCap = ctas_per_graph > 0 ? ctas_per_graph : 1;
+                h->g.teamCap = ctas_per_graph;
                 h->g.blockingSync = true;
                 status[i] = regenerate ? pgc_generate(h) : PGC_OK;
                 if (status[i] == PGC_OK)

@@ -253,14 +253,15 @@ class product_graph_generator:
         return dict(zip(keys, list(buf)))
 
 
-def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas_per_graph: int = 1,
+def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas_per_graph: int = 0,
                 workers: int = 0, regenerate: bool = False):
     """Solve many generators concurrently (no counterpart in the reference).
 
     Each generator is solved as ``solve_with_cost_time_ratio`` (solver
     ``"lawlercpu"``/``"lawlergpu"``) or ``solve_with_minimum_cost`` (any other
     name) would, on its own CUDA stream with a Bellman-Ford team of at most
-    ``ctas_per_graph`` CTAs, by ``workers`` native threads (0: 32); with
+    ``ctas_per_graph`` CTAs (0: SMs / min(graphs, 32)), by ``workers`` native
+    threads (0: 64); with
     ``regenerate`` each first recomputes its edge costs.  Returns the list of
     ``(passes_layers_just_once, final_objective, matching)`` triples.
     """

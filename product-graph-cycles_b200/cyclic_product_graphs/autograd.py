@@ -26,10 +26,16 @@ def _as_host(fd: torch.Tensor) -> np.ndarray:
     return fd.detach().to(device="cpu", dtype=torch.float64).contiguous().numpy()
 
 
-def _adjoint(gen, grad_out: torch.Tensor, like: torch.Tensor) -> torch.Tensor:
+def _adjoint(gen, grad_out: torch.Tensor, like: torch.Tensor, synced: bool = False) -> torch.Tensor:
+    # the library writes on the handle's own stream and synchronises it before
+    # returning; torch's stream must be idle first (grad_out may still be
+    # computed on it) unless the caller already synchronised
     grad = torch.empty(like.shape, dtype=torch.float64, device="cuda")
-    torch.cuda.synchronize()
-    gen.backward_feat_diff(float(grad_out), grad.data_ptr())
+    g = float(grad_out) if synced else None
+    if not synced:
+        torch.cuda.synchronize()
+        g = float(grad_out)
+    gen.backward_feat_diff(g, grad.data_ptr())
     return grad.to(device=like.device, dtype=like.dtype)
 
 
@@ -82,7 +88,9 @@ class _BatchedRatio(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_out):
         fds = ctx.saved_tensors
-        return (None, None) + tuple(_adjoint(g, grad_out[i], fd) for i, (g, fd) in enumerate(zip(ctx.gens, fds)))
+        torch.cuda.synchronize()
+        go = grad_out.detach().cpu()
+        return (None, None) + tuple(_adjoint(g, go[i], fd, synced=True) for i, (g, fd) in enumerate(zip(ctx.gens, fds)))
 
 
 def ratio_cycle_objectives(gens, feat_diffs, max_depth=None) -> torch.Tensor:
