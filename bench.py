@@ -48,6 +48,8 @@ WORKLOADS = {
     "plain_642_60_k2": (642, 60, 32, False, False, False, "vanilla", "nomode", 2),
     # smaller conjugate pair used for ncu captures (inputs still larger than L2)
     "conj_2k_100_k3": (2000, 100, 64, True, False, False, "vanilla", "lengthnormalisation", 3),
+    # large pair at the HBM-bound scale: conjugate + pruned, SO(3) robust cost against feature time
+    "conj_prune_20k_500_k4": (20000, 500, 64, True, True, True, "robustso3", "feature", 4),
 }
 DEFAULT_WORKLOAD = "single_pair_conj_5k_200_k3"
 # batched serving: many plain pairs of uneven size solved concurrently
@@ -181,14 +183,17 @@ def algorithmic_bytes_per_sweep(info, k, ratio_mode):
     once per depth 1..K-1; a visit reads the int32 source index and c fp32
     cost columns (c = 2 in ratio mode with a time column, else 1).  Every
     (node, depth) of the nY + 1 layers writes an fp32-sized value and an
-    int32 predecessor.  Gathered source values are not counted.
+    int32 predecessor.  Gathered source values are not counted.  Without
+    intralayer edges (pruned graphs) only depth 0 of each layer is ever
+    reached, so K is replaced by 1 in the node term.
     """
     L = info["layers"]
     c = 2 if (ratio_mode and info["cost_columns"] > 1) else 1
     e_inter = L * info["inter_edges_per_layer"]
     e_intra = L * info["intra_edges_per_layer"]
     nodes = info["nodes_per_layer"] * (L + 1)
-    return (4 + 4 * c) * (e_inter + (k - 1) * e_intra) + 8 * k * nodes
+    depths = k if e_intra > 0 else 1
+    return (4 + 4 * c) * (e_inter + (k - 1) * e_intra) + 8 * depths * nodes
 
 
 def run_ours(args, world, rank):

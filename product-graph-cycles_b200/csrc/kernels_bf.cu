@@ -803,9 +803,15 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     const long long numNodes = p.numNodes;
     int sweep = 0;
     unsigned step = 0;
+    // Without intralayer edges (pruned graphs) the depth steps 1..K-1 relax
+    // nothing: every record they would write is +inf and stays +inf (layer 0's
+    // too: no edge ever reaches its depths >= 1), and the origins they would
+    // write are never read (an unreached source never wins).  Only the
+    // interlayer step of each layer runs.
+    const int kSteps = p.intraEntries == 0 ? 1 : K;
     for (;;) {
         // the first step of the sweep is staged while the backup row is copied
-        stage_issue(p, st, s0, s1, 0, K > 1 ? 0 : 1, K > 1 ? 1 : 0);
+        stage_issue(p, st, s0, s1, 0, kSteps > 1 ? 0 : 1, kSteps > 1 ? 1 : 0);
         for (long long i = tid; i < n; i += nth) p.bak[i] = ldV<S>(p, (size_t)i * Kp);
         if (!team_sync(t)) { stage_drain(st); return; }
         // Layers are relaxed in order; a CTA hands each step off to its
@@ -819,7 +825,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         unsigned long long cycRelax = 0, cycHand = 0;
         int sb = 0;  // buffer of the current step
         for (int l = 0; l <= p.nY; ++l) {
-            for (int k = 0; k < K; ++k) {
+            for (int k = 0; k < kSteps; ++k) {
                 if (l == 0 && k == 0) continue;
                 const unsigned long long ta = isLead ? clock64() : 0;
                 if (!stage_wait(st, sb)) {
@@ -827,8 +833,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     stage_drain(st);
                     return;
                 }
-                const bool last = l == p.nY && k == K - 1;
-                if (!last) stage_issue(p, st, s0, s1, sb ^ 1, k + 1 < K ? l : l + 1, k + 1 < K ? k + 1 : 0);
+                const bool last = l == p.nY && k == kSteps - 1;
+                if (!last) stage_issue(p, st, s0, s1, sb ^ 1, k + 1 < kSteps ? l : l + 1, k + 1 < kSteps ? k + 1 : 0);
                 const bool any = relax_step<CT, TK, S>(p, st, sb, s0, s1, l, k);
                 if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) p.layerFlag[l] = stamp;
                 const unsigned long long tb = isLead ? clock64() : 0;

@@ -913,7 +913,7 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     stats.cycB += c.cycPhaseB;
     stats.cycSync += c.cycSync;
     stats.cycTail += c.cycTail;
-    stats.steps += (long long)c.sweeps * ((long long)(T.nY + 1) * r.K - 1);
+    stats.steps += (long long)c.sweeps * ((long long)(T.nY + 1) * (T.entries[INTRA] == 0 ? 1 : r.K) - 1);
     stats.ctas = r.blocks;
     stats.threads = r.threads;
     stats.waitEntries = r.blocks > 1 ? waitEntries : 0;
