@@ -50,6 +50,8 @@ WORKLOADS = {
     "conj_2k_100_k3": (2000, 100, 64, True, False, False, "vanilla", "lengthnormalisation", 3),
     # large pair at the HBM-bound scale: conjugate + pruned, SO(3) robust cost against feature time
     "conj_prune_20k_500_k4": (20000, 500, 64, True, True, True, "robustso3", "feature", 4),
+    # the same layer with 100 layers: ncu captures of the large pair's steps (about 3 GB on the device)
+    "conj_prune_20k_100_k4": (20000, 100, 64, True, True, True, "robustso3", "feature", 4),
 }
 DEFAULT_WORKLOAD = "single_pair_conj_5k_200_k3"
 # batched serving: many plain pairs of uneven size solved concurrently
@@ -239,6 +241,7 @@ def run_ours(args, world, rank):
             ev[i][1].record(stream)
             st = g.last_stats()
             prof = g.last_profile()
+            last_sweeps = st["sweeps"]
             sweeps += st["sweeps"]
             bf_us += st["device_us"]
             launches += st["kernel_launches"] + 1  # + the energy kernel of generate()
@@ -311,7 +314,12 @@ def run_ours(args, world, rank):
         "bf_team": {"ctas": prof["ctas"], "threads": prof["threads"], "wait_list_entries": prof["wait_entries"],
                     "cycles_per_step": {key[7:]: round(prof[key] / max(1, prof["steps"]), 1)
                                         for key in ("cycles_relax", "cycles_handoff", "cycles_bookkeeping",
-                                                    "cycles_sweep_tail")}},
+                                                    "cycles_sweep_tail")},
+                    "tail_cycles_per_sweep": {key[12:]: round(prof[key] / max(1, last_sweeps), 1)
+                                              for key in ("cycles_tail_wrap", "cycles_tail_candidates",
+                                                          "cycles_tail_lead")},
+                    "last_solve": {key: st[key] for key in ("bf_calls", "sweeps", "candidates", "fallback_walks",
+                                                            "lawler_iters")}},
         "clocks": clocks.summary(),
         "result": {"objective": result[1], "cycle_edges": int(result[2].shape[0])},
         "wall_s": wall,

@@ -48,6 +48,9 @@ struct Control {
     // SM cycles seen by CTA 0's thread 0 (profiling counters): relaxation,
     // sweep bookkeeping, step hand-offs / barriers, sweep tail
     unsigned long long cycPhaseA, cycPhaseB, cycSync, cycTail;
+    // parts of the sweep tail: wrap-around and lap function (up to its team
+    // barrier), candidate walks (up to the lead's barrier), the lead's choice
+    unsigned long long cycWrap, cycCand, cycLead;
     // minimum-cost outputs
     double firstLb;
     int firstV;
@@ -184,6 +187,12 @@ constexpr int kStepDoneStride = 8;  // one 32-byte sector per CTA step counter
 // Most threads per Bellman-Ford CTA: 20 warps fit the kernel's registers
 // (about 100 per thread) on one SM without spilling the relaxation loop.
 constexpr int kBfThreads = 640;
+// Source values a lane gathers before folding them (one batch of rows).
+constexpr int kGather = 20;
+// Rows of one gather batch when every row has nk source depths (nk > 0).
+__host__ __device__ constexpr int bf_rows_per_batch(int nk) {
+    return kGather / nk < 1 ? 1 : kGather / nk > 8 ? 8 : kGather / nk;
+}
 // Bytes of shared memory a single-CTA launch needs to keep its DP records
 // and backup row on chip (128-byte aligned).
 __host__ __device__ inline size_t bf_shared_table_bytes(int n, int Kp) {

@@ -345,7 +345,6 @@ __device__ __forceinline__ void stage_drain(Stage& st) {
 // it.  The winner's origin and path length are read once per node after the
 // fold.  Returns whether this thread improved a node.
 // ---------------------------------------------------------------------------
-constexpr int kGather = 20;
 
 struct StepView {
     const int* src;     // source index per entry, from the step's first row
@@ -416,7 +415,7 @@ template <class CT, int TK, bool S, int NK>
 __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, int j1, double& thr) {
     int win = -1;
     if constexpr (NK > 0) {
-        constexpr int RB = kGather / NK < 1 ? 1 : kGather / NK > 8 ? 8 : kGather / NK;
+        constexpr int RB = bf_rows_per_batch(NK);
         for (; j1 - row >= RB; row += RB) fold_batch<CT, TK, S, NK, RB>(v, lane, row, thr, win);
         if (row < j1) fold_tail<CT, TK, S, NK, RB>(v, lane, row, j1 - row, thr, win);
     } else {
@@ -652,6 +651,44 @@ __device__ int extract_cycle(const BfParams& p, int v0, long long cLength) {
     }
     p.ctl->cycleLen = len;
     return BF_FOUND_CYCLE;
+}
+
+// The laps of the cycle that closes at v0, for a parallel extract_cycle:
+// x_0 = v0, x_(j+1) = lapNext[x_j] until the lap function returns to v0.
+// Lap j holds lapSteps[x_j] entries of the cycle buffer from offs[j] on.
+// Returns the lap count and the cycle's length in *total, or -1 (unknown
+// lap, or longer than the cycle buffer): extract_cycle then walks serially.
+__device__ int lap_cycle_list(const BfParams& p, int v0, int* nodes, long long* offs, long long* total) {
+    long long off = 0;
+    int x = v0;
+    for (int j = 0; j < p.n; ++j) {
+        nodes[j] = x;
+        offs[j] = off;
+        off += __ldcg(p.lapSteps + x);
+        x = __ldcg(p.lapNext + x);
+        if (x < 0 || off > p.cycleCap) return -1;
+        if (x == v0) {
+            *total = off;
+            return j + 1;
+        }
+    }
+    return -1;
+}
+
+// Lap j of a parallel extract_cycle: len predecessor steps from x, written
+// from cycleBuf[off] on.  The lap must stay off layer-0 start nodes until its
+// last step, which must reach xNext; otherwise (or when a predecessor leaves
+// the node range) it returns non-zero and the serial walk decides.
+__device__ int walk_lap(const BfParams& p, int x, int xNext, long long off, long long len) {
+    const long long total = (long long)p.n * (p.nY + 1) * p.K;
+    int pr = x;
+    for (long long s = 0; s < len; ++s) {
+        pr = __ldcg(p.pred + pr);
+        if (pr < 0 || pr >= total) return 1;
+        if (pr < p.n && s + 1 < len) return 2;
+        p.cycleBuf[off + s] = original_index(p.n, p.K, pr);
+    }
+    return pr == xNext ? 0 : 2;
 }
 
 // Upper-bound path (cost_time_ratio_solver.cpp:370-397): from the closing
@@ -965,6 +1002,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             }
             bool ok;
             improved = team_sync_or(t, improved, ok);
+            if (isLead) atomicAdd(&p.ctl->cycWrap, clock64() - tTail);
             if (!ok) return;
             if (!improved) {
                 if (isLead) { p.ctl->status = BF_WRAP_NO_IMPROVE; p.ctl->sweeps = sweep; p.ctl->epoch = epochBase + sweep; }
@@ -1011,7 +1049,12 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                 p.redAux64[blockIdx.x] = (long long)sdec;
             }
         }
+        __shared__ int sLaps, sBad;
+        __shared__ long long sCycLen;
+        const unsigned long long tCand = isLead ? clock64() : 0;
         if (!team_sync(t)) return;
+        const unsigned long long tLead = isLead ? clock64() : 0;
+        if (isLead) atomicAdd(&p.ctl->cycCand, tLead - tCand);
         int finished = 0;
         if (isLead) {
             Key ok{kInfD, 0x7fffffff}, unk{kInfD, 0x7fffffff};
@@ -1057,17 +1100,55 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     }
                 }
             }
+            sLaps = 0;
             if (winner >= 0) {
                 p.ctl->v0 = v0;
                 p.ctl->cLength = steps;
                 p.ctl->candidateVi = winner;
-                p.ctl->status = extract_cycle(p, v0, steps);
+                // A cycle of many laps is one long chain of dependent
+                // predecessor loads; its laps are walked side by side by
+                // CTA 0 (lap nodes and offsets in the candidate arrays, which
+                // are not read again in this launch).
+                long long total = 0;
+                const int laps = lap_cycle_list(p, v0, p.candV0, p.candSteps, &total);
+                if (laps > 0) {
+                    sLaps = laps;
+                    sCycLen = total;
+                } else {
+                    p.ctl->status = extract_cycle(p, v0, steps);
+                }
             } else if (sweep >= numNodes - 1 || (p.maxSweeps > 0 && sweep >= p.maxSweeps)) {
                 p.ctl->status = BF_MAX_SWEEPS;
             }
+        }
+        if (blockIdx.x == 0) {
+            __syncthreads();
+            const int laps = sLaps;
+            if (laps > 0) {
+                if (threadIdx.x == 0) sBad = 0;
+                __syncthreads();
+                for (int j = (int)threadIdx.x; j < laps; j += blockDim.x) {
+                    const long long o0 = __ldcg(p.candSteps + j);
+                    const long long o1 = j + 1 < laps ? __ldcg(p.candSteps + j + 1) : sCycLen;
+                    const int xn = __ldcg(p.candV0 + (j + 1 < laps ? j + 1 : 0));
+                    if (walk_lap(p, __ldcg(p.candV0 + j), xn, o0, o1 - o0) != 0) sBad = 1;
+                }
+                __syncthreads();
+                if (isLead) {
+                    if (sBad) {
+                        p.ctl->status = extract_cycle(p, p.ctl->v0, p.ctl->cLength);
+                    } else {
+                        p.ctl->cycleLen = (int)sCycLen;
+                        p.ctl->status = BF_FOUND_CYCLE;
+                    }
+                }
+            }
+        }
+        if (isLead) {
             p.ctl->sweeps = sweep;
             p.ctl->epoch = epochBase + sweep;
             finished = p.ctl->status != BF_RUNNING;
+            atomicAdd(&p.ctl->cycLead, clock64() - tLead);
         }
         bool ok;
         finished = team_sync_or(t, finished, ok);

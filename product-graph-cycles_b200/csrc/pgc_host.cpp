@@ -209,6 +209,7 @@ struct Stats {
     double deviceMs = 0;
     long long launches = 0;
     unsigned long long cycA = 0, cycB = 0, cycSync = 0, cycTail = 0;
+    unsigned long long cycWrap = 0, cycCand = 0, cycLead = 0;  // parts of cycTail
     long long steps = 0;
     long long ctas = 0, threads = 0, waitEntries = 0;  // team shape of the last launch
 };
@@ -248,7 +249,8 @@ class Graph {
     DBuf<double> wBak, wRedVal, wLb, wCOut, wTOut;
     DBuf<int> wCtaSlice, wWaitPtr, wWaitIdx;
     DBuf<unsigned> wStepDone;
-    int ctaSliceBlocks = -1;
+    std::vector<int> ctaCut;   // slice ranges of the uploaded partition
+    int cutBlocks = -1, cutK = -1, cutWarps = -1;  // the partition ctaCut was made for
     long long waitEntries = 0;  // wait-list entries over all CTAs of the current partition
     DBuf<int> wPred, wLapNext, wLapSteps, wMark, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
         wRedIdx, wRedAux, wOrigin, wPairS, wPairT, wCount;
@@ -354,7 +356,8 @@ class Graph {
     };
     Run prepare_run(int K, bool ratio);
     void ensure_workspace(int K, int blocks);
-    void upload_cta_slices(int blocks);
+    std::vector<int> cta_cuts(int blocks, int K, int warps) const;
+    void upload_cta_slices(const std::vector<int>& cut, int K, int warps);
     void upload_branch(const std::vector<int>& branchOf);
     // Every solve starts from an unwritten predecessor table (-1), like the
     // reference's freshly allocated solver state.
@@ -674,11 +677,13 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     const size_t smemCap = (size_t)std::max(0, smemOptin - 1024);  // static shared memory of the kernel
     const int costBytes = r.costF32 ? 4 : 8, timeBytes = r.timeKind == 1 ? 4 : r.timeKind == 2 ? 8 : 0;
     const bool stageOn = env_int("PGC_BF_STAGE", 1) != 0;
+    std::vector<int> cut;
     auto stage_need = [&](int blocks, int& maxSl, int& rowCap) -> size_t {
+        cut = cta_cuts(blocks, K, r.threads / 32);
         maxSl = 0;
         rowCap = 0;
         for (int c = 0; c < blocks; ++c) {
-            const int a = (int)((long long)c * T.nslices / blocks), b = (int)((long long)(c + 1) * T.nslices / blocks);
+            const int a = cut[(size_t)c], b = cut[(size_t)c + 1];
             maxSl = std::max(maxSl, b - a);
             for (int p = 0; p < 2; ++p) rowCap = std::max(rowCap, T.sp[p][(size_t)b] - T.sp[p][(size_t)a]);
         }
@@ -735,21 +740,91 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     r.coop = blocks > 1;
     r.flagSync = env_int("PGC_BF_FLAGS", 1) ? 1 : 0;
     ensure_workspace(K, blocks);
-    upload_cta_slices(blocks);
+    if (cut.size() != (size_t)blocks + 1) stage_need(blocks, maxSl, rowCap);
+    upload_cta_slices(cut, K, r.threads / 32);
     return r;
 }
 
-// Slice range of every CTA (equal slice counts: a warp's step time depends on
-// its own slice only), and every CTA's wait list: the CTAs that own a source
+// Contiguous slice ranges for `blocks` CTAs of `warps` warps with balanced
+// step times.  A warp relaxes the CTA's slices round-robin, and one slice of
+// one step costs it about (gather batches + 1) memory latencies: the batches
+// of its rows and the epilogue (the winner's record, the stores); a slice
+// without rows only stores.  A CTA's time per layer is its slowest warp in
+// the interlayer step plus K - 1 times its slowest warp in an intralayer
+// step (those steps run only when the layer has intralayer edges).  The
+// cost of a range never grows when the range shrinks, so filling CTAs
+// greedily up to a bound is optimal for that bound; a binary search finds
+// the smallest bound that fits in `blocks` CTAs.  Costs are in quarter
+// latencies.
+std::vector<int> Graph::cta_cuts(int blocks, int K, int warps) const {
+    const int ns = T.nslices;
+    std::vector<int> cut((size_t)blocks + 1, ns);
+    cut[0] = 0;
+    if (blocks <= 1 || ns == 0) return cut;
+    warps = std::max(1, warps);
+    const bool intra = T.entries[INTRA] > 0;
+    const int rb[2] = {K <= 4 ? bf_rows_per_batch(K) : 1, bf_rows_per_batch(1)};
+    std::vector<long long> w[2];
+    long long lo = 0, hi = 0;
+    for (int p = 0; p < 2; ++p) {
+        w[p].resize((size_t)ns);
+        const long long reps = p == 0 ? 1 : (intra ? K - 1 : 0);
+        for (int s = 0; s < ns; ++s) {
+            const int rows = T.sp[p][(size_t)s + 1] - T.sp[p][(size_t)s];
+            w[p][(size_t)s] = rows > 0 ? 4LL * ((rows + rb[p] - 1) / rb[p] + 1) : 1;
+            lo = std::max(lo, reps * w[p][(size_t)s]);
+            hi += reps * w[p][(size_t)s];
+        }
+    }
+    const long long repIntra = intra ? K - 1 : 0;
+    std::vector<long long> acc[2] = {std::vector<long long>((size_t)warps), std::vector<long long>((size_t)warps)};
+    // fills CTAs greedily under `bound`; returns the CTAs used (cuts in c when given)
+    auto fill = [&](long long bound, std::vector<int>* c) -> int {
+        int used = 1, start = 0;
+        long long m[2] = {0, 0};
+        std::fill(acc[0].begin(), acc[0].end(), 0);
+        std::fill(acc[1].begin(), acc[1].end(), 0);
+        for (int s = 0; s < ns; ++s) {
+            int i = (s - start) % warps;
+            long long a0 = acc[0][(size_t)i] + w[0][(size_t)s], a1 = acc[1][(size_t)i] + w[1][(size_t)s];
+            if (s > start && std::max(m[0], a0) + repIntra * std::max(m[1], a1) > bound) {
+                if (c && used < blocks) (*c)[(size_t)used] = s;
+                ++used;
+                start = s;
+                m[0] = m[1] = 0;
+                std::fill(acc[0].begin(), acc[0].end(), 0);
+                std::fill(acc[1].begin(), acc[1].end(), 0);
+                i = 0;
+                a0 = w[0][(size_t)s];
+                a1 = w[1][(size_t)s];
+            }
+            acc[0][(size_t)i] = a0;
+            acc[1][(size_t)i] = a1;
+            m[0] = std::max(m[0], a0);
+            m[1] = std::max(m[1], a1);
+        }
+        return used;
+    };
+    while (lo < hi) {
+        const long long mid = lo + (hi - lo) / 2;
+        if (fill(mid, nullptr) <= blocks) hi = mid;
+        else lo = mid + 1;
+    }
+    const int used = fill(lo, &cut);
+    // CTAs past the last range keep empty ranges at the end
+    for (int c = used; c < blocks; ++c) cut[(size_t)c] = ns;
+    return cut;
+}
+
+// Slice range of every CTA (cta_cuts), and every CTA's wait list: the CTAs that own a source
 // of one of its in-edges (it reads their rows) or read one of its nodes
 // through an in-edge (they must be done before it overwrites a row).  The
 // product graph repeats one layer template, so one pass over the template
 // covers every layer; the closing layer's sources are a subset of the
 // interlayer ones.
-void Graph::upload_cta_slices(int blocks) {
-    if (ctaSliceBlocks == blocks) return;
-    std::vector<int> cut((size_t)blocks + 1);
-    for (int c = 0; c <= blocks; ++c) cut[(size_t)c] = (int)((long long)c * T.nslices / blocks);
+void Graph::upload_cta_slices(const std::vector<int>& cut, int K, int warps) {
+    const int blocks = (int)cut.size() - 1;
+    if (cutBlocks == blocks && cutK == K && cutWarps == warps && ctaCut == cut) return;
     std::vector<int> owner((size_t)T.nslices);
     for (int c = 0; c < blocks; ++c)
         for (int s = cut[(size_t)c]; s < cut[(size_t)c + 1]; ++s) owner[(size_t)s] = c;
@@ -779,7 +854,10 @@ void Graph::upload_cta_slices(int blocks) {
     if (idx.empty()) idx.push_back(0);  // keep a valid pointer; ptr says the lists are empty
     wWaitIdx.upload(idx.data(), idx.size(), stream);
     waitEntries = ptr.back();
-    ctaSliceBlocks = blocks;
+    ctaCut = cut;
+    cutBlocks = blocks;
+    cutK = K;
+    cutWarps = warps;
 }
 
 void Graph::ensure_workspace(int K, int blocks) {
@@ -913,6 +991,9 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     stats.cycB += c.cycPhaseB;
     stats.cycSync += c.cycSync;
     stats.cycTail += c.cycTail;
+    stats.cycWrap += c.cycWrap;
+    stats.cycCand += c.cycCand;
+    stats.cycLead += c.cycLead;
     stats.steps += (long long)c.sweeps * ((long long)(T.nY + 1) * (T.entries[INTRA] == 0 ? 1 : r.K) - 1);
     stats.ctas = r.blocks;
     stats.threads = r.threads;
@@ -1892,6 +1973,16 @@ int pgc_result_profile(pgc_graph* h, int64_t* out8) {
         out8[5] = s.ctas;
         out8[6] = s.threads;
         out8[7] = s.waitEntries;
+    });
+}
+
+int pgc_result_profile_tail(pgc_graph* h, int64_t* out3) {
+    return guarded([&] {
+        if (!out3) throw pgc::Failure(PGC_ERR_ARG, "null output");
+        const pgc::Stats& s = h->g.stats;
+        out3[0] = (int64_t)s.cycWrap;
+        out3[1] = (int64_t)s.cycCand;
+        out3[2] = (int64_t)s.cycLead;
     });
 }
 
