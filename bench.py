@@ -313,8 +313,8 @@ def run_ours(args, world, rank):
                      "bf_ms_per_solve": bf_us / 1000.0 / args.steps},
         "bf_team": {"ctas": prof["ctas"], "threads": prof["threads"], "wait_list_entries": prof["wait_entries"],
                     "cycles_per_step": {key[7:]: round(prof[key] / max(1, prof["steps"]), 1)
-                                        for key in ("cycles_relax", "cycles_handoff", "cycles_bookkeeping",
-                                                    "cycles_sweep_tail")},
+                                        for key in ("cycles_relax", "cycles_stage_wait", "cycles_handoff",
+                                                    "cycles_bookkeeping", "cycles_sweep_tail")},
                     "tail_cycles_per_sweep": {key[12:]: round(prof[key] / max(1, last_sweeps), 1)
                                               for key in ("cycles_tail_wrap", "cycles_tail_candidates",
                                                           "cycles_tail_lead")},

@@ -177,11 +177,12 @@ int pgc_result_stats(pgc_graph* g, int64_t* out8);
  * run; team shape of the last launch: [5] CTAs, [6] threads per CTA,
  * [7] wait-list entries over all CTAs. */
 int pgc_result_profile(pgc_graph* g, int64_t* out8);
-/* No reference counterpart.  The sweep tail of pgc_result_profile split in
- * three (SM cycles of CTA 0's thread 0, summed over the last solve):
- * out3 = {wrap-around and lap function, candidate walks, the lead's choice
- * and cycle extraction}. */
-int pgc_result_profile_tail(pgc_graph* g, int64_t* out3);
+/* No reference counterpart.  Parts of pgc_result_profile's counters (SM
+ * cycles of CTA 0's thread 0, summed over the last solve): out4 = {waits
+ * for staged streams (part of the relaxation), and the sweep tail's
+ * wrap-around with lap function, candidate walks, and the lead's choice
+ * with cycle extraction}. */
+int pgc_result_profile_detail(pgc_graph* g, int64_t* out4);
 
 /* utils::normals2d (helper/utils.cpp:93-157, bindings.cpp:27): outward
  * vertex normals of an ordered closed curve lying in a coordinate plane.

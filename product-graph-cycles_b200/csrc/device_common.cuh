@@ -51,6 +51,8 @@ struct Control {
     // parts of the sweep tail: wrap-around and lap function (up to its team
     // barrier), candidate walks (up to the lead's barrier), the lead's choice
     unsigned long long cycWrap, cycCand, cycLead;
+    // part of cycPhaseA spent waiting for the staged streams of a step
+    unsigned long long cycStage;
     // minimum-cost outputs
     double firstLb;
     int firstV;
@@ -127,7 +129,8 @@ struct EnergyArgs {
     const double* VX;    // nvx x 3
     const double* VY;    // nvy x 3
     const double* FD;    // nvx x nvy
-    const double4* quat; // nY * n (w, x, y, z) or nullptr
+    const double4* quat; // nY * quatEX distinct frames (w, x, y, z) or nullptr
+    int quatEX, quatPrune;  // |EX| and the prune flag: node -> frame map
     // plain graph
     int lengthMode;      // ("feature", "lengthnormalisation"): columns [fd, length]
     int lineIntegral;

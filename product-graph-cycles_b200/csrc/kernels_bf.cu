@@ -859,7 +859,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         // the stop is decided from the per-layer stamps after the sweep.
         const int stamp = epochBase + sweep + 1;
         const unsigned long long tRelax = isLead ? clock64() : 0;
-        unsigned long long cycRelax = 0, cycHand = 0;
+        unsigned long long cycRelax = 0, cycHand = 0, cycStage = 0;
         int sb = 0;  // buffer of the current step
         for (int l = 0; l <= p.nY; ++l) {
             for (int k = 0; k < kSteps; ++k) {
@@ -870,6 +870,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     stage_drain(st);
                     return;
                 }
+                if (isLead) cycStage += clock64() - ta;
                 const bool last = l == p.nY && k == kSteps - 1;
                 if (!last) stage_issue(p, st, s0, s1, sb ^ 1, k + 1 < kSteps ? l : l + 1, k + 1 < kSteps ? k + 1 : 0);
                 const bool any = relax_step<CT, TK, S>(p, st, sb, s0, s1, l, k);
@@ -898,6 +899,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         if (isLead) {
             p.ctl->cycPhaseA += cycRelax;
             p.ctl->cycSync += cycHand;
+            p.ctl->cycStage += cycStage;
             p.ctl->cycPhaseB += tTail - tRelax - cycRelax - cycHand;
         }
         if (stop) {

@@ -216,14 +216,17 @@ __device__ double4 frame_quaternion(const double v2[3], const double n2[3], cons
 }
 
 
+// The frame of conjugate node j in layer i depends only on a Y edge and the
+// X edge j mod |EX| (higherOrderDeformationEnergy.cpp:95-134): the Y edge is
+// i, or i - 1 for the degenerate-2d nodes |EX| <= j < 2|EX| of an unpruned
+// graph.  The reference stores 3|EX| frames per layer; every one of them is
+// a copy of frame (Y edge, X edge) of the |EX| x nY distinct ones, which is
+// all that is computed here (quat_index maps a node to its frame).
 __global__ void quaternion_kernel(QuatArgs a) {
-    const long long total = (long long)a.nY * a.n;
+    const long long total = (long long)a.nY * a.nEX;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx / a.n), j = (int)(idx % a.n);
-        const int e3 = j - (j / a.nEX) * a.nEX;
-        int i2 = i;
-        if (j >= a.nEX && j < 2 * a.nEX && !a.prune) i2 = (i + a.nY - 1) % a.nY;  // degenerate-2d node
+        const int i2 = (int)(idx / a.nEX), e3 = (int)(idx % a.nEX);
         double v2[3], n2[3], v3[3], n3[3];
         const int ya = a.EY[2 * i2], yb = a.EY[2 * i2 + 1];
         const int xa = a.EX[2 * e3], xb = a.EX[2 * e3 + 1];
@@ -248,6 +251,13 @@ __device__ __forceinline__ double robust_loss(const EnergyArgs& a, double x) {
     const double t = pow(x / a.rlC, a.rlPwr);
     const double am2 = fabs(a.rlAlpha - 2);
     return am2 / a.rlAlpha * (pow(t / am2 + 1, 0.5 * a.rlAlpha) - 1);
+}
+
+// Frame of conjugate node j of layer i (see quaternion_kernel).
+__device__ __forceinline__ long long quat_index(const EnergyArgs& a, int i, int j) {
+    const int e3 = j % a.quatEX;
+    const int i2 = (j >= a.quatEX && j < 2 * a.quatEX && !a.quatPrune) ? (i + a.nY - 1) % a.nY : i;
+    return (long long)i2 * a.quatEX + e3;
 }
 
 __global__ void ho_energy_kernel(EnergyArgs a) {
@@ -277,8 +287,8 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
         const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1], x2 = a.eX[3 * t + 2];
         double so3 = 0.0;
         if (a.quat) {
-            const long long q0 = (long long)b * a.n + a.eSrc[t];
-            const long long q1 = (long long)((b + a.eNext[t]) % a.nY) * a.n + a.eTrgt[t];
+            const long long q0 = quat_index(a, b, a.eSrc[t]);
+            const long long q1 = quat_index(a, (b + a.eNext[t]) % a.nY, a.eTrgt[t]);
             so3 = so3_distance(a.quat[q0], a.quat[q1]);
         }
         const double rl = a.quat ? robust_loss(a, so3) : rl0;
@@ -508,7 +518,7 @@ cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
-    quaternion_kernel<<<grid_for((long long)a.nY * a.n, 128), 128, 0, s>>>(a);
+    quaternion_kernel<<<grid_for((long long)a.nY * a.nEX, 128), 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {

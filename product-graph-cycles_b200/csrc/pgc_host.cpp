@@ -210,6 +210,7 @@ struct Stats {
     long long launches = 0;
     unsigned long long cycA = 0, cycB = 0, cycSync = 0, cycTail = 0;
     unsigned long long cycWrap = 0, cycCand = 0, cycLead = 0;  // parts of cycTail
+    unsigned long long cycStage = 0;                           // part of cycA
     long long steps = 0;
     long long ctas = 0, threads = 0, waitEntries = 0;  // team shape of the last launch
 };
@@ -471,7 +472,7 @@ void Graph::generate() {
         if (reg) {
             dNX.upload(NX.data(), NX.size(), s);
             dNY.upload(NY.data(), NY.size(), s);
-            dQuat.alloc((size_t)T.nY * (size_t)T.n);
+            dQuat.alloc((size_t)T.nY * (size_t)nex);
             QuatArgs q{};
             q.nEX = (int)nex;
             q.nY = T.nY;
@@ -486,6 +487,8 @@ void Graph::generate() {
             q.out = dQuat.p;
             PGC_CUDA(launch_quaternions(q, s));
             a.quat = dQuat.p;
+            a.quatEX = (int)nex;
+            a.quatPrune = prune ? 1 : 0;
         }
         e64[0].alloc((size_t)total);
         a.out0 = e64[0].p;
@@ -994,6 +997,7 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     stats.cycWrap += c.cycWrap;
     stats.cycCand += c.cycCand;
     stats.cycLead += c.cycLead;
+    stats.cycStage += c.cycStage;
     stats.steps += (long long)c.sweeps * ((long long)(T.nY + 1) * (T.entries[INTRA] == 0 ? 1 : r.K) - 1);
     stats.ctas = r.blocks;
     stats.threads = r.threads;
@@ -1976,13 +1980,14 @@ int pgc_result_profile(pgc_graph* h, int64_t* out8) {
     });
 }
 
-int pgc_result_profile_tail(pgc_graph* h, int64_t* out3) {
+int pgc_result_profile_detail(pgc_graph* h, int64_t* out4) {
     return guarded([&] {
-        if (!out3) throw pgc::Failure(PGC_ERR_ARG, "null output");
+        if (!out4) throw pgc::Failure(PGC_ERR_ARG, "null output");
         const pgc::Stats& s = h->g.stats;
-        out3[0] = (int64_t)s.cycWrap;
-        out3[1] = (int64_t)s.cycCand;
-        out3[2] = (int64_t)s.cycLead;
+        out4[0] = (int64_t)s.cycStage;
+        out4[1] = (int64_t)s.cycWrap;
+        out4[2] = (int64_t)s.cycCand;
+        out4[3] = (int64_t)s.cycLead;
     });
 }
 

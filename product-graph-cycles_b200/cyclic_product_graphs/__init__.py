@@ -67,7 +67,7 @@ _lib.pgc_compute_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
 _lib.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
 _lib.pgc_graph_info.argtypes = [_h, _lp]
 _lib.pgc_result_profile.argtypes = [_h, _lp]
-_lib.pgc_result_profile_tail.argtypes = [_h, _lp]
+_lib.pgc_result_profile_detail.argtypes = [_h, _lp]
 _lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
 _lib.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
 _lib.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
@@ -208,11 +208,11 @@ class product_graph_generator:
         """SM-cycle counters (one thread of CTA 0) and team shape of the last solve's Bellman-Ford launches."""
         buf = (ctypes.c_int64 * 8)()
         _check(_lib.pgc_result_profile(self._h, buf))
-        tail = (ctypes.c_int64 * 3)()
-        _check(_lib.pgc_result_profile_tail(self._h, tail))
+        detail = (ctypes.c_int64 * 4)()
+        _check(_lib.pgc_result_profile_detail(self._h, detail))
         return dict(zip(["cycles_relax", "cycles_bookkeeping", "cycles_handoff", "cycles_sweep_tail", "steps",
-                         "ctas", "threads", "wait_entries", "cycles_tail_wrap", "cycles_tail_candidates",
-                         "cycles_tail_lead"], list(buf) + list(tail)))
+                         "ctas", "threads", "wait_entries", "cycles_stage_wait", "cycles_tail_wrap",
+                         "cycles_tail_candidates", "cycles_tail_lead"], list(buf) + list(detail)))
 
     def graph_info(self) -> dict:
         """Sizes of the generated product graph (generates it if needed)."""
