@@ -35,9 +35,9 @@ __device__ __forceinline__ double line_integral(const EnergyArgs& a, int y0, int
 }
 
 // Visits the per-layer streams in work items of consecutive positions of one
-// layer (one division per item, not per entry): f(idx, valid, inRange) for
-// every position; `valid` marks a real edge (l >= 1 for interlayer entries,
-// l < nY for intralayer ones, template edge >= 0).  Positions are visited
+// layer (one division per item, not per entry): f(idx, l, pos, t, inRange)
+// for every position; t is the template edge, >= 0 for a real edge (l >= 1
+// for interlayer entries, l < nY for intralayer ones).  Positions are visited
 // warp-aligned, so every lane of a warp makes the same calls (warp
 // collectives inside f are allowed); lanes past the item's end get
 // inRange = false.
@@ -60,11 +60,51 @@ __device__ __forceinline__ void for_stream_layers(long long layerStride, long lo
         }
     }
 }
-template <class F>
-__device__ __forceinline__ void for_stream_entries(long long layerStride, long long interEntries, int nY,
-                                                   const int* ti, const int* tr, F f) {
-    for_stream_layers(layerStride, interEntries, nY, ti, tr,
-                      [&](long long idx, int, long long, int t, bool inRange) { f(idx, t >= 0, inRange); });
+
+// The same visit for passes that read one column: f(idx, x, valid, inRange)
+// with x = col[idx] (0 where !inRange).  Each thread first loads U positions
+// (template ids and values) and then calls f on them, so U loads of each
+// stream are in flight per thread however much f synchronises; one load at
+// a time left a pass at about a quarter of HBM bandwidth.
+template <int U, class F>
+__device__ __forceinline__ void for_stream_values(const double* col, long long layerStride, long long interEntries,
+                                                  int nY, const int* ti, const int* tr, F f) {
+    // positions inside a layer fit 32 bits (the streams of one layer are
+    // indexed by int slot offsets), which keeps the U-fold unrolled body small
+    const int stride = (int)layerStride, inter = (int)interEntries;
+    const int chunk = 8 * (int)blockDim.x;  // a multiple of U * blockDim.x
+    const int perLayer = (stride + chunk - 1) / chunk;
+    const long long items = (long long)perLayer * (nY + 1);
+    const int lane = threadIdx.x & 31, step = (int)blockDim.x;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int l = (int)(it / perLayer);
+        const int p0 = (int)(it - (long long)l * perLayer) * chunk;
+        const int p1 = min(p0 + chunk, stride);
+        const long long rowBase = (long long)l * layerStride;
+        const double* row = col + rowBase;
+        const int* tInter = l >= 1 ? ti : nullptr;
+        const int* tIntra = l < nY ? tr - inter : nullptr;
+        for (int base = p0 + (int)threadIdx.x; base - lane < p1; base += U * step) {
+            int t[U];
+            double x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int pos = base + u * step;
+                t[u] = -1;
+                x[u] = 0.0;
+                if (pos < p1) {
+                    const int* tb = pos < inter ? tInter : tIntra;
+                    if (tb) t[u] = tb[pos];
+                    x[u] = row[pos];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int pos = base + u * step;
+                if (pos - lane < p1) f(rowBase + pos, x[u], t[u] >= 0, pos < p1);
+            }
+        }
+    }
 }
 
 __global__ void plain_energy_kernel(EnergyArgs a) {
@@ -329,8 +369,9 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
 
 // ---------------------------------------------------------------------------
 // Median by radix selection over the valid entries of one column.  Keys are
-// the order-preserving 64-bit images of the doubles; 11-bit digits, six
-// passes from the most significant digit.
+// the order-preserving 64-bit images of the doubles; digits from the most
+// significant one (the host picks their width and stops when the bucket is
+// small enough to finish on the host).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long order_key(double x) {
     const unsigned long long u = (unsigned long long)__double_as_longlong(x);
@@ -339,30 +380,33 @@ __device__ __forceinline__ unsigned long long order_key(double x) {
 
 
 // Histogram of the next digit of the keys that match the current prefix.
-// Costs cluster in a few digit values (equal exponents, repeated integers),
-// so lanes holding the same digit are combined with __match_any_sync before
-// one of them updates the block's shared-memory counter.  A small persistent
-// grid keeps the final flush of the block histograms short.
+// A grid of one wave (occupancy-sized) keeps the final flush of the block
+// histograms short.
 __global__ void select_hist_kernel(SelectArgs a) {
     extern __shared__ unsigned int sh[];
     const int nb = 1 << a.bits;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    for_stream_entries(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
-                       [&](long long idx, bool valid, bool inRange) {
-                           // the value is loaded whether or not the slot is an
-                           // edge (empty slots hold NaN), so both loads overlap
-                           const double x = inRange ? a.col[idx] : 0.0;
-                           unsigned bin = 0xffffffffu;
-                           if (valid) {
-                               const unsigned long long k = order_key(x);
-                               if ((k & a.prefixMask) == a.prefix)
-                                   bin = (unsigned)((k >> a.shift) & (unsigned long long)(nb - 1));
-                           }
-                           const unsigned peers = __match_any_sync(0xffffffffu, bin);
-                           if (bin != 0xffffffffu && lane == __ffs(peers) - 1) atomicAdd(&sh[bin], (unsigned)__popc(peers));
-                       });
+    // Each thread counts a run of equal digits in a register and adds the run
+    // to the shared histogram when the digit changes: the most significant
+    // digits of one column fall into a few bins, where per-entry atomics (or
+    // warp matching) would serialise.
+    unsigned runBin = 0xffffffffu, runCnt = 0;
+    for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                         [&](long long, double x, bool valid, bool) {
+                             if (!valid) return;
+                             const unsigned long long k = order_key(x);
+                             if ((k & a.prefixMask) != a.prefix) return;
+                             const unsigned bin = (unsigned)((k >> a.shift) & (unsigned long long)(nb - 1));
+                             if (bin == runBin) {
+                                 ++runCnt;
+                             } else {
+                                 if (runCnt) atomicAdd(&sh[runBin], runCnt);
+                                 runBin = bin;
+                                 runCnt = 1;
+                             }
+                         });
+    if (runCnt) atomicAdd(&sh[runBin], runCnt);
     __syncthreads();
     for (int i = threadIdx.x; i < nb; i += blockDim.x)
         if (sh[i]) atomicAdd(a.hist + i, (unsigned long long)sh[i]);
@@ -370,9 +414,8 @@ __global__ void select_hist_kernel(SelectArgs a) {
 
 // Copies the values whose key matches (prefix, prefixMask) to out[0..cap).
 __global__ void select_compact_kernel(SelectArgs a, double* out, unsigned long long* count, long long cap) {
-    for_stream_entries(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
-                       [&](long long idx, bool valid, bool inRange) {
-                           const double x = inRange ? a.col[idx] : 0.0;
+    for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                         [&](long long, double x, bool valid, bool) {
                            if (!valid || (order_key(x) & a.prefixMask) != a.prefix) return;
                            const unsigned long long at = atomicAdd(count, 1ull);
                            if ((long long)at < cap) out[at] = x;
@@ -382,9 +425,8 @@ __global__ void select_compact_kernel(SelectArgs a, double* out, unsigned long l
 // Smallest key strictly greater than `above` (all bits); *out starts at ~0.
 __global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, unsigned long long* out) {
     unsigned long long best = ~0ull;
-    for_stream_entries(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
-                       [&](long long idx, bool valid, bool inRange) {
-                           const double x = inRange ? a.col[idx] : 0.0;
+    for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
+                         [&](long long, double x, bool valid, bool) {
                            if (!valid) return;
                            const unsigned long long k = order_key(x);
                            if (k > above && k < best) best = k;
@@ -402,10 +444,9 @@ __global__ void rescale_kernel(double* col, float* col32, long long total, long 
                                long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
                                double factor, double clip, int* exact) {
     (void)total;
-    for_stream_entries(layerStride, interEntries, nY, tedgeInter, tedgeIntra,
-                       [&](long long idx, bool valid, bool inRange) {
+    for_stream_values<4>(col, layerStride, interEntries, nY, tedgeInter, tedgeIntra,
+                         [&](long long idx, double v, bool valid, bool inRange) {
                            if (!inRange) return;
-                           const double v = col[idx];
                            if (!valid) {
                                if (col32) col32[idx] = __int_as_float(0x7fc00000);
                                return;
@@ -422,10 +463,9 @@ __global__ void to_f32_kernel(const double* col, float* col32, long long total, 
                               long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
                               int* exact) {
     (void)total;
-    for_stream_entries(layerStride, interEntries, nY, tedgeInter, tedgeIntra,
-                       [&](long long idx, bool valid, bool inRange) {
+    for_stream_values<4>(col, layerStride, interEntries, nY, tedgeInter, tedgeIntra,
+                         [&](long long idx, double x, bool valid, bool inRange) {
                            if (!inRange) return;
-                           const double x = col[idx];
                            if (!valid) {
                                col32[idx] = __int_as_float(0x7fc00000);
                                return;
