@@ -26,9 +26,9 @@ enum HoMode { NOMODE = 0, VANILLA, FEATURE, LENGTH, SO3_PLAIN, SO3_ROBUST, PENAL
 __device__ __forceinline__ double line_integral(const EnergyArgs& a, int y0, int y1, int x0, int x1) {
     double li = 0.0;
     for (int j = 0; j < 3; ++j) {
-        const double dy = a.VY[3 * y0 + j] - a.VY[3 * y1 + j];
+        const double dy = __ldg(a.VY + 3 * y0 + j) - __ldg(a.VY + 3 * y1 + j);
         li = li + dy * dy;
-        const double dx = a.VX[3 * x0 + j] - a.VX[3 * x1 + j];
+        const double dx = __ldg(a.VX + 3 * x0 + j) - __ldg(a.VX + 3 * x1 + j);
         li = li + dx * dx;
     }
     return sqrt(li);
@@ -44,19 +44,36 @@ __device__ __forceinline__ double line_integral(const EnergyArgs& a, int y0, int
 template <class F>
 __device__ __forceinline__ void for_stream_layers(long long layerStride, long long interEntries, int nY,
                                                   const int* ti, const int* tr, F f) {
-    const long long chunk = 8LL * blockDim.x;
-    const long long perLayer = (layerStride + chunk - 1) / chunk;
-    const long long items = perLayer * (nY + 1);
-    const int lane = threadIdx.x & 31;
+    // Two positions per thread and round: their template ids are loaded
+    // together, and f reads its tables through the read-only path (__ldg), so
+    // the compiler may overlap the two positions' table reads with the
+    // other's stores.  Positions inside a layer fit 32 bits.
+    constexpr int U = 2;
+    const int stride = (int)layerStride, inter = (int)interEntries;
+    const int chunk = 8 * (int)blockDim.x;  // a multiple of U * blockDim.x
+    const int perLayer = (stride + chunk - 1) / chunk;
+    const long long items = (long long)perLayer * (nY + 1);
+    const int lane = threadIdx.x & 31, step = (int)blockDim.x;
     for (long long it = blockIdx.x; it < items; it += gridDim.x) {
-        const long long l = it / perLayer;
-        const long long p0 = (it - l * perLayer) * chunk;
-        const long long p1 = p0 + chunk < layerStride ? p0 + chunk : layerStride;
-        for (long long pos = p0 + threadIdx.x; pos - lane < p1; pos += blockDim.x) {
-            const bool inRange = pos < p1;
-            int t = -1;
-            if (inRange) t = pos < interEntries ? (l >= 1 ? ti[pos] : -1) : (l < nY ? tr[pos - interEntries] : -1);
-            f(l * layerStride + pos, (int)l, pos, t, inRange);
+        const int l = (int)(it / perLayer);
+        const int p0 = (int)(it - (long long)l * perLayer) * chunk;
+        const int p1 = min(p0 + chunk, stride);
+        const long long rowBase = (long long)l * layerStride;
+        const int* tInter = l >= 1 ? ti : nullptr;
+        const int* tIntra = l < nY ? tr - inter : nullptr;
+        for (int base = p0 + (int)threadIdx.x; base - lane < p1; base += U * step) {
+            int t[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int pos = base + u * step;
+                const int* tb = pos < inter ? tInter : tIntra;
+                t[u] = (pos < p1 && tb) ? __ldg(tb + pos) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int pos = base + u * step;
+                if (pos - lane < p1) f(rowBase + pos, l, (long long)pos, t[u], pos < p1);
+            }
         }
     }
 }
@@ -118,11 +135,12 @@ __global__ void plain_energy_kernel(EnergyArgs a) {
                               return;
                           }
                           const int b = pos < a.interEntries ? l - 1 : l;
-                          const int y0 = a.EY[2 * b];
-                          const int y1 = a.eY[t] == 0 ? y0 : a.EY[2 * b + 1];
-                          const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1];
+                          const int y0 = __ldg(a.EY + 2 * b);
+                          const int y1 = __ldg(a.eY + t) == 0 ? y0 : __ldg(a.EY + 2 * b + 1);
+                          const int x0 = __ldg(a.eX + 3 * t), x1 = __ldg(a.eX + 3 * t + 1);
                           const double li = a.lineIntegral ? line_integral(a, y0, y1, x0, x1) : 1.0;
-                          const double fd = a.FD[(long long)x0 * a.nvy + y0] + a.FD[(long long)x1 * a.nvy + y1];
+                          const double fd = __ldg(a.FD + (long long)x0 * a.nvy + y0) +
+                                            __ldg(a.FD + (long long)x1 * a.nvy + y1);
                           if (a.lengthMode) {
                               a.out0[idx] = fd;
                               a.out1[idx] = li;
@@ -293,6 +311,12 @@ __device__ __forceinline__ double robust_loss(const EnergyArgs& a, double x) {
     return am2 / a.rlAlpha * (pow(t / am2 + 1, 0.5 * a.rlAlpha) - 1);
 }
 
+__device__ __forceinline__ double4 ldg_quat(const double4* q) {
+    const double2 lo = __ldg(reinterpret_cast<const double2*>(q));
+    const double2 hi = __ldg(reinterpret_cast<const double2*>(q) + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
 // Frame of conjugate node j of layer i (see quaternion_kernel).
 __device__ __forceinline__ long long quat_index(const EnergyArgs& a, int i, int j) {
     const int e3 = j % a.quatEX;
@@ -316,23 +340,24 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
             return;
         }
         const int b = pos < a.interEntries ? l - 1 : l;
-        const int s2 = a.EY[2 * b], m2 = a.EY[2 * b + 1], t2 = a.EY[2 * ((b + 1) % a.nY) + 1];
+        const int s2 = __ldg(a.EY + 2 * b), m2 = __ldg(a.EY + 2 * b + 1);
+        const int t2 = __ldg(a.EY + 2 * ((b + 1) % a.nY) + 1);
         int y0, y1, y2;
-        switch (a.eY[t]) {
+        switch (__ldg(a.eY + t)) {
             case 2: y0 = s2; y1 = s2; y2 = s2; break;
             case 3: y0 = s2; y1 = s2; y2 = m2; break;
             case 4: y0 = s2; y1 = m2; y2 = t2; break;
             default: y0 = s2; y1 = m2; y2 = m2; break;
         }
-        const int x0 = a.eX[3 * t], x1 = a.eX[3 * t + 1], x2 = a.eX[3 * t + 2];
+        const int x0 = __ldg(a.eX + 3 * t), x1 = __ldg(a.eX + 3 * t + 1), x2 = __ldg(a.eX + 3 * t + 2);
         double so3 = 0.0;
         if (a.quat) {
-            const long long q0 = quat_index(a, b, a.eSrc[t]);
-            const long long q1 = quat_index(a, (b + a.eNext[t]) % a.nY, a.eTrgt[t]);
-            so3 = so3_distance(a.quat[q0], a.quat[q1]);
+            const long long q0 = quat_index(a, b, __ldg(a.eSrc + t));
+            const long long q1 = quat_index(a, (b + __ldg(a.eNext + t)) % a.nY, __ldg(a.eTrgt + t));
+            so3 = so3_distance(ldg_quat(a.quat + q0), ldg_quat(a.quat + q1));
         }
         const double rl = a.quat ? robust_loss(a, so3) : rl0;
-        const double fd = a.FD[(long long)x2 * a.nvy + y2];
+        const double fd = __ldg(a.FD + (long long)x2 * a.nvy + y2);
         const double li = needLi ? line_integral(a, y0, y1, x0, x1) : 0.0;
         const bool degenerate = (y2 == y1 || x2 == x1);
         const int cm = a.costMode, tm = a.timeMode;
