@@ -140,7 +140,13 @@ struct EnergyArgs {
     double maxSO3, maxFd;  // already rounded through float as in the reference
     double* out0;
     double* out1;        // nullptr for one column
+    // histograms of the top kTopDigitBits of the columns' keys (the first
+    // median pass), filled when non-null; hist1 only with out1
+    unsigned long long* hist0;
+    unsigned long long* hist1;
 };
+// Width of the first digit of the median selection.
+constexpr int kTopDigitBits = 12;
 
 struct QuatArgs {
     int nEX, nY, n, prune;

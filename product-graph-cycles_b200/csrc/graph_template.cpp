@@ -16,11 +16,12 @@ namespace pgc {
 
 namespace {
 
-// Runs f(begin, end) over [0, n) split across the host's cores.
+// Runs f(begin, end) over [0, n) split across the host's cores, in parts of
+// at least `grain` items.
 template <class F>
-void parallel_for(int64_t n, F f) {
+void parallel_for(int64_t n, F f, int64_t grain = 2048) {
     const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 16), n / 2048));
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 16), n / grain));
     if (parts <= 1) {
         f((int64_t)0, n);
         return;
@@ -129,55 +130,100 @@ void build_conj(const int* EX, int64_t nEX, LayerTemplate& T) {
 
 void build_sell(LayerTemplate& T) {
     T.nslices = (T.n + 31) / 32;
-    const size_t n = (size_t)T.n;
-    T.ePos.assign((size_t)T.eBlock, -1);
-    auto part = [&](int p) {
-        // in-edges of every target in ascending template edge id (counting sort, stable)
-        std::vector<int> ptr(n + 1, 0), list;
-        for (int64_t t = 0; t < T.eBlock; ++t)
-            if ((T.eNext[(size_t)t] ? INTER : INTRA) == p) ++ptr[(size_t)T.eTrgt[(size_t)t] + 1];
-        for (size_t v = 0; v < n; ++v) ptr[v + 1] += ptr[v];
-        list.resize((size_t)ptr[n]);
-        {
-            std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-            for (int64_t t = 0; t < T.eBlock; ++t)
-                if ((T.eNext[(size_t)t] ? INTER : INTRA) == p) list[(size_t)fill[(size_t)T.eTrgt[(size_t)t]]++] = (int)t;
+    const int64_t n = T.n, nt = T.eBlock;
+    // In-edges of every (part, target) in ascending template edge id: one
+    // stable counting sort on the key part * n + target, in parallel.  Chunk
+    // c of the edge range counts its keys, the counts give each chunk its
+    // start inside every key's list, and each chunk places its edges in
+    // order.
+    const int64_t nk = 2 * n;
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 16), nt / 65536));
+    auto key = [&](int64_t t) { return (int64_t)(T.eNext[(size_t)t] ? INTER : INTRA) * n + T.eTrgt[(size_t)t]; };
+    auto range = [&](int64_t c, int64_t& t0, int64_t& t1) {
+        t0 = nt * c / chunks;
+        t1 = nt * (c + 1) / chunks;
+    };
+    std::vector<RawVec<int>> cnt((size_t)chunks);
+    parallel_for(chunks, [&](int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; ++c) {
+            RawVec<int>& h = cnt[(size_t)c];
+            h.assign((size_t)nk, 0);
+            int64_t t0, t1;
+            range(c, t0, t1);
+            for (int64_t t = t0; t < t1; ++t) ++h[(size_t)key(t)];
         }
-        std::vector<int>& sp = T.sp[p];
-        sp.assign((size_t)T.nslices + 1, 0);
+    }, 1);
+    RawVec<int> ptr((size_t)nk + 1);  // start of key k's list
+    parallel_for(nk, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) {
+            int d = 0;
+            for (int c = 0; c < chunks; ++c) d += cnt[(size_t)c][(size_t)k];
+            ptr[(size_t)k + 1] = d;
+        }
+    });
+    ptr[0] = 0;
+    for (int64_t k = 0; k < nk; ++k) ptr[(size_t)k + 1] += ptr[(size_t)k];
+    parallel_for(nk, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k) {
+            int at = ptr[(size_t)k];
+            for (int c = 0; c < chunks; ++c) {
+                const int m = cnt[(size_t)c][(size_t)k];
+                cnt[(size_t)c][(size_t)k] = at;
+                at += m;
+            }
+        }
+    });
+    RawVec<int> list((size_t)nt);
+    parallel_for(chunks, [&](int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; ++c) {
+            RawVec<int>& at = cnt[(size_t)c];
+            int64_t t0, t1;
+            range(c, t0, t1);
+            for (int64_t t = t0; t < t1; ++t) list[(size_t)at[(size_t)key(t)]++] = (int)t;
+        }
+    }, 1);
+    // slot offsets: a slice is as wide as its largest in-degree
+    for (int p = 0; p < 2; ++p) {
+        const int* pp = ptr.data() + (size_t)p * n;
+        RawVec<int>& sp = T.sp[p];
+        sp.resize((size_t)T.nslices + 1);
+        sp[0] = 0;
         for (int s = 0; s < T.nslices; ++s) {
             int w = 0;
             for (int i = 0; i < 32; ++i) {
-                const size_t v = (size_t)(32 * s + i);
-                if (v < n) w = std::max(w, ptr[v + 1] - ptr[v]);
+                const int64_t v = 32LL * s + i;
+                if (v < n) w = std::max(w, pp[v + 1] - pp[v]);
             }
             sp[(size_t)s + 1] = sp[(size_t)s] + w;
         }
         T.entries[p] = (int64_t)sp.back() * 32;
         T.src[p].resize((size_t)T.entries[p]);
         T.tedge[p].resize((size_t)T.entries[p]);
-        parallel_for(T.nslices, [&](int64_t s0, int64_t s1) {
-            for (int64_t s = s0; s < s1; ++s) {
-                const size_t r0 = (size_t)sp[(size_t)s] * 32, r1 = (size_t)sp[(size_t)s + 1] * 32;
-                std::fill(T.src[p].begin() + r0, T.src[p].begin() + r1, -1);
-                std::fill(T.tedge[p].begin() + r0, T.tedge[p].begin() + r1, -1);
-                for (int i = 0; i < 32; ++i) {
-                    const size_t v = (size_t)(32 * s + i);
-                    if (v >= n) continue;
-                    for (int j = 0; j < ptr[v + 1] - ptr[v]; ++j) {
-                        const int t = list[(size_t)(ptr[v] + j)];
-                        const size_t at = r0 + (size_t)j * 32 + (size_t)i;
-                        T.src[p][at] = T.eSrc[(size_t)t];
-                        T.tedge[p][at] = t;
-                        T.ePos[(size_t)t] = (int)at | (p << 30);
-                    }
+    }
+    T.ePos.resize((size_t)nt);  // every template edge is placed in its part below
+    parallel_for(2LL * T.nslices, [&](int64_t q0, int64_t q1) {
+        for (int64_t q = q0; q < q1; ++q) {
+            const int p = (int)(q / T.nslices);
+            const int64_t s = q - (int64_t)p * T.nslices;
+            const int* pp = ptr.data() + (size_t)p * n;
+            const RawVec<int>& sp = T.sp[p];
+            const size_t r0 = (size_t)sp[(size_t)s] * 32, r1 = (size_t)sp[(size_t)s + 1] * 32;
+            std::fill(T.src[p].begin() + r0, T.src[p].begin() + r1, -1);
+            std::fill(T.tedge[p].begin() + r0, T.tedge[p].begin() + r1, -1);
+            for (int i = 0; i < 32; ++i) {
+                const int64_t v = 32 * s + i;
+                if (v >= n) continue;
+                for (int j = 0; j < pp[v + 1] - pp[v]; ++j) {
+                    const int t = list[(size_t)(pp[v] + j)];
+                    const size_t at = r0 + (size_t)j * 32 + (size_t)i;
+                    T.src[p][at] = T.eSrc[(size_t)t];
+                    T.tedge[p][at] = t;
+                    T.ePos[(size_t)t] = (int)at | (p << 30);
                 }
             }
-        });
-    };
-    std::thread other(part, 1);
-    part(0);
-    other.join();
+        }
+    }, 64);
     // The closing layer takes the INTER edges of block nY-1 whose global
     // source id is strictly greater than n (cost_time_ratio_solver.cpp:56);
     // with two layers that drops the edges leaving node 0 of layer 1.

@@ -18,10 +18,36 @@
 // holds an edge of block l.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace pgc {
+
+// Allocator whose resize leaves elements default-initialised (unset for
+// ints): the template builder writes every element it sizes, and zeroing
+// tens of MB first was a visible part of building a large template.
+template <class T>
+struct RawAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = RawAlloc<U>;
+    };
+    RawAlloc() = default;
+    template <class U>
+    RawAlloc(const RawAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using RawVec = std::vector<T, RawAlloc<T>>;
 
 enum Part { INTER = 0, INTRA = 1 };
 
@@ -44,17 +70,17 @@ struct LayerTemplate {
     int nslices = 0;
     int64_t eBlock = 0; // edges per block
     // sliced-ELL in-edge lists, per part
-    std::vector<int> sp[2];        // nslices + 1 slot offsets
-    std::vector<int> src[2];       // 32 * slots: local source node or -1
-    std::vector<int> tedge[2];     // 32 * slots: template edge offset or -1
-    std::vector<int> srcDummy;     // INTER src list used by the closing layer
+    RawVec<int> sp[2];             // nslices + 1 slot offsets
+    RawVec<int> src[2];            // 32 * slots: local source node or -1
+    RawVec<int> tedge[2];          // 32 * slots: template edge offset or -1
+    RawVec<int> srcDummy;          // INTER src list used by the closing layer
     int64_t entries[2] = {0, 0};   // 32 * slots per part
     // per template edge offset (eBlock entries)
-    std::vector<int> eSrc, eTrgt;  // local source / target node
-    std::vector<int8_t> eNext;     // 1 if the target is in the next layer
-    std::vector<int> eX;           // 3 ints per edge: x columns of the row (x2 unused for plain)
-    std::vector<int8_t> eY;        // YPattern
-    std::vector<int> ePos;         // entry index (part encoded in bit 30) of the edge in its part
+    RawVec<int> eSrc, eTrgt;       // local source / target node
+    RawVec<int8_t> eNext;          // 1 if the target is in the next layer
+    RawVec<int> eX;                // 3 ints per edge: x columns of the row (x2 unused for plain)
+    RawVec<int8_t> eY;             // YPattern
+    RawVec<int> ePos;              // entry index (part encoded in bit 30) of the edge in its part
 
     int64_t layerStride() const { return entries[0] + entries[1]; }
     int cols() const { return conj ? 6 : 4; }

@@ -124,8 +124,53 @@ __device__ __forceinline__ void for_stream_values(const double* col, long long l
     }
 }
 
+// Order-preserving 64-bit image of a double (the median selection's keys).
+__device__ __forceinline__ unsigned long long order_key(double x) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+}
+
+// The energy kernels also count the most significant 12-bit digit of every
+// value they write (the first pass of the median selection), when the host
+// asks for it: per-thread runs of equal digits, added to shared counters when
+// the digit changes, then the block's non-zero counters to the column's
+// global histogram.  A column's values share a few exponents, so the runs
+// are long.
+constexpr int kTopBins = 1 << kTopDigitBits;
+struct DigitRun {
+    unsigned bin = 0xffffffffu, cnt = 0;
+};
+__device__ __forceinline__ void count_top_digit(unsigned* sh, DigitRun& r, double x) {
+    const unsigned bin = (unsigned)(order_key(x) >> (64 - kTopDigitBits));
+    if (bin == r.bin) {
+        ++r.cnt;
+        return;
+    }
+    if (r.cnt) atomicAdd(sh + r.bin, r.cnt);
+    r.bin = bin;
+    r.cnt = 1;
+}
+__device__ __forceinline__ void top_digit_begin(const EnergyArgs& a, unsigned* sh) {
+    if (!a.hist0) return;
+    for (int i = threadIdx.x; i < 2 * kTopBins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+}
+__device__ __forceinline__ void top_digit_end(const EnergyArgs& a, unsigned* sh, DigitRun& r0, DigitRun& r1) {
+    if (!a.hist0) return;
+    if (r0.cnt) atomicAdd(sh + r0.bin, r0.cnt);
+    if (r1.cnt) atomicAdd(sh + kTopBins + r1.bin, r1.cnt);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kTopBins; i += blockDim.x) {
+        if (sh[i]) atomicAdd(a.hist0 + i, (unsigned long long)sh[i]);
+        if (a.hist1 && sh[kTopBins + i]) atomicAdd(a.hist1 + i, (unsigned long long)sh[kTopBins + i]);
+    }
+}
+
 __global__ void plain_energy_kernel(EnergyArgs a) {
+    extern __shared__ unsigned int topSh[];  // [2][kTopBins] when a.hist0
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    DigitRun r0, r1;
+    top_digit_begin(a, topSh);
     for_stream_layers(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
                       [&](long long idx, int l, long long pos, int t, bool inRange) {
                           if (!inRange) return;
@@ -141,13 +186,15 @@ __global__ void plain_energy_kernel(EnergyArgs a) {
                           const double li = a.lineIntegral ? line_integral(a, y0, y1, x0, x1) : 1.0;
                           const double fd = __ldg(a.FD + (long long)x0 * a.nvy + y0) +
                                             __ldg(a.FD + (long long)x1 * a.nvy + y1);
-                          if (a.lengthMode) {
-                              a.out0[idx] = fd;
-                              a.out1[idx] = li;
-                          } else {
-                              a.out0[idx] = 0.5 * fd * li;
+                          const double c0 = a.lengthMode ? fd : 0.5 * fd * li;
+                          a.out0[idx] = c0;
+                          if (a.lengthMode) a.out1[idx] = li;
+                          if (a.hist0) {
+                              count_top_digit(topSh, r0, c0);
+                              if (a.hist1) count_top_digit(topSh + kTopBins, r1, li);
                           }
                       });
+    top_digit_end(a, topSh, r0, r1);
 }
 
 // Adjoint of plain_energy_kernel for the edges of a cycle: scatters
@@ -325,6 +372,9 @@ __device__ __forceinline__ long long quat_index(const EnergyArgs& a, int i, int 
 }
 
 __global__ void ho_energy_kernel(EnergyArgs a) {
+    extern __shared__ unsigned int topSh[];  // [2][kTopBins] when a.hist0
+    DigitRun r0, r1;
+    top_digit_begin(a, topSh);
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     const double twoPi = 2 * 3.14159265358979323846;
     const bool needLi = (a.costMode == LENGTH || a.timeMode == LENGTH);
@@ -389,7 +439,12 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
         }
         a.out0[idx] = c0;
         if (a.out1) a.out1[idx] = c1;
+        if (a.hist0) {
+            count_top_digit(topSh, r0, c0);
+            if (a.hist1) count_top_digit(topSh + kTopBins, r1, c1);
+        }
     });
+    top_digit_end(a, topSh, r0, r1);
 }
 
 // ---------------------------------------------------------------------------
@@ -398,11 +453,6 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
 // significant one (the host picks their width and stops when the bucket is
 // small enough to finish on the host).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long order_key(double x) {
-    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
-    return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
-}
-
 
 // Histogram of the next digit of the keys that match the current prefix.
 // A grid of one wave (occupancy-sized) keeps the final flush of the block
@@ -575,11 +625,13 @@ static int grid_for(long long total, int threads) {
 }
 
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s) {
-    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, 0), 256, 0, s>>>(a);
+    const size_t smem = a.hist0 ? 2 * kTopBins * sizeof(unsigned) : 0;
+    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, smem), 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
-    ho_energy_kernel<<<stream_grid(ho_energy_kernel, 256, 0), 256, 0, s>>>(a);
+    const size_t smem = a.hist0 ? 2 * kTopBins * sizeof(unsigned) : 0;
+    ho_energy_kernel<<<stream_grid(ho_energy_kernel, 256, smem), 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {

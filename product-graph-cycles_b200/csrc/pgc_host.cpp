@@ -307,13 +307,19 @@ class Graph {
 
     // -------------------------------------------------------------------
     void generate();
+    void count_top_digits(EnergyArgs& a);
     void upload_template();
     void ensure_generated() {
         if (!generated) generate();
     }
     void energy_changed() {
         f32Known[0] = f32Known[1] = false;
+        topHistValid[0] = topHistValid[1] = false;
     }
+    // First median pass of each column, counted by the energy kernel that
+    // wrote it; valid until the column changes.
+    DBuf<unsigned long long> topHist[2];
+    bool topHistValid[2] = {false, false};
     EnergyArgs energy_args() const;
 
     // What the adjoint of the last solve needs: the product of the rescale
@@ -389,10 +395,21 @@ void Graph::upload_template() {
         dSrc[p].upload(T.src[p].data(), T.src[p].size(), s);
         dTedge[p].upload(T.tedge[p].data(), T.tedge[p].size(), s);
     }
-    dSrcDummy.upload(T.srcDummy.data(), T.srcDummy.size(), s);
-    dESrc.upload(T.eSrc.data(), T.eSrc.size(), s);
-    dETrgt.upload(T.eTrgt.data(), T.eTrgt.size(), s);
-    dENext.upload(T.eNext.data(), T.eNext.size(), s);
+    // The closing layer's source list differs from the interlayer one only
+    // with two layers; otherwise the kernels read the interlayer list.
+    if (T.nY == 2) dSrcDummy.upload(T.srcDummy.data(), T.srcDummy.size(), s);
+    else dSrcDummy.release();
+    // Template edge endpoints are read on the device only by the SO(3)
+    // energies (frames of the edge's source and target).
+    if (conj && reg) {
+        dESrc.upload(T.eSrc.data(), T.eSrc.size(), s);
+        dETrgt.upload(T.eTrgt.data(), T.eTrgt.size(), s);
+        dENext.upload(T.eNext.data(), T.eNext.size(), s);
+    } else {
+        dESrc.release();
+        dETrgt.release();
+        dENext.release();
+    }
     dEXcols.upload(T.eX.data(), T.eX.size(), s);
     dEYpat.upload(T.eY.data(), T.eY.size(), s);
     dEY.upload(EY.data(), EY.size(), s);
@@ -430,6 +447,16 @@ EnergyArgs Graph::energy_args() const {
 // ---------------------------------------------------------------------------
 // generate(): product_graph_generators.cpp:21-89
 // ---------------------------------------------------------------------------
+// Lets the energy kernel count the first median digit of its columns.
+void Graph::count_top_digits(EnergyArgs& a) {
+    for (int c = 0; c < ncols; ++c) {
+        topHist[c].alloc((size_t)1 << kTopDigitBits);
+        topHist[c].zero(stream);
+    }
+    a.hist0 = topHist[0].p;
+    a.hist1 = ncols > 1 ? topHist[1].p : nullptr;
+}
+
 void Graph::generate() {
     if (conj && !normalsGiven)
         throw Failure(PGC_ERR_STATE, "cannot generate the conjugate product graph without normals (set_normals)");
@@ -452,6 +479,7 @@ void Graph::generate() {
             e64[1].alloc((size_t)total);
             a.out1 = e64[1].p;
         }
+        count_top_digits(a);
         PGC_CUDA(launch_plain_energy(a, s));
     } else {
         const int cm = string_to_mode(costName), tm = string_to_mode(timeName);
@@ -496,11 +524,13 @@ void Graph::generate() {
             e64[1].alloc((size_t)total);
             a.out1 = e64[1].p;
         }
+        count_top_digits(a);
         PGC_CUDA(launch_ho_energy(a, s));
         dQuat.release();
     }
     PGC_CUDA(sync_stream());
     energy_changed();
+    for (int c = 0; c < ncols; ++c) topHistValid[c] = true;
     colScale[0] = colScale[1] = 1.0;
     adjKind = 0;
     generated = true;
@@ -510,6 +540,13 @@ void Graph::generate() {
 // Rescaling: cost_time_ratio_solver.cpp:709-721 with utils::median
 // (utils.hpp:196-209).  The k-th value is found by radix selection.
 // ---------------------------------------------------------------------------
+// The device's order-preserving 64-bit image of a double (order_key).
+static unsigned long long host_order_key(double x) {
+    unsigned long long u;
+    std::memcpy(&u, &x, sizeof(u));
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+}
+
 double Graph::median_of_column(int col) {
     const long long stride = T.layerStride();
     const long long total = (long long)(T.nY + 1) * stride;
@@ -520,7 +557,7 @@ double Graph::median_of_column(int col) {
     // holding rank k has at most kCompact members it is copied out and
     // finished on the host.  If rank k is the largest of its bucket, rank k+1
     // is the smallest key above the bucket (one reduction pass).
-    const int bits = 12;
+    const int bits = kTopDigitBits;
     const long long kCompact = 1 << 16;
     DBuf<unsigned long long> hist, cnt;
     DBuf<double> band;
@@ -554,10 +591,15 @@ double Graph::median_of_column(int col) {
         a.prefixMask = mask;
         a.shift = shift;
         a.bits = b;
-        PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
-        PGC_CUDA(launch_select_hist(a, stream));
-        stats.launches++;
-        d2h(h.data(), hist.p, sizeof(unsigned long long) << b);
+        if (mask == 0 && b == kTopDigitBits && topHistValid[col]) {
+            // the first digit was counted when the column was written
+            d2h(h.data(), topHist[col].p, sizeof(unsigned long long) << b);
+        } else {
+            PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
+            PGC_CUDA(launch_select_hist(a, stream));
+            stats.launches++;
+            d2h(h.data(), hist.p, sizeof(unsigned long long) << b);
+        }
         PGC_CUDA(sync_stream());
         int digit = 0;
         long long acc = 0;
@@ -587,9 +629,12 @@ double Graph::median_of_column(int col) {
         std::vector<double> vals((size_t)bucket);
         d2h(vals.data(), band.p, sizeof(double) * (size_t)bucket);
         PGC_CUDA(sync_stream());
-        std::sort(vals.begin(), vals.end());
+        // the bucket's order statistics rank (and rank + 1) in the key order
+        // of the passes (numeric order for every non-NaN value)
+        auto keyLess = [](double x, double y) { return host_order_key(x) < host_order_key(y); };
+        std::nth_element(vals.begin(), vals.begin() + rank, vals.end(), keyLess);
         xk = vals[(size_t)rank];
-        if (even && rank + 1 < bucket) xk1 = vals[(size_t)rank + 1];
+        if (even && rank + 1 < bucket) xk1 = *std::min_element(vals.begin() + rank + 1, vals.end(), keyLess);
         bucketTop = prefix | ~mask;
     }
     if (!even) return xk;
@@ -622,6 +667,7 @@ void Graph::rescale_column(int col, double scaling) {
     PGC_CUDA(sync_stream());
     f32Valid[col] = exact != 0;
     f32Known[col] = true;
+    topHistValid[col] = false;
     colScale[col] *= factor;
 }
 
@@ -921,7 +967,7 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.spInter = dSp[INTER].p;
     p.spIntra = dSp[INTRA].p;
     p.srcInter = dSrc[INTER].p;
-    p.srcDummy = dSrcDummy.p;
+    p.srcDummy = dSrcDummy.p ? dSrcDummy.p : dSrc[INTER].p;
     p.srcIntra = dSrc[INTRA].p;
     p.interEntries = T.entries[INTER];
     p.intraEntries = T.entries[INTRA];
@@ -1039,7 +1085,7 @@ void Graph::lookup_pairs(const std::vector<int>& src, const std::vector<int>& tr
     a.spInter = dSp[INTER].p;
     a.spIntra = dSp[INTRA].p;
     a.srcInter = dSrc[INTER].p;
-    a.srcDummy = dSrcDummy.p;
+    a.srcDummy = dSrcDummy.p ? dSrcDummy.p : dSrc[INTER].p;
     a.srcIntra = dSrc[INTRA].p;
     a.tedgeInter = dTedge[INTER].p;
     a.tedgeIntra = dTedge[INTRA].p;
