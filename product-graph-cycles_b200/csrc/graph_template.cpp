@@ -10,26 +10,126 @@
 
 #include <algorithm>
 #include <climits>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 
 namespace pgc {
 
 namespace {
 
+// A pool of host threads that lives for the process: creating and joining
+// a thread per part cost about 50 us each, most of a template build's time
+// on a 16-core host.  One job runs at a time; a caller that finds the pool
+// busy (templates of a batch built by concurrent workers) runs its loop
+// itself.
+class WorkerPool {
+  public:
+    static WorkerPool& get() {
+        static WorkerPool pool;
+        return pool;
+    }
+    int size() const { return (int)threads_.size() + 1; }
+    // Runs f(i) for every i in [0, parts) on the pool and the caller;
+    // returns false, having run nothing, when another job holds the pool.
+    template <class F>
+    bool run(int parts, F& f) {
+        std::unique_lock<std::mutex> own(busy_, std::try_to_lock);
+        if (!own.owns_lock()) return false;
+        Job job;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            job.call = [](void* ctx, int i) { (*static_cast<F*>(ctx))(i); };
+            job.ctx = &f;
+            job.parts = parts;
+            job.gen = ++gen_;
+            job_ = job;
+            remaining_ = parts;
+            // parts are claimed from (generation, next index): a thread still
+            // holding an older job's snapshot can claim nothing of this one
+            next_.store((uint64_t)job.gen << 32);
+        }
+        cv_.notify_all();
+        work(job);
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return remaining_ == 0; });
+        return true;
+    }
+
+  private:
+    struct Job {
+        void (*call)(void*, int) = nullptr;
+        void* ctx = nullptr;
+        int parts = 0;
+        uint32_t gen = 0;
+    };
+    WorkerPool() {
+        const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+        for (int i = 1; i < std::min(hw, 16); ++i) threads_.emplace_back([this] { loop(); });
+    }
+    ~WorkerPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    void work(const Job& job) {
+        int done = 0;
+        uint64_t v = next_.load();
+        for (;;) {
+            if ((uint32_t)(v >> 32) != job.gen) break;
+            const int i = (int)(uint32_t)v;
+            if (i >= job.parts) break;
+            if (!next_.compare_exchange_weak(v, v + 1)) continue;
+            job.call(job.ctx, i);
+            ++done;
+            v = next_.load();
+        }
+        if (done) {
+            std::lock_guard<std::mutex> lk(m_);
+            remaining_ -= done;
+            if (remaining_ == 0) done_.notify_all();
+        }
+    }
+    void loop() {
+        uint32_t seen = 0;
+        for (;;) {
+            Job job;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                job = job_;
+            }
+            work(job);
+        }
+    }
+    std::vector<std::thread> threads_;
+    std::mutex busy_, m_;
+    std::condition_variable cv_, done_;
+    Job job_;
+    int remaining_ = 0;
+    std::atomic<uint64_t> next_{0};
+    uint32_t gen_ = 0;
+    bool stop_ = false;
+};
+
 // Runs f(begin, end) over [0, n) split across the host's cores, in parts of
 // at least `grain` items.
 template <class F>
 void parallel_for(int64_t n, F f, int64_t grain = 2048) {
-    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 16), n / grain));
+    WorkerPool& pool = WorkerPool::get();
+    const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(pool.size(), n / grain));
     if (parts <= 1) {
         f((int64_t)0, n);
         return;
     }
-    std::vector<std::thread> th;
-    for (int64_t i = 1; i < parts; ++i) th.emplace_back(f, n * i / parts, n * (i + 1) / parts);
-    f((int64_t)0, n / parts);
-    for (auto& t : th) t.join();
+    auto part = [&](int i) { f(n * i / parts, n * (i + 1) / parts); };
+    if (!pool.run((int)parts, part)) f((int64_t)0, n);
 }
 
 struct EdgeOut {
@@ -137,8 +237,7 @@ void build_sell(LayerTemplate& T) {
     // start inside every key's list, and each chunk places its edges in
     // order.
     const int64_t nk = 2 * n;
-    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 16), nt / 65536));
+    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(WorkerPool::get().size(), nt / 65536));
     auto key = [&](int64_t t) { return (int64_t)(T.eNext[(size_t)t] ? INTER : INTRA) * n + T.eTrgt[(size_t)t]; };
     auto range = [&](int64_t c, int64_t& t0, int64_t& t1) {
         t0 = nt * c / chunks;
@@ -226,11 +325,13 @@ void build_sell(LayerTemplate& T) {
     }, 64);
     // The closing layer takes the INTER edges of block nY-1 whose global
     // source id is strictly greater than n (cost_time_ratio_solver.cpp:56);
-    // with two layers that drops the edges leaving node 0 of layer 1.
-    T.srcDummy = T.src[INTER];
-    if (T.nY == 2)
+    // with two layers that drops the edges leaving node 0 of layer 1.  With
+    // more layers the list equals the INTER one and is not stored.
+    if (T.nY == 2) {
+        T.srcDummy = T.src[INTER];
         for (auto& s : T.srcDummy)
             if (s == 0) s = -1;
+    }
 }
 
 }  // namespace

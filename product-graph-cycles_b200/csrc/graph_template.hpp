@@ -73,7 +73,7 @@ struct LayerTemplate {
     RawVec<int> sp[2];             // nslices + 1 slot offsets
     RawVec<int> src[2];            // 32 * slots: local source node or -1
     RawVec<int> tedge[2];          // 32 * slots: template edge offset or -1
-    RawVec<int> srcDummy;          // INTER src list used by the closing layer
+    RawVec<int> srcDummy;          // INTER src list of the closing layer; stored for nY == 2 only (else == src[INTER])
     int64_t entries[2] = {0, 0};   // 32 * slots per part
     // per template edge offset (eBlock entries)
     RawVec<int> eSrc, eTrgt;       // local source / target node
