@@ -87,6 +87,7 @@ struct BfParams {
     int flagSync;                  // 1: neighbour hand-offs between steps, 0: team barrier
     int maxCtaSlices;              // most slices any CTA owns
     int rowCap;                    // rows (of 32 entries) one step buffer holds
+    int stageSrcOnly;              // 1: the buffers hold source indices only (costs, times prefetched to L2)
     int* lapNext;                  // [n]
     int* lapSteps;                 // [n]
     int* mark;                     // [n] visited marks for literal walks

@@ -269,6 +269,11 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
         : "memory");
 }
 
+// Brings [src, src + bytes) into L2 (16-byte aligned, a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // Shared-memory state of a CTA: its slices' row offsets per part (staged
 // once per launch) and the two step buffers.
 struct Stage {
@@ -278,6 +283,7 @@ struct Stage {
     char* buf1;
     unsigned long long* bar;     // [2]
     int rowCap;                  // rows one buffer holds
+    bool srcOnly;                // buffers hold the source indices only; costs and times are read in place
     unsigned phase;              // bit b: parity of buffer b's next completion
     unsigned pending;            // bit b: copies issued into buffer b, not yet waited for
     int costBytes, timeBytes;    // bytes per entry of the cost and time streams
@@ -305,6 +311,15 @@ __device__ void stage_issue(const BfParams& p, Stage& st, int s0, int s1, int b,
     char* dst = st.buf(b);
     const unsigned bs = (unsigned)(cnt * 4), bc = (unsigned)(cnt * st.costBytes), bt = (unsigned)(cnt * st.timeBytes);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (st.srcOnly) {
+        // the costs and times are read in place during the step; bring them
+        // into L2 meanwhile, so those reads overlap the gathers at L2 latency
+        mbar_expect(st.bar + b, bs);
+        bulk_load(dst, src + e0, bs, st.bar + b);
+        bulk_prefetch_l2((const char*)p.cost + (base + e0) * st.costBytes, bc);
+        if (bt) bulk_prefetch_l2((const char*)p.time + (base + e0) * st.timeBytes, bt);
+        return;
+    }
     mbar_expect(st.bar + b, bs + bc + bt);
     bulk_load(dst, src + e0, bs, st.bar + b);
     bulk_load(dst + (size_t)st.rowCap * 32 * 4, (const char*)p.cost + (base + e0) * st.costBytes, bc, st.bar + b);
@@ -445,6 +460,13 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
     const double ub = p.ub;
     bool any = false;
     for (int s = s0 + (int)(threadIdx.x >> 5); s < s1; s += nwarps) {
+        // A slice without rows in this step's part always writes (+inf,
+        // unknown, 0).  From layer 3 on, its row slot already holds exactly
+        // that, written two layers before by the same kind of step (layers 1
+        // and 2 still overwrite what layer 0's start values and the previous
+        // sweep left), so the writes -- most of such a slice's cost -- are
+        // skipped.
+        if (l >= 3 && spl[s + 1 - s0] == spl[s - s0]) continue;
         const int v = s * 32 + lane;
         const bool valid = v < n;
         const size_t me = cur + (size_t)v * Kp + k;
@@ -504,16 +526,18 @@ __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, i
     const int* spl = st.spl(part);
     const int r0 = spl[0];
     StepView v;
-    // the step's streams from row r0 on: staged in shared memory, or read in
-    // place when a step of this CTA does not fit a buffer (rowCap == 0)
-    if (st.rowCap > 0) {
+    // the step's streams from row r0 on: staged in shared memory; or the
+    // source indices staged and the costs and times read in place
+    // (srcOnly); or all read in place when no buffer fits (rowCap == 0)
+    if (st.rowCap > 0 && !st.srcOnly) {
         char* b = st.buf(sb);
         v.src = reinterpret_cast<const int*>(b);
         v.cost = b + (size_t)st.rowCap * 32 * 4;
         v.time = b + (size_t)st.rowCap * 32 * (4 + sizeof(CT));
     } else {
         const size_t off = (size_t)l * (size_t)p.layerStride + (inter ? 0 : (size_t)p.interEntries) + (size_t)r0 * 32;
-        v.src = (inter ? (l == p.nY ? p.srcDummy : p.srcInter) : p.srcIntra) + (size_t)r0 * 32;
+        v.src = st.rowCap > 0 ? reinterpret_cast<const int*>(st.buf(sb))
+                              : (inter ? (l == p.nY ? p.srcDummy : p.srcInter) : p.srcIntra) + (size_t)r0 * 32;
         v.cost = reinterpret_cast<const CT*>(p.cost) + off;
         v.time = TK == 0 ? nullptr : reinterpret_cast<const char*>(p.time) + off * st.timeBytes;
     }
@@ -775,7 +799,9 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         st.costBytes = sizeof(CT);
         st.timeBytes = TK == 1 ? 4 : TK == 2 ? 8 : 0;
         st.rowCap = p.rowCap;
-        const size_t bufBytes = bf_stage_buffer_bytes(p.rowCap, st.costBytes, st.timeBytes);
+        st.srcOnly = p.stageSrcOnly != 0;
+        const size_t bufBytes =
+            bf_stage_buffer_bytes(p.rowCap, st.srcOnly ? 0 : st.costBytes, st.srcOnly ? 0 : st.timeBytes);
         st.buf0 = smem + bf_stage_offset(p.maxCtaSlices);
         st.buf1 = st.buf0 + bufBytes;
         st.bar = stageBar;

@@ -251,6 +251,7 @@ class Graph {
     DBuf<int> wCtaSlice, wWaitPtr, wWaitIdx;
     DBuf<unsigned> wStepDone;
     std::vector<int> ctaCut;   // slice ranges of the uploaded partition
+    mutable std::map<std::string, std::vector<int>> cutCache;  // cta_cuts per (blocks, K, warps)
     int cutBlocks = -1, cutK = -1, cutWarps = -1;  // the partition ctaCut was made for
     long long waitEntries = 0;  // wait-list entries over all CTAs of the current partition
     DBuf<int> wPred, wLapNext, wLapSteps, wMark, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
@@ -359,6 +360,7 @@ class Graph {
         int flagSync;       // neighbour hand-offs between steps (multi-CTA teams)
         int maxCtaSlices;   // most slices any CTA owns
         int rowCap;         // rows a step buffer holds (0: streams read in place)
+        int stageSrcOnly;   // the buffers hold source indices only
         size_t smemBytes;   // dynamic shared memory per CTA
     };
     Run prepare_run(int K, bool ratio);
@@ -765,9 +767,20 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     const size_t fixed = r.sharedTables ? tables : 0;
     size_t need = stage_need(blocks, maxSl, rowCap);
     r.rowCap = rowCap;
-    if (!stageOn || fixed + need > smemCap) {
-        r.rowCap = 0;  // read the streams in place
-        need = bf_stage_offset(maxSl);
+    r.stageSrcOnly = 0;
+    // PGC_BF_STAGE_SRC: 0 never stage the source indices alone, 1 (default)
+    // when the whole streams do not fit, 2 always (tests)
+    const int srcMode = env_int("PGC_BF_STAGE_SRC", 1);
+    if (!stageOn || fixed + need > smemCap || srcMode == 2) {
+        // the source indices alone, the costs and times prefetched to L2
+        const size_t srcOnly = bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(rowCap, 0, 0);
+        if (stageOn && srcMode && fixed + srcOnly <= smemCap) {
+            r.stageSrcOnly = 1;
+            need = srcOnly;
+        } else {
+            r.rowCap = 0;  // read the streams in place
+            need = bf_stage_offset(maxSl);
+        }
     }
     r.maxCtaSlices = maxSl;
     r.smemBytes = fixed + need;
@@ -781,6 +794,7 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
             blocks = sms * perSm;
             stage_need(blocks, maxSl, rowCap);
             r.rowCap = 0;
+            r.stageSrcOnly = 0;
             r.maxCtaSlices = maxSl;
             r.smemBytes = bf_stage_offset(maxSl);
         }
@@ -797,71 +811,94 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
 // Contiguous slice ranges for `blocks` CTAs of `warps` warps with balanced
 // step times.  A warp relaxes the CTA's slices round-robin, and one slice of
 // one step costs it about (gather batches + 1) memory latencies: the batches
-// of its rows and the epilogue (the winner's record, the stores); a slice
-// without rows only stores.  A CTA's time per layer is its slowest warp in
-// the interlayer step plus K - 1 times its slowest warp in an intralayer
-// step (those steps run only when the layer has intralayer edges).  The
-// cost of a range never grows when the range shrinks, so filling CTAs
-// greedily up to a bound is optimal for that bound; a binary search finds
-// the smallest bound that fits in `blocks` CTAs.  Costs are in quarter
-// latencies.
+// of its rows and the epilogue (the winner's record, the stores).  A slice
+// without rows skips its step from layer 3 on and costs a loop iteration.
+// Steps are coupled across the team by the hand-offs, so a layer costs the
+// slowest warp of any CTA in the interlayer step plus K - 1 times the
+// slowest in an intralayer step (those run only when the layer has
+// intralayer edges).  The cuts therefore bound the two kinds separately:
+// for bounds (bi, bj) CTAs are filled greedily while their slowest warps
+// stay within both -- optimal for the pair, since a range's costs never grow
+// when it shrinks -- and the pair with the smallest bi + (K - 1) bj that
+// fits in `blocks` CTAs is kept (bj in steps of one latency, bi by binary
+// search).  Costs are in 1/32 of a latency.  Cached per (blocks, K, warps).
 std::vector<int> Graph::cta_cuts(int blocks, int K, int warps) const {
     const int ns = T.nslices;
     std::vector<int> cut((size_t)blocks + 1, ns);
     cut[0] = 0;
     if (blocks <= 1 || ns == 0) return cut;
     warps = std::max(1, warps);
-    const bool intra = T.entries[INTRA] > 0;
+    const std::string key = std::to_string(blocks) + "/" + std::to_string(K) + "/" + std::to_string(warps);
+    {
+        const auto it = cutCache.find(key);
+        if (it != cutCache.end()) return it->second;
+    }
+    const bool intra = T.entries[INTRA] > 0 && K > 1;
     const int rb[2] = {K <= 4 ? bf_rows_per_batch(K) : 1, bf_rows_per_batch(1)};
     std::vector<long long> w[2];
-    long long lo = 0, hi = 0;
+    long long lo[2] = {0, 0}, hi[2] = {0, 0};
     for (int p = 0; p < 2; ++p) {
         w[p].resize((size_t)ns);
-        const long long reps = p == 0 ? 1 : (intra ? K - 1 : 0);
         for (int s = 0; s < ns; ++s) {
             const int rows = T.sp[p][(size_t)s + 1] - T.sp[p][(size_t)s];
-            w[p][(size_t)s] = rows > 0 ? 4LL * ((rows + rb[p] - 1) / rb[p] + 1) : 1;
-            lo = std::max(lo, reps * w[p][(size_t)s]);
-            hi += reps * w[p][(size_t)s];
+            w[p][(size_t)s] = (p == 1 && !intra) ? 0 : rows > 0 ? 32LL * ((rows + rb[p] - 1) / rb[p] + 1) : 1;
+            lo[p] = std::max(lo[p], w[p][(size_t)s]);
+            hi[p] += w[p][(size_t)s];
         }
     }
-    const long long repIntra = intra ? K - 1 : 0;
     std::vector<long long> acc[2] = {std::vector<long long>((size_t)warps), std::vector<long long>((size_t)warps)};
-    // fills CTAs greedily under `bound`; returns the CTAs used (cuts in c when given)
-    auto fill = [&](long long bound, std::vector<int>* c) -> int {
+    // fills CTAs greedily under (bi, bj); returns the CTAs used (cuts in c when given)
+    auto fill = [&](long long bi, long long bj, std::vector<int>* c) -> int {
         int used = 1, start = 0;
-        long long m[2] = {0, 0};
         std::fill(acc[0].begin(), acc[0].end(), 0);
         std::fill(acc[1].begin(), acc[1].end(), 0);
         for (int s = 0; s < ns; ++s) {
             int i = (s - start) % warps;
-            long long a0 = acc[0][(size_t)i] + w[0][(size_t)s], a1 = acc[1][(size_t)i] + w[1][(size_t)s];
-            if (s > start && std::max(m[0], a0) + repIntra * std::max(m[1], a1) > bound) {
+            if (s > start && (acc[0][(size_t)i] + w[0][(size_t)s] > bi || acc[1][(size_t)i] + w[1][(size_t)s] > bj)) {
                 if (c && used < blocks) (*c)[(size_t)used] = s;
-                ++used;
+                if (++used > blocks && !c) return used;
                 start = s;
-                m[0] = m[1] = 0;
                 std::fill(acc[0].begin(), acc[0].end(), 0);
                 std::fill(acc[1].begin(), acc[1].end(), 0);
                 i = 0;
-                a0 = w[0][(size_t)s];
-                a1 = w[1][(size_t)s];
             }
-            acc[0][(size_t)i] = a0;
-            acc[1][(size_t)i] = a1;
-            m[0] = std::max(m[0], a0);
-            m[1] = std::max(m[1], a1);
+            acc[0][(size_t)i] += w[0][(size_t)s];
+            acc[1][(size_t)i] += w[1][(size_t)s];
         }
         return used;
     };
-    while (lo < hi) {
-        const long long mid = lo + (hi - lo) / 2;
-        if (fill(mid, nullptr) <= blocks) hi = mid;
-        else lo = mid + 1;
+    const long long reps = intra ? K - 1 : 0;
+    // the smallest intralayer bound that fits at all, then up from there
+    long long j0 = lo[1], j1 = hi[1];
+    while (j0 < j1) {
+        const long long mid = j0 + (j1 - j0) / 2;
+        if (fill(hi[0], mid, nullptr) <= blocks) j1 = mid;
+        else j0 = mid + 1;
     }
-    const int used = fill(lo, &cut);
+    long long bestI = -1, bestJ = -1, bestCost = 0;
+    for (long long bj = j0, tries = 0; tries < 64; bj += 32, ++tries) {
+        if (bestI >= 0 && reps * bj >= bestCost) break;
+        if (bj > hi[1]) bj = hi[1];
+        if (fill(hi[0], bj, nullptr) <= blocks) {
+            long long a = lo[0], b = hi[0];
+            while (a < b) {
+                const long long mid = a + (b - a) / 2;
+                if (fill(mid, bj, nullptr) <= blocks) b = mid;
+                else a = mid + 1;
+            }
+            const long long cost = a + reps * bj;
+            if (bestI < 0 || cost < bestCost) {
+                bestI = a;
+                bestJ = bj;
+                bestCost = cost;
+            }
+        }
+        if (bj >= hi[1] || !intra) break;
+    }
+    const int used = fill(bestI, bestJ, &cut);
     // CTAs past the last range keep empty ranges at the end
     for (int c = used; c < blocks; ++c) cut[(size_t)c] = ns;
+    cutCache[key] = cut;
     return cut;
 }
 
@@ -986,6 +1023,7 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.flagSync = r.flagSync;
     p.maxCtaSlices = r.maxCtaSlices;
     p.rowCap = r.rowCap;
+    p.stageSrcOnly = r.stageSrcOnly;
     p.lapNext = wLapNext.p;
     p.lapSteps = wLapSteps.p;
     p.mark = wMark.p;

@@ -137,6 +137,20 @@ def test_multi_cta_team(cpg, oracle, monkeypatch):
     _same(g.solve_with_minimum_cost("dijkstragpu", 3), o.solve_with_minimum_cost("dijkstracpu", 3))
 
 
+@pytest.mark.parametrize("stage", ["2", "0"])
+def test_staging_modes(cpg, oracle, monkeypatch, stage):
+    """Source indices staged alone (costs and times read in place after an
+    L2 prefetch), and no staging at all, on a multi-CTA conjugate team."""
+    monkeypatch.setenv("PGC_BF_BLOCKS", "12")
+    monkeypatch.setenv("PGC_BF_STAGE_SRC", stage)
+    if stage == "0":
+        monkeypatch.setenv("PGC_BF_STAGE", "0")
+    p = _pair(nv=300, ny=10, dim=8, seed=21)
+    g, o = _both(cpg, oracle, p, conj=True, cost="vanilla", time="lengthnormalisation")
+    _same(g.solve_with_cost_time_ratio("lawlergpu", 3), o.solve_with_cost_time_ratio("lawlercpu", 3))
+    _same(g.solve_with_minimum_cost("dijkstragpu", 3), o.solve_with_minimum_cost("dijkstracpu", 3))
+
+
 def test_conjugate_multi_cta(cpg, oracle, monkeypatch):
     monkeypatch.setenv("PGC_BF_BLOCKS", "16")
     p = _pair(nv=300, ny=10, dim=8, seed=21)
