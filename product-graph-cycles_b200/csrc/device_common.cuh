@@ -209,9 +209,10 @@ __host__ __device__ inline size_t bf_shared_table_bytes(int n, int Kp) {
     const size_t b = (size_t)2 * n * Kp * (sizeof(double) + sizeof(int2)) + (size_t)n * sizeof(double);
     return (b + 127) & ~(size_t)127;
 }
-// Offset of the first step buffer after the staged row offsets (128-byte aligned).
+// Offset of the first step buffer after the staged row offsets and the
+// lists of slices with rows, both per part (128-byte aligned).
 __host__ __device__ inline size_t bf_stage_offset(int maxCtaSlices) {
-    return ((size_t)2 * (maxCtaSlices + 1) * sizeof(int) + 127) & ~(size_t)127;
+    return ((size_t)(2 * (maxCtaSlices + 1) + 2 * maxCtaSlices) * sizeof(int) + 127) & ~(size_t)127;
 }
 // Bytes of one step buffer: source index, cost and time of rowCap rows.
 __host__ __device__ inline size_t bf_stage_buffer_bytes(int rowCap, int costBytes, int timeBytes) {

@@ -279,6 +279,9 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes
 struct Stage {
     const int* splInter;         // sp[s0 + i] of the interlayer part, i = 0..s1-s0
     const int* splIntra;         // same for the intralayer part
+    const int* actInter;         // the CTA's slices (s - s0) with interlayer rows
+    const int* actIntra;         // ... with intralayer rows
+    int nActInter, nActIntra;
     char* buf0;
     char* buf1;
     unsigned long long* bar;     // [2]
@@ -288,6 +291,8 @@ struct Stage {
     unsigned pending;            // bit b: copies issued into buffer b, not yet waited for
     int costBytes, timeBytes;    // bytes per entry of the cost and time streams
     __device__ const int* spl(int part) const { return part ? splIntra : splInter; }
+    __device__ const int* act(int part) const { return part ? actIntra : actInter; }
+    __device__ int nAct(int part) const { return part ? nActIntra : nActInter; }
     __device__ char* buf(int b) const { return b ? buf1 : buf0; }
 };
 
@@ -449,7 +454,8 @@ __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, i
 }
 
 template <class CT, int TK, bool S, int NK>
-__device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* spl, int s0, int s1, int l, int k) {
+__device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* spl, const int* act, int nAct, int s0,
+                             int s1, int l, int k) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const size_t cur = (size_t)(l & 1) * n * Kp;
     const bool empty = step_empty(p, l, k);
@@ -459,14 +465,18 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
     const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const double ub = p.ub;
     bool any = false;
-    for (int s = s0 + (int)(threadIdx.x >> 5); s < s1; s += nwarps) {
-        // A slice without rows in this step's part always writes (+inf,
-        // unknown, 0).  From layer 3 on, its row slot already holds exactly
-        // that, written two layers before by the same kind of step (layers 1
-        // and 2 still overwrite what layer 0's start values and the previous
-        // sweep left), so the writes -- most of such a slice's cost -- are
-        // skipped.
-        if (l >= 3 && spl[s + 1 - s0] == spl[s - s0]) continue;
+    // A slice without rows in this step's part only writes (+inf, unknown
+    // or end of walk, 0): its nodes are never reached through this part.
+    // Their row slots already hold +inf -- from the set-up, or written by an
+    // earlier step of the same kind -- except depth 0 of the even layers,
+    // whose parity row also holds layer 0's start values: the interlayer
+    // step of layer 2 overwrites those.  So that step and the layer-0 steps
+    // visit every slice of the CTA; the others only the slices with rows
+    // (the origins of a never-reached record are never read).
+    const bool all = l == 0 || (l == 2 && k == 0);
+    const int count = all ? s1 - s0 : nAct;
+    for (int i = (int)(threadIdx.x >> 5); i < count; i += nwarps) {
+        const int s = s0 + (all ? i : act[i]);
         const int v = s * 32 + lane;
         const bool valid = v < n;
         const size_t me = cur + (size_t)v * Kp + k;
@@ -548,13 +558,15 @@ __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, i
     v.nk = inter ? K : 1;
     v.lam = p.lambda;
     v.tconst = p.tconst;
-    if (!inter) return relax_slices<CT, TK, S, 1>(p, v, spl, s0, s1, l, k);
+    const int* act = st.act(part);
+    const int na = st.nAct(part);
+    if (!inter) return relax_slices<CT, TK, S, 1>(p, v, spl, act, na, s0, s1, l, k);
     switch (K) {
-        case 1: return relax_slices<CT, TK, S, 1>(p, v, spl, s0, s1, l, k);
-        case 2: return relax_slices<CT, TK, S, 2>(p, v, spl, s0, s1, l, k);
-        case 3: return relax_slices<CT, TK, S, 3>(p, v, spl, s0, s1, l, k);
-        case 4: return relax_slices<CT, TK, S, 4>(p, v, spl, s0, s1, l, k);
-        default: return relax_slices<CT, TK, S, 0>(p, v, spl, s0, s1, l, k);
+        case 1: return relax_slices<CT, TK, S, 1>(p, v, spl, act, na, s0, s1, l, k);
+        case 2: return relax_slices<CT, TK, S, 2>(p, v, spl, act, na, s0, s1, l, k);
+        case 3: return relax_slices<CT, TK, S, 3>(p, v, spl, act, na, s0, s1, l, k);
+        case 4: return relax_slices<CT, TK, S, 4>(p, v, spl, act, na, s0, s1, l, k);
+        default: return relax_slices<CT, TK, S, 0>(p, v, spl, act, na, s0, s1, l, k);
     }
 }
 
@@ -784,18 +796,42 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     const int s0 = __ldg(p.ctaSlice + blockIdx.x), s1 = __ldg(p.ctaSlice + blockIdx.x + 1);
     const bool handoff = t.ncta > 1 && p.flagSync;
     if (handoff && threadIdx.x == 0) p.stepDone[(size_t)t.cta * kStepDoneStride] = 0;
-    // shared memory: [row offsets of both parts][step buffer 0][step buffer 1]
+    // shared memory: [row offsets of both parts][slices with rows, per part]
+    // [step buffer 0][step buffer 1]
     __shared__ unsigned long long stageBar[2];
+    __shared__ int nActive[2];
     Stage st;
     {
         int* spl0 = reinterpret_cast<int*>(smem);
         int* spl1 = spl0 + p.maxCtaSlices + 1;
+        int* act0 = spl1 + p.maxCtaSlices + 1;
+        int* act1 = act0 + p.maxCtaSlices;
         for (int i = threadIdx.x; i <= s1 - s0; i += blockDim.x) {
             spl0[i] = __ldg(p.spInter + s0 + i);
             spl1[i] = __ldg(p.spIntra + s0 + i);
         }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            // stream compaction by warp 0: the slices with rows, in order
+            const int lane = threadIdx.x;
+            for (int part = 0; part < 2; ++part) {
+                const int* spl = part ? spl1 : spl0;
+                int* act = part ? act1 : act0;
+                int base = 0;
+                for (int i0 = 0; i0 < s1 - s0; i0 += 32) {
+                    const int i = i0 + lane;
+                    const bool a = i < s1 - s0 && spl[i + 1] > spl[i];
+                    const unsigned m = __ballot_sync(0xffffffffu, a);
+                    if (a) act[base + __popc(m & ((1u << lane) - 1u))] = i;
+                    base += __popc(m);
+                }
+                if (lane == 0) nActive[part] = base;
+            }
+        }
         st.splInter = spl0;
         st.splIntra = spl1;
+        st.actInter = act0;
+        st.actIntra = act1;
         st.costBytes = sizeof(CT);
         st.timeBytes = TK == 1 ? 4 : TK == 2 ? 8 : 0;
         st.rowCap = p.rowCap;
@@ -813,6 +849,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         __syncthreads();
+        st.nActInter = nActive[0];
+        st.nActIntra = nActive[1];
     }
 
     // set-up (cost_time_ratio_solver.cpp:264-287): DP := inf, branch starts := 0

@@ -809,10 +809,11 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
 }
 
 // Contiguous slice ranges for `blocks` CTAs of `warps` warps with balanced
-// step times.  A warp relaxes the CTA's slices round-robin, and one slice of
-// one step costs it about (gather batches + 1) memory latencies: the batches
-// of its rows and the epilogue (the winner's record, the stores).  A slice
-// without rows skips its step from layer 3 on and costs a loop iteration.
+// step times.  A warp relaxes the CTA's slices that have rows in the step's
+// part, round-robin, and one slice of one step costs it about (gather
+// batches + 1) memory latencies: the batches of its rows and the epilogue
+// (the winner's record, the stores).  Slices without rows are visited only
+// by two steps per sweep and cost nothing here.
 // Steps are coupled across the team by the hand-offs, so a layer costs the
 // slowest warp of any CTA in the interlayer step plus K - 1 times the
 // slowest in an intralayer step (those run only when the layer has
@@ -841,29 +842,41 @@ std::vector<int> Graph::cta_cuts(int blocks, int K, int warps) const {
         w[p].resize((size_t)ns);
         for (int s = 0; s < ns; ++s) {
             const int rows = T.sp[p][(size_t)s + 1] - T.sp[p][(size_t)s];
-            w[p][(size_t)s] = (p == 1 && !intra) ? 0 : rows > 0 ? 32LL * ((rows + rb[p] - 1) / rb[p] + 1) : 1;
+            w[p][(size_t)s] = (p == 1 && !intra) || rows == 0 ? 0 : 32LL * ((rows + rb[p] - 1) / rb[p] + 1);
             lo[p] = std::max(lo[p], w[p][(size_t)s]);
             hi[p] += w[p][(size_t)s];
         }
     }
     std::vector<long long> acc[2] = {std::vector<long long>((size_t)warps), std::vector<long long>((size_t)warps)};
-    // fills CTAs greedily under (bi, bj); returns the CTAs used (cuts in c when given)
+    // fills CTAs greedily under (bi, bj); returns the CTAs used (cuts in c
+    // when given).  A CTA's warps take its slices with rows in a part
+    // round-robin (act[p] counts them); slices without rows cost nothing.
     auto fill = [&](long long bi, long long bj, std::vector<int>* c) -> int {
         int used = 1, start = 0;
+        long long act[2] = {0, 0};
         std::fill(acc[0].begin(), acc[0].end(), 0);
         std::fill(acc[1].begin(), acc[1].end(), 0);
         for (int s = 0; s < ns; ++s) {
-            int i = (s - start) % warps;
-            if (s > start && (acc[0][(size_t)i] + w[0][(size_t)s] > bi || acc[1][(size_t)i] + w[1][(size_t)s] > bj)) {
+            const bool has[2] = {w[0][(size_t)s] > 0, w[1][(size_t)s] > 0};
+            size_t i0 = (size_t)(act[0] % warps), i1 = (size_t)(act[1] % warps);
+            if (s > start && ((has[0] && acc[0][i0] + w[0][(size_t)s] > bi) ||
+                              (has[1] && acc[1][i1] + w[1][(size_t)s] > bj))) {
                 if (c && used < blocks) (*c)[(size_t)used] = s;
                 if (++used > blocks && !c) return used;
                 start = s;
+                act[0] = act[1] = 0;
                 std::fill(acc[0].begin(), acc[0].end(), 0);
                 std::fill(acc[1].begin(), acc[1].end(), 0);
-                i = 0;
+                i0 = i1 = 0;
             }
-            acc[0][(size_t)i] += w[0][(size_t)s];
-            acc[1][(size_t)i] += w[1][(size_t)s];
+            if (has[0]) {
+                acc[0][i0] += w[0][(size_t)s];
+                ++act[0];
+            }
+            if (has[1]) {
+                acc[1][i1] += w[1][(size_t)s];
+                ++act[1];
+            }
         }
         return used;
     };
