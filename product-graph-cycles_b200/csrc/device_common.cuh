@@ -77,7 +77,7 @@ struct BfParams {
     double tconst;
     // state
     double* dv;                    // [2][n][Kp] path value of every (node, depth) of two layers
-    int2* doh;                     // [2][n][Kp] its path's origin (layer-0 start node or kLap* code) and length
+    int2* doh;                     // [2][Kp][n] its path's origin (layer-0 start node or kLap* code) and length
     double* bak;                   // [n]
     int* pred;                     // [(nY+1)*K*n], expanded index layer*n*K + k*n + v
     const int* ctaSlice;           // [ncta+1] slice range of every CTA (both parts)

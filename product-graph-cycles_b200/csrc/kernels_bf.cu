@@ -169,30 +169,31 @@ __device__ __forceinline__ int original_index(int n, int K, int e) {
     return rem - depth * n + layer * n;
 }
 
-// DP record access by record index parity * n * Kp + node * Kp + depth: the
-// value lives in p.dv, the path origin and length in p.doh.  Loads come from
-// shared memory when the whole team is one CTA that keeps its tables there
-// (S), else through L2 (other CTAs write the records during the launch, so
-// L1 must not serve stale lines).
-struct DpRec {
-    double v;
-    int o, h;
-};
+// DP record of node v at depth k in the parity row starting at rowBase =
+// parity * n * Kp.  Its value lives in p.dv at rowBase + v * Kp + k (a
+// node's depths side by side: one vector load gathers them); its path origin
+// and length live in p.doh at rowBase + k * n + v (depth-major: the stores
+// of a warp's 32 consecutive nodes are 256 contiguous bytes, where the
+// node-major index would spread them over 32 sectors; they are read one at
+// a time).  Loads come from shared memory when the whole team is one CTA
+// that keeps its tables there (S), else through L2 (other CTAs write the
+// records during the launch, so L1 must not serve stale lines).
 template <bool S>
 __device__ __forceinline__ double ldV(const BfParams& p, size_t r) {
     if constexpr (S) return p.dv[r];
     else return __ldcg(p.dv + r);
 }
-template <bool S>
-__device__ __forceinline__ DpRec ldE(const BfParams& p, size_t r) {
-    int2 oh;
-    if constexpr (S) oh = p.doh[r];
-    else oh = __ldcg(p.doh + r);
-    return DpRec{ldV<S>(p, r), oh.x, oh.y};
+__device__ __forceinline__ size_t oh_index(const BfParams& p, size_t rowBase, int v, int k) {
+    return rowBase + (size_t)k * p.n + v;
 }
-__device__ __forceinline__ void stE(const BfParams& p, size_t r, double v, int o, int h) {
-    p.dv[r] = v;
-    p.doh[r] = make_int2(o, h);
+template <bool S>
+__device__ __forceinline__ int2 ldOH(const BfParams& p, size_t rowBase, int v, int k) {
+    if constexpr (S) return p.doh[oh_index(p, rowBase, v, k)];
+    else return __ldcg(p.doh + oh_index(p, rowBase, v, k));
+}
+__device__ __forceinline__ void stE(const BfParams& p, size_t rowBase, int v, int k, double val, int o, int h) {
+    p.dv[rowBase + (size_t)v * p.Kp + k] = val;
+    p.doh[oh_index(p, rowBase, v, k)] = make_int2(o, h);
 }
 
 // The NK values of consecutive depths starting at `rec` (a node's row of
@@ -500,9 +501,9 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
                 o = bs;
                 h = 1;
             } else {
-                const DpRec e = ldE<S>(p, sv.sbase + (size_t)bs * Kp + bk);
-                o = e.o;
-                h = e.h + 1;
+                const int2 e = ldOH<S>(p, sv.sbase, bs, bk);
+                o = e.x;
+                h = e.y + 1;
             }
         } else if (l == 0) {
             // Layer 0 keeps an older value and its older predecessor.
@@ -517,13 +518,13 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
                     o = ps;
                     h = 1;
                 } else {
-                    const DpRec e = ldE<S>(p, cur + (size_t)ps * Kp + (k - 1));
-                    o = e.o;
-                    h = e.h + 1;
+                    const int2 e = ldOH<S>(p, cur, ps, k - 1);
+                    o = e.x;
+                    h = e.y + 1;
                 }
             }
         }
-        stE(p, me, best, o, h);
+        stE(p, cur, v, k, best, o, h);
     }
     return any;
 }
@@ -858,7 +859,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     for (long long r = tid; r < 2LL * n * Kp; r += nth) {
         const long long node = (r / Kp) % n;
         const bool start = r < (long long)n * Kp && r % Kp == 0 && p.branchOf[node] == p.branchId;
-        stE(p, (size_t)r, start ? 0.0 : kInfD, kLapUnknown, 0);
+        p.dv[r] = start ? 0.0 : kInfD;
+        p.doh[r] = make_int2(kLapUnknown, 0);  // every (origin, hops) word, in either layout
     }
     for (long long i = tid; i < n; i += nth) {
         p.bak[i] = kInfD;
@@ -988,7 +990,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             for (long long i = tid; i < n; i += nth) {
                 if (p.branchOf[i] != p.branchId) { p.lbOut[i] = kInfD; p.originOut[i] = -1; continue; }
                 const double lb = ldV<S>(p, lastRowBase + (size_t)i * Kp);
-                int o = ldE<S>(p, dRow + (size_t)i * Kp).o;
+                int o = ldOH<S>(p, dRow, (int)i, 0).x;
                 if (o < 0 && !isinf((float)lb)) o = dij_walk_end(p, (int)i);
                 p.lbOut[i] = lb;
                 p.originOut[i] = o;
@@ -1058,9 +1060,9 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     if (pe < 0 || lp != p.nY - 1) {
                         nx = kLapUnknown;
                     } else {
-                        const DpRec w = ldE<S>(p, wRow + (size_t)wv * Kp + kp);
-                        nx = w.o;
-                        st = 1 + w.h;
+                        const int2 w = ldOH<S>(p, wRow, wv, kp);
+                        nx = w.x;
+                        st = 1 + w.y;
                     }
                 }
                 p.lapNext[i] = nx;
