@@ -28,7 +28,7 @@ import numpy as np
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
-           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch"]
+           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -255,6 +255,39 @@ class product_graph_generator:
         keys = ["bf_calls", "sweeps", "candidates", "lawler_iters", "branches", "fallback_walks", "device_us",
                 "kernel_launches"]
         return dict(zip(keys, list(buf)))
+
+
+def load_export(directory: str = ".") -> dict:
+    """Reads back the CSV files that the "export" solver writes
+    (product_graph_generators.cpp:272-282: VX, VY, EX, EY, FeatDiffMatrix and,
+    for a conjugate graph, NX and NY; one row per line, values separated by
+    ", ", doubles with 17 significant digits, so they round-trip exactly).
+
+    Returns {"VX", "VY", "EX", "EY", "feat_diff"} and "NX", "NY" when those
+    files exist.  No counterpart in the reference, which only writes them.
+    """
+    def read(name, dtype):
+        return np.loadtxt(os.path.join(directory, name + ".csv"), delimiter=",", dtype=dtype, ndmin=2)
+
+    out = {"VX": read("VX", np.float64), "VY": read("VY", np.float64), "EX": read("EX", np.int32),
+           "EY": read("EY", np.int32), "feat_diff": read("FeatDiffMatrix", np.float64)}
+    if os.path.exists(os.path.join(directory, "NX.csv")):
+        out["NX"] = read("NX", np.float64)
+        out["NY"] = read("NY", np.float64)
+    return out
+
+
+def from_export(directory: str = ".", conjugate: bool = False, regularising_cost_term: bool = False,
+                prune_intralayer_edges: bool = False) -> "product_graph_generator":
+    """A generator built from an "export" directory (load_export), with its
+    normals set when the files hold them: replays an exported problem.  The
+    flags are not part of the export and are given again."""
+    d = load_export(directory)
+    g = product_graph_generator(d["VX"], d["EX"], d["VY"], d["EY"], d["feat_diff"], conjugate,
+                                regularising_cost_term, prune_intralayer_edges)
+    if "NX" in d:
+        g.set_normals(d["NX"], d["NY"])
+    return g
 
 
 def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas_per_graph: int = 0,
