@@ -117,14 +117,16 @@ int pgc_solve_with_cost_time_ratio(pgc_graph* g, const char* solver_name, int ma
 int pgc_solve_with_minimum_cost(pgc_graph* g, const char* solver_name, int max_depth);
 
 /* No reference counterpart.  Adjoint of the last solve's objective with
- * respect to feat_diff, for the plain product graph: adds (accumulate != 0)
- * or writes grad_objective * d objective / d feat_diff into the DEVICE
- * buffer grad_feat_diff [|VX| x |VY|] f64 of the handle's device.  Ratio:
- * d lambda* / d c_e = 1[e in cycle] / T(cycle) over the rescaled costs;
- * minimum cost: 1[e in cycle].  The rescale factor is held fixed and its
- * rounding passed straight through; the energy's adjoint scatters every
- * cycle edge into the two feat_diff entries its cost reads.  PGC_ERR_STATE
- * without a result, PGC_ERR_MODE for the conjugate graph. */
+ * respect to feat_diff: adds (accumulate != 0) or writes grad_objective *
+ * d objective / d feat_diff into the DEVICE buffer grad_feat_diff
+ * [|VX| x |VY|] f64 of the handle's device.  Ratio: d lambda* / d c_e =
+ * 1[e in cycle] / T(cycle) over the rescaled costs; minimum cost:
+ * 1[e in cycle].  The rescale factor is held fixed and its rounding passed
+ * straight through; the energy's adjoint scatters every cycle edge into the
+ * feat_diff entries its cost reads (plain graph: two; conjugate graph:
+ * fd[x2, y2] in the ("vanilla", *) and ("feature", *) modes, none in the
+ * others).  PGC_ERR_STATE without a result; PGC_ERR_MODE for a ratio on a
+ * conjugate graph whose time column reads feat_diff ("*", "feature"). */
 int pgc_backward_feat_diff(pgc_graph* g, double grad_objective, double* grad_feat_diff, int accumulate);
 
 /* No reference counterpart (the oracle's setCostVector).  Sets the edge costs

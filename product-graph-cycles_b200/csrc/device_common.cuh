@@ -247,6 +247,8 @@ constexpr long long kNoAllocExportValues = 1LL << 21;
 cudaError_t noalloc_export_scratch(int device, double** ptr);
 cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
                                         double coef, double* grad, cudaStream_t s);
+cudaError_t launch_conj_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
+                                       double coef, double* grad, cudaStream_t s);
 cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,
                           long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
                           cudaStream_t s);

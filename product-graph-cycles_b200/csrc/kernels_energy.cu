@@ -220,6 +220,32 @@ __global__ void plain_energy_backward_kernel(EnergyArgs a, const long long* edge
     atomicAdd(grad + (long long)x1 * a.nvy + y1, d);
 }
 
+// Adjoint of ho_energy_kernel's cost column for the edges of a cycle, in the
+// modes where that column reads feat_diff once, linearly with slope 1:
+// ("vanilla", *) has cost = robust loss + fd[x2, y2], ("feature", *) has
+// cost = fd[x2, y2] (higherOrderDeformationEnergy.cpp).  Scatters coef into
+// grad[x2, y2] of every listed product edge; an edge listed twice
+// contributes twice.
+__global__ void conj_energy_backward_kernel(EnergyArgs a, const long long* edges, int count, long long eBlock,
+                                            double coef, double* grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const long long e = edges[i];
+    if (e < 0) return;
+    const int b = (int)(e / eBlock), t = (int)(e - (long long)b * eBlock);
+    if (b >= a.nY) return;
+    const int s2 = a.EY[2 * b], m2 = a.EY[2 * b + 1], t2 = a.EY[2 * ((b + 1) % a.nY) + 1];
+    int y2;
+    switch (a.eY[t]) {
+        case 2: y2 = s2; break;
+        case 3: y2 = m2; break;
+        case 4: y2 = t2; break;
+        default: y2 = m2; break;
+    }
+    const int x2 = a.eX[3 * t + 2];
+    atomicAdd(grad + (long long)x2 * a.nvy + y2, coef);
+}
+
 // Inverse of export_kernel: column c of a [rows x cols] edge-ordered matrix
 // into the per-layer stream (empty slots get NaN).
 __global__ void import_kernel(const double* in, double* col, int cols, int c, long long total, long long layerStride,
@@ -708,6 +734,12 @@ cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* e
                                         double coef, double* grad, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     plain_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, grad);
+    return cudaGetLastError();
+}
+cudaError_t launch_conj_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
+                                       double coef, double* grad, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    conj_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, grad);
     return cudaGetLastError();
 }
 cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,

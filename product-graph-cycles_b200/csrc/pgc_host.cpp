@@ -1661,7 +1661,18 @@ void Graph::cost_vector_noalloc(double* out) {
 // straight through (d c_scaled / d c = product of the factors applied), and
 // the energy's adjoint scatters into feat_diff (plain_energy_backward_kernel).
 void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
-    if (conj) throw Failure(PGC_ERR_MODE, "the feat_diff adjoint covers the plain product graph");
+    int cm = 0, tm = 0;
+    if (conj) {
+        // The conjugate energies read feat_diff once per edge, fd[x2, y2]:
+        // in the cost column with slope 1 for ("vanilla", *) and
+        // ("feature", *), not at all for the other cost modes.  Their time
+        // column reads it only in ("*", "feature") as max(fd) - fd, a
+        // maximum over the whole matrix, which is not differentiated here.
+        cm = string_to_mode(costName);
+        tm = string_to_mode(timeName);
+        if (adjKind == 1 && tm == FEATURE)
+            throw Failure(PGC_ERR_MODE, "the ratio adjoint does not cover a time column that reads feat_diff (\"feature\")");
+    }
     if (adjKind == 0 || !generated) throw Failure(PGC_ERR_STATE, "no ratio or minimum-cost result to differentiate");
     double coef = grad * colScale[0];
     if (adjKind == 1) coef /= adjT;
@@ -1670,7 +1681,11 @@ void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
     a.lengthMode = costName == "feature" && timeName == "lengthnormalisation";
     a.lineIntegral = reg || a.lengthMode;
     wAdjEdges.upload(resEdges.data(), resEdges.size(), stream);
-    PGC_CUDA(launch_plain_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coef, gradFd, stream));
+    if (!conj) {
+        PGC_CUDA(launch_plain_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coef, gradFd, stream));
+    } else if (cm == VANILLA || cm == FEATURE) {
+        PGC_CUDA(launch_conj_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coef, gradFd, stream));
+    }
     stats.launches++;
     PGC_CUDA(sync_stream());
 }

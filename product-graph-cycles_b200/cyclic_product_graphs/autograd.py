@@ -8,8 +8,9 @@ library's hand-written adjoint kernel (``pgc_backward_feat_diff``):
   fixed and its rounding passed straight through;
 * minimum cost: d cost*/d c_e = 1[e in C*];
 
-and the plain energy's adjoint scatters every cycle edge into the two
-feat_diff entries it reads.  torch carries the gradient on from feat_diff
+and the energy's adjoint scatters every cycle edge into the feat_diff
+entries its cost reads (plain graph: two; conjugate graph: one, in the
+("vanilla", *) and ("feature", *) modes).  torch carries the gradient on from feat_diff
 (e.g. to learnable features).  ``BlackboxMinCostCycle`` implements blackbox
 interpolation (Vlastelica et al., ICLR 2020) over the edge costs: its
 backward solves again at w + tau * dL/dy and returns -(y(w) - y(w')) / tau.
@@ -40,8 +41,9 @@ def _adjoint(gen, grad_out: torch.Tensor, like: torch.Tensor, synced: bool = Fal
 
 
 class RatioCycleObjective(torch.autograd.Function):
-    """lambda*(feat_diff) of ``gen`` (a plain product_graph_generator whose
-    geometry and modes are set) by ``solve_with_cost_time_ratio``."""
+    """lambda*(feat_diff) of ``gen`` (a product_graph_generator whose geometry
+    and modes are set: plain, or conjugate with a time mode other than
+    "feature") by ``solve_with_cost_time_ratio``."""
 
     @staticmethod
     def forward(ctx, feat_diff, gen, max_depth=None):

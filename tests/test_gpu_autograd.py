@@ -9,6 +9,9 @@
   gives the single-pair results and gradients.
 * Blackbox interpolation reproduces its definition -(y(w) - y(w + tau g)) / tau,
   with both solves recomputed independently by the oracle.
+* Conjugate graph: the adjoint scatters into fd[x2, y2] of every cycle edge
+  (ratio: the rescale factor over T; minimum cost: 1), and a ratio whose time
+  column reads feat_diff ("feature") is refused.
 """
 import numpy as np
 import pytest
@@ -160,3 +163,56 @@ def test_blackbox_interpolation_reproduces_its_definition(cpg, oracle):
     assert np.array_equal(y.detach().cpu().numpy(), y_w)
     y_w2 = oracle_y(w0 + tau * gy.cpu().numpy())
     np.testing.assert_array_equal(w.grad.cpu().numpy(), -(y_w - y_w2) / tau)
+
+
+def _conj_gens(cpg, oracle, p, reg, cost, time):
+    args = (p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], True, reg, False)
+    g, o = cpg.product_graph_generator(*args), oracle.OracleGenerator(*args)
+    for x in (g, o):
+        x.set_normals(p["NX"], p["NY"])
+        x.set_cost_time_ratio_mode(cost, time)
+    # the SO(3) energies agree to 1e-9, not bitwise: both sides use the device's
+    o.set_cost_vector(g.get_cost_vector())
+    return g, o
+
+
+@pytest.mark.parametrize("reg,cost,time", [(False, "vanilla", "lengthnormalisation"), (False, "vanilla", "vanilla"),
+                                           (True, "feature", "plainso3")])
+def test_conjugate_ratio_adjoint_matches_gradient_from_oracle_cycle(cpg, oracle, reg, cost, time):
+    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=13)
+    g, o = _conj_gens(cpg, oracle, p, reg, cost, time)
+    raw = o.get_cost_vector()
+    K = 2
+    rg = g.solve_with_cost_time_ratio("lawlergpu", K)
+    ro = o.solve_with_cost_time_ratio("lawlercpu", K)
+    assert rg[1] == ro[1] and np.array_equal(rg[2], ro[2])
+    edges = o.last_cycle_edges()
+    assert np.array_equal(np.sort(g.last_cycle_edges()), np.sort(edges))
+    s0 = 1e5 / (2 * max(np.median(raw[:, 0]), 0.001))
+    scaled = o.get_cost_vector()
+    T = scaled[edges, 1].sum() if raw.shape[1] > 1 else 5e4 * len(edges)
+    ps = o.get_product_space()
+    want = np.zeros(p["feat_diff"].shape)
+    for e in edges:  # cost = (robust loss +) fd[x2, y2]
+        y2, x2 = ps[e][2], ps[e][5]
+        want[x2, y2] += s0 / T
+    got = _device_grad(g, want.shape)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-18)
+
+
+def test_conjugate_min_cost_adjoint_and_unsupported_time_mode(cpg, oracle):
+    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=13)
+    g, o = _conj_gens(cpg, oracle, p, False, "vanilla", "lengthnormalisation")
+    rg = g.solve_with_minimum_cost("dijkstragpu", 2)
+    ro = o.solve_with_minimum_cost("dijkstracpu", 2)
+    assert rg[1] == ro[1] and np.array_equal(rg[2], ro[2])
+    ps = o.get_product_space()
+    want = np.zeros(p["feat_diff"].shape)
+    for e in o.last_cycle_edges():
+        want[ps[e][5], ps[e][2]] += 1.0
+    np.testing.assert_allclose(_device_grad(g, want.shape, 3.0), 3.0 * want, rtol=1e-12, atol=1e-18)
+    # a time column that reads feat_diff through its maximum is not differentiated
+    g2, _ = _conj_gens(cpg, oracle, p, True, "robustso3", "feature")
+    g2.solve_with_cost_time_ratio("lawlergpu", 2)
+    with pytest.raises(cpg.PGCError, match="feature"):
+        _device_grad(g2, p["feat_diff"].shape)
