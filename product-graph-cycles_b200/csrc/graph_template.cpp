@@ -336,6 +336,10 @@ void build_sell(LayerTemplate& T) {
 
 }  // namespace
 
+void host_parallel_for(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)>& f) {
+    parallel_for(n, [&](int64_t a, int64_t b) { f(a, b); }, grain);
+}
+
 std::string build_template(const int* EX, int64_t nEX, const int* EY, int64_t nEY, int64_t nVX, bool conj,
                            bool prune, LayerTemplate& T) {
     if (nEX < 1) return "EX must have at least one row";

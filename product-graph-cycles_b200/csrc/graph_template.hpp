@@ -18,6 +18,7 @@
 // holds an edge of block l.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <string>
 #include <utility>
@@ -89,6 +90,10 @@ struct LayerTemplate {
 // Builds the template; returns an empty string or an error message.
 std::string build_template(const int* EX, int64_t nEX, const int* EY, int64_t nEY, int64_t nVX, bool conj,
                            bool prune, LayerTemplate& T);
+
+// Runs f(begin, end) over parts of [0, n) of at least `grain` items on the
+// process's host worker pool (inline when another job holds the pool).
+void host_parallel_for(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)>& f);
 
 // productspace row of global edge id e (product_space.cpp / conj_product_space.cpp order).
 void product_row(const LayerTemplate& T, const int* EY, int64_t e, int* out);

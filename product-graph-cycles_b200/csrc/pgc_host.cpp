@@ -850,32 +850,33 @@ std::vector<int> Graph::cta_cuts(int blocks, int K, int warps) const {
     std::vector<long long> acc[2] = {std::vector<long long>((size_t)warps), std::vector<long long>((size_t)warps)};
     // fills CTAs greedily under (bi, bj); returns the CTAs used (cuts in c
     // when given).  A CTA's warps take its slices with rows in a part
-    // round-robin (act[p] counts them); slices without rows cost nothing.
+    // round-robin (a0, a1: the warp that gets the next one); slices without
+    // rows cost nothing.
     auto fill = [&](long long bi, long long bj, std::vector<int>* c) -> int {
-        int used = 1, start = 0;
-        long long act[2] = {0, 0};
-        std::fill(acc[0].begin(), acc[0].end(), 0);
-        std::fill(acc[1].begin(), acc[1].end(), 0);
+        int used = 1, start = 0, a0 = 0, a1 = 0;
+        long long* acc0 = acc[0].data();
+        long long* acc1 = acc[1].data();
+        std::fill(acc0, acc0 + warps, 0);
+        std::fill(acc1, acc1 + warps, 0);
+        const long long* w0 = w[0].data();
+        const long long* w1 = w[1].data();
         for (int s = 0; s < ns; ++s) {
-            const bool has[2] = {w[0][(size_t)s] > 0, w[1][(size_t)s] > 0};
-            size_t i0 = (size_t)(act[0] % warps), i1 = (size_t)(act[1] % warps);
-            if (s > start && ((has[0] && acc[0][i0] + w[0][(size_t)s] > bi) ||
-                              (has[1] && acc[1][i1] + w[1][(size_t)s] > bj))) {
+            const long long x0 = w0[s], x1 = w1[s];
+            if (s > start && ((x0 && acc0[a0] + x0 > bi) || (x1 && acc1[a1] + x1 > bj))) {
                 if (c && used < blocks) (*c)[(size_t)used] = s;
                 if (++used > blocks && !c) return used;
                 start = s;
-                act[0] = act[1] = 0;
-                std::fill(acc[0].begin(), acc[0].end(), 0);
-                std::fill(acc[1].begin(), acc[1].end(), 0);
-                i0 = i1 = 0;
+                a0 = a1 = 0;
+                std::fill(acc0, acc0 + warps, 0);
+                std::fill(acc1, acc1 + warps, 0);
             }
-            if (has[0]) {
-                acc[0][i0] += w[0][(size_t)s];
-                ++act[0];
+            if (x0) {
+                acc0[a0] += x0;
+                if (++a0 == warps) a0 = 0;
             }
-            if (has[1]) {
-                acc[1][i1] += w[1][(size_t)s];
-                ++act[1];
+            if (x1) {
+                acc1[a1] += x1;
+                if (++a1 == warps) a1 = 0;
             }
         }
         return used;
@@ -927,21 +928,31 @@ void Graph::upload_cta_slices(const std::vector<int>& cut, int K, int warps) {
     std::vector<int> owner((size_t)T.nslices);
     for (int c = 0; c < blocks; ++c)
         for (int s = cut[(size_t)c]; s < cut[(size_t)c + 1]; ++s) owner[(size_t)s] = c;
+    // the CTA pairs joined by an in-edge, in parallel over slices (each part
+    // of the range marks its own matrix; the matrices are OR-ed)
     std::vector<unsigned char> adj((size_t)blocks * blocks, 0);
-    for (int p = 0; p < 2; ++p) {
-        for (int s = 0; s < T.nslices; ++s) {
-            const int ct = owner[(size_t)s];
-            for (int j = T.sp[p][(size_t)s]; j < T.sp[p][(size_t)s + 1]; ++j)
-                for (int lane = 0; lane < 32; ++lane) {
-                    const int sv = T.src[p][(size_t)j * 32 + lane];
-                    if (sv < 0) continue;
-                    const int cs = owner[(size_t)(sv >> 5)];
-                    if (cs == ct) continue;
-                    adj[(size_t)ct * blocks + cs] = 1;
-                    adj[(size_t)cs * blocks + ct] = 1;
-                }
+    std::mutex adjMu;
+    host_parallel_for(T.nslices, 256, [&](int64_t s0, int64_t s1) {
+        std::vector<unsigned char> mine((size_t)blocks * blocks, 0);
+        for (int p = 0; p < 2; ++p) {
+            for (int64_t s = s0; s < s1; ++s) {
+                const int ct = owner[(size_t)s];
+                int last = ct;
+                for (int j = T.sp[p][(size_t)s]; j < T.sp[p][(size_t)s + 1]; ++j)
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int sv = T.src[p][(size_t)j * 32 + lane];
+                        if (sv < 0) continue;
+                        const int cs = owner[(size_t)(sv >> 5)];
+                        if (cs == ct || cs == last) continue;
+                        last = cs;
+                        mine[(size_t)ct * blocks + cs] = 1;
+                        mine[(size_t)cs * blocks + ct] = 1;
+                    }
+            }
         }
-    }
+        std::lock_guard<std::mutex> lock(adjMu);
+        for (size_t i = 0; i < adj.size(); ++i) adj[i] |= mine[i];
+    });
     std::vector<int> ptr((size_t)blocks + 1, 0), idx;
     for (int c = 0; c < blocks; ++c) {
         for (int d = 0; d < blocks; ++d)
