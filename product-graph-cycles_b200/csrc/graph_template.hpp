@@ -20,15 +20,23 @@
 #include <cstdint>
 #include <functional>
 #include <memory>
+#include <new>
 #include <string>
 #include <utility>
 #include <vector>
 
 namespace pgc {
 
-// Allocator whose resize leaves elements default-initialised (unset for
-// ints): the template builder writes every element it sizes, and zeroing
-// tens of MB first was a visible part of building a large template.
+// Host memory for buffers that are copied to the device (pinned where
+// possible, from a process-wide cache; defined with the CUDA host code).
+void* host_buffer_alloc(size_t bytes);
+void host_buffer_free(void* p);
+
+// Allocator of the template arrays and of a handle's inputs: memory from
+// host_buffer_alloc, so their uploads are plain DMA, and a resize that leaves
+// elements default-initialised (unset for ints): the template builder writes
+// every element it sizes, and zeroing tens of MB first was a visible part of
+// building a large template.
 template <class T>
 struct RawAlloc : std::allocator<T> {
     template <class U>
@@ -38,6 +46,12 @@ struct RawAlloc : std::allocator<T> {
     RawAlloc() = default;
     template <class U>
     RawAlloc(const RawAlloc<U>&) noexcept {}
+    T* allocate(size_t n) {
+        void* p = host_buffer_alloc(n * sizeof(T));
+        if (!p && n) throw std::bad_alloc();
+        return static_cast<T*>(p);
+    }
+    void deallocate(T* p, size_t) noexcept { host_buffer_free(p); }
     template <class U>
     void construct(U* p) noexcept {
         ::new ((void*)p) U;

@@ -57,6 +57,63 @@ struct Failure : std::runtime_error {
 // similar size) does not pay cudaMalloc/cudaFree every time.  Every handle
 // synchronises its stream before it returns memory here, so a cached block is
 // never still in use.  pgc_release_cached_memory() returns the cache to CUDA.
+// Pinned host memory for what a handle uploads (its inputs and the layer
+// template): copies from it are DMA the host does not stage.  cudaHostAlloc
+// is slow, so freed blocks are kept by size and handed out again to requests
+// of at least half their size, for the process's lifetime; a handle's
+// buffers come back only after its stream has been synchronised.  Pageable
+// memory stands in when pinning fails.
+class HostPool {
+  public:
+    static HostPool& get() {
+        static HostPool* pool = new HostPool();  // never destroyed: outlives all handles
+        return *pool;
+    }
+    void* allocate(size_t bytes) {
+        if (bytes == 0) return nullptr;
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            auto it = free_.lower_bound(bytes);
+            if (it != free_.end() && it->first <= 2 * bytes + (1 << 20)) {
+                void* p = it->second;
+                sizes_[p] = it->first;
+                free_.erase(it);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+            (void)cudaGetLastError();
+            p = std::malloc(bytes);
+            if (!p) return nullptr;
+            std::lock_guard<std::mutex> lock(mu_);
+            pageable_.insert(p);
+            return p;
+        }
+        std::lock_guard<std::mutex> lock(mu_);
+        sizes_[p] = bytes;
+        return p;
+    }
+    void deallocate(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lock(mu_);
+        if (pageable_.erase(p)) {
+            std::free(p);
+            return;
+        }
+        auto it = sizes_.find(p);
+        if (it == sizes_.end()) return;
+        free_.emplace(it->second, p);
+        sizes_.erase(it);
+    }
+
+  private:
+    std::mutex mu_;
+    std::multimap<size_t, void*> free_;
+    std::map<void*, size_t> sizes_;
+    std::set<void*> pageable_;
+};
+
 class DevicePool {
   public:
     static DevicePool& get() {
@@ -191,6 +248,10 @@ int env_int(const char* name, int dflt) {
 
 }  // namespace
 
+// The template's and the inputs' allocator (graph_template.hpp).
+void* host_buffer_alloc(size_t bytes) { return HostPool::get().allocate(bytes); }
+void host_buffer_free(void* p) { HostPool::get().deallocate(p); }
+
 // A closed walk of the product graph as the reference stores it: original
 // node ids (targets in layer 0 that close a lap are written as the closing
 // copy numNodes + v only at the end), plus the edge and its cost/time for
@@ -218,8 +279,8 @@ struct Stats {
 class Graph {
   public:
     // inputs
-    std::vector<double> VX, VY, FD, NX, NY;
-    std::vector<int> EX, EY;
+    RawVec<double> VX, VY, FD, NX, NY;
+    RawVec<int> EX, EY;
     int64_t nvx = 0, nvy = 0, nex = 0, ney = 0;
     bool conj = false, reg = false, prune = false, normalsGiven = false;
     double rlAlpha = 0.7, rlC = 0.6, rlPwr = 4;
@@ -1745,7 +1806,7 @@ void Graph::product_space(int32_t* out) {
 // utils::writeMatrixToFile (utils.hpp:24-32): full precision, ", " between
 // columns, a newline between rows and none after the last row.
 void Graph::export_csv() {
-    auto writeD = [](const std::vector<double>& m, int64_t rows, int64_t cols, const std::string& name) {
+    auto writeD = [](const RawVec<double>& m, int64_t rows, int64_t cols, const std::string& name) {
         std::ofstream f(name + ".csv");
         if (!f.is_open()) return;
         f.precision(17);
@@ -1757,7 +1818,7 @@ void Graph::export_csv() {
             if (i + 1 < rows) f << "\n";
         }
     };
-    auto writeI = [](const std::vector<int>& m, int64_t rows, int64_t cols, const std::string& name) {
+    auto writeI = [](const RawVec<int>& m, int64_t rows, int64_t cols, const std::string& name) {
         std::ofstream f(name + ".csv");
         if (!f.is_open()) return;
         for (int64_t i = 0; i < rows; ++i) {
