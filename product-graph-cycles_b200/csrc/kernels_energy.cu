@@ -665,8 +665,15 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
-    select_hist_kernel<<<stream_grid(select_hist_kernel, 512, (1 << a.bits) * sizeof(unsigned)), 512,
-                         (1 << a.bits) * sizeof(unsigned), s>>>(a);
+    const size_t smem = (size_t)(1 << a.bits) * sizeof(unsigned);
+    if (smem > 48 * 1024) {
+        // digits wider than 13 bits need the opt-in shared memory; every
+        // caller sets the same value, so concurrent solves do not race
+        const cudaError_t e = cudaFuncSetAttribute(select_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)(sizeof(unsigned) << 14));
+        if (e != cudaSuccess) return e;
+    }
+    select_hist_kernel<<<stream_grid(select_hist_kernel, 512, smem), 512, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,

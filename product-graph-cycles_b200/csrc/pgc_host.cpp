@@ -620,13 +620,16 @@ double Graph::median_of_column(int col) {
     // holding rank k has at most kCompact members it is copied out and
     // finished on the host.  If rank k is the largest of its bucket, rank k+1
     // is the smallest key above the bucket (one reduction pass).
-    const int bits = kTopDigitBits;
+    // digit widths: the first (counted by the energy kernel), a wider second
+    // one (a 64 KB shared histogram: on the default pair it leaves a bucket
+    // small enough to copy out, where 12 bits needed a third pass), then 12
+    const int bits = kTopDigitBits, bits2 = 14, bitsMax = 14;
     const long long kCompact = 1 << 16;
     DBuf<unsigned long long> hist, cnt;
     DBuf<double> band;
-    hist.alloc((size_t)1 << bits);
+    hist.alloc((size_t)1 << bitsMax);
     cnt.alloc(1);
-    std::vector<unsigned long long> h((size_t)1 << bits);
+    std::vector<unsigned long long> h((size_t)1 << bitsMax);
     SelectArgs a{};
     a.col = e64[col].p;
     a.total = total;
@@ -648,7 +651,7 @@ double Graph::median_of_column(int col) {
     int shift = 64;
     long long rank = k, bucket = count;
     while (shift > 0 && bucket > kCompact) {
-        const int b = std::min(bits, shift);
+        const int b = std::min(mask == 0 ? bits : shift == 64 - bits ? bits2 : bits, shift);
         shift -= b;
         a.prefix = prefix;
         a.prefixMask = mask;
