@@ -184,6 +184,8 @@ struct LookupArgs {
     long long interEntries, layerStride;
     const double* c64;
     const double* t64;   // nullptr: constant time
+    const float* c32;    // when set: the exact float copies of the rescaled columns, read instead
+    const float* t32;
     double tconst;
     const int* pairSrc;
     const int* pairTrgt;
@@ -233,7 +235,9 @@ cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long abov
                                     cudaStream_t s);
 cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
                            int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
-                           cudaStream_t s);
+                           int writeF64, cudaStream_t s);
+cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
+                          const int* ti, const int* tr, cudaStream_t s);
 cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,
                           long long interEntries, int nY, const int* ti, const int* tr, int* exact, cudaStream_t s);
 cudaError_t launch_export(const double* col, double* out, int cols, int c, long long total, long long layerStride,
@@ -253,6 +257,9 @@ cudaError_t launch_import(const double* in, double* col, int cols, int c, long l
                           long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
                           cudaStream_t s);
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
+                               const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
+                               int* countOut, cudaStream_t s);
+cudaError_t launch_layer1_mean(const float* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s);
 

@@ -1284,8 +1284,8 @@ __global__ void lookup_pairs_kernel(LookupArgs a) {
         if (src[e] == s) {
             const long long off = (long long)lt * a.layerStride + (part ? a.interEntries : 0) + e;
             a.edgeOut[i] = block * a.eBlock + ted[e];
-            a.cOut[i] = a.c64[off];
-            a.tOut[i] = a.t64 ? a.t64[off] : a.tconst;
+            a.cOut[i] = a.c32 ? (double)a.c32[off] : a.c64[off];
+            a.tOut[i] = a.t32 ? (double)a.t32[off] : a.t64 ? a.t64[off] : a.tconst;
             return;
         }
     }

@@ -539,11 +539,13 @@ __global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, 
     if ((threadIdx.x & 31) == 0 && best != ~0ull) atomicMin(out, best);
 }
 
-// x <- min(round(factor * x), clip), in place on the valid entries; also
-// writes the float copy and clears *exact when a value is not a float.
+// x <- min(round(factor * x), clip) on the valid entries: the float copy
+// always, the double column in place only when writeF64 (the host first
+// runs without it and keeps the float copy as the rescaled column when every
+// value is exact); clears *exact when a value is not a float.
 __global__ void rescale_kernel(double* col, float* col32, long long total, long long layerStride,
                                long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
-                               double factor, double clip, int* exact) {
+                               double factor, double clip, int* exact, int writeF64) {
     (void)total;
     for_stream_values<4>(col, layerStride, interEntries, nY, tedgeInter, tedgeIntra,
                          [&](long long idx, double v, bool valid, bool inRange) {
@@ -554,12 +556,21 @@ __global__ void rescale_kernel(double* col, float* col32, long long total, long 
                            }
                            double x = round(factor * v);
                            if (x > clip) x = clip;
-                           col[idx] = x;
+                           if (writeF64) col[idx] = x;
                            const float f = (float)x;
                            if (col32) col32[idx] = f;
                            if ((double)f != x) *exact = 0;
                        });
 }
+// The double column from its exact float copy, on the valid entries.
+__global__ void to_f64_kernel(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
+                              const int* tedgeInter, const int* tedgeIntra) {
+    for_stream_layers(layerStride, interEntries, nY, tedgeInter, tedgeIntra,
+                      [&](long long idx, int, long long, int t, bool inRange) {
+                          if (inRange && t >= 0) col[idx] = (double)col32[idx];
+                      });
+}
+
 __global__ void to_f32_kernel(const double* col, float* col32, long long total, long long layerStride,
                               long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
                               int* exact) {
@@ -602,25 +613,27 @@ __global__ void export_kernel(const double* col, double* out, int cols, int c, l
 
 // Mean incoming cost of every node of layer 1, accumulated in float in
 // in-edge order (cost_time_ratio_solver.cpp:656-675).
-__global__ void layer1_mean_kernel(const double* cost, long long layerStride, long long interEntries, int n,
+// CT: the fp64 column or its exact fp32 copy (the same values).
+template <class CT>
+__global__ void layer1_mean_kernel(const CT* cost, long long layerStride, long long interEntries, int n,
                                    int nslices, const int* spInter, const int* spIntra, const int* srcInter,
                                    const int* srcIntra, float* meanOut, int* countOut) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     const int s = v >> 5, lane = v & 31;
-    const double* c1 = cost + layerStride;  // layer 1
+    const CT* c1 = cost + layerStride;  // layer 1
     float mean = 0;
     int num = 0;
     for (int j = spInter[s]; j < spInter[s + 1]; ++j) {
         const long long e = (long long)j * 32 + lane;
         if (srcInter[e] < 0) continue;
-        mean = (float)((double)mean + c1[e]);
+        mean = (float)((double)mean + (double)c1[e]);
         ++num;
     }
     for (int j = spIntra[s]; j < spIntra[s + 1]; ++j) {
         const long long e = (long long)j * 32 + lane;
         if (srcIntra[e] < 0) continue;
-        mean = (float)((double)mean + c1[interEntries + e]);
+        mean = (float)((double)mean + (double)c1[interEntries + e]);
         ++num;
     }
     meanOut[v] = mean / (float)num;
@@ -688,9 +701,14 @@ cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long abov
 }
 cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
                            int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
-                           cudaStream_t s) {
+                           int writeF64, cudaStream_t s) {
     rescale_kernel<<<stream_grid(rescale_kernel, 256, 0), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
-                                                        factor, clip, exact);
+                                                        factor, clip, exact, writeF64);
+    return cudaGetLastError();
+}
+cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
+                          const int* ti, const int* tr, cudaStream_t s) {
+    to_f64_kernel<<<stream_grid(to_f64_kernel, 256, 0), 256, 0, s>>>(col32, col, layerStride, interEntries, nY, ti, tr);
     return cudaGetLastError();
 }
 cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,
@@ -759,8 +777,15 @@ cudaError_t launch_import(const double* in, double* col, int cols, int c, long l
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s) {
-    layer1_mean_kernel<<<(n + 255) / 256, 256, 0, s>>>(cost, layerStride, interEntries, n, nslices, spI, spA, srcI,
-                                                       srcA, meanOut, countOut);
+    layer1_mean_kernel<double><<<(n + 255) / 256, 256, 0, s>>>(cost, layerStride, interEntries, n, nslices, spI, spA,
+                                                               srcI, srcA, meanOut, countOut);
+    return cudaGetLastError();
+}
+cudaError_t launch_layer1_mean(const float* cost, long long layerStride, long long interEntries, int n, int nslices,
+                               const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
+                               int* countOut, cudaStream_t s) {
+    layer1_mean_kernel<float><<<(n + 255) / 256, 256, 0, s>>>(cost, layerStride, interEntries, n, nslices, spI, spA,
+                                                              srcI, srcA, meanOut, countOut);
     return cudaGetLastError();
 }
 

@@ -377,7 +377,13 @@ class Graph {
     void energy_changed() {
         f32Known[0] = f32Known[1] = false;
         topHistValid[0] = topHistValid[1] = false;
+        e64Stale[0] = e64Stale[1] = false;
     }
+    // After a rescale whose values are all exact floats, the float copy is
+    // the rescaled column and the double column still holds the values
+    // before the rescale: it is rewritten only for a reader that needs it.
+    bool e64Stale[2] = {false, false};
+    void ensure_e64(int col);
     // First median pass of each column, counted by the energy kernel that
     // wrote it; valid until the column changes.
     DBuf<unsigned long long> topHist[2];
@@ -631,6 +637,7 @@ double Graph::median_of_column(int col) {
     cnt.alloc(1);
     std::vector<unsigned long long> h((size_t)1 << bitsMax);
     SelectArgs a{};
+    ensure_e64(col);
     a.col = e64[col].p;
     a.total = total;
     a.layerStride = stride;
@@ -725,20 +732,38 @@ void Graph::rescale_column(int col, double scaling) {
     wCount.alloc(1);
     const int one = 1;
     PGC_CUDA(cudaMemcpyAsync(wCount.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    // the float copy first; the double column only when a value is not exact
     PGC_CUDA(launch_rescale(e64[col].p, e32[col].p, total, stride, T.entries[INTER], T.nY, dTedge[INTER].p,
-                            dTedge[INTRA].p, factor, 100 * scaling, wCount.p, stream));
+                            dTedge[INTRA].p, factor, 100 * scaling, wCount.p, 0, stream));
     stats.launches++;
     int exact = 0;
     d2h(&exact, wCount.p, sizeof(int));
     PGC_CUDA(sync_stream());
+    if (exact) {
+        e64Stale[col] = true;
+    } else {
+        PGC_CUDA(launch_rescale(e64[col].p, e32[col].p, total, stride, T.entries[INTER], T.nY, dTedge[INTER].p,
+                                dTedge[INTRA].p, factor, 100 * scaling, wCount.p, 1, stream));
+        stats.launches++;
+        PGC_CUDA(sync_stream());
+    }
     f32Valid[col] = exact != 0;
     f32Known[col] = true;
     topHistValid[col] = false;
     colScale[col] *= factor;
 }
 
+void Graph::ensure_e64(int col) {
+    if (!e64Stale[col]) return;
+    PGC_CUDA(launch_to_f64(e32[col].p, e64[col].p, T.layerStride(), T.entries[INTER], T.nY, dTedge[INTER].p,
+                           dTedge[INTRA].p, stream));
+    stats.launches++;
+    e64Stale[col] = false;
+}
+
 void Graph::ensure_f32(int col) {
     if (f32Known[col]) return;
+    ensure_e64(col);
     const long long stride = T.layerStride();
     const long long total = (long long)(T.nY + 1) * stride;
     e32[col].alloc((size_t)total);
@@ -768,10 +793,12 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     while (r.Kp < K) r.Kp <<= 1;
     ensure_f32(0);
     r.costF32 = f32Valid[0] ? 1 : 0;
+    if (!r.costF32) ensure_e64(0);
     r.cost = r.costF32 ? (const void*)e32[0].p : (const void*)e64[0].p;
     if (ratio && ncols > 1) {
         ensure_f32(1);
         r.timeKind = f32Valid[1] ? 1 : 2;
+        if (!f32Valid[1]) ensure_e64(1);
         r.time = f32Valid[1] ? (const void*)e32[1].p : (const void*)e64[1].p;
         r.tconst = 0;
     } else {
@@ -1219,6 +1246,8 @@ void Graph::lookup_pairs(const std::vector<int>& src, const std::vector<int>& tr
     a.layerStride = T.layerStride();
     a.c64 = e64[0].p;
     a.t64 = ncols > 1 ? e64[1].p : nullptr;
+    a.c32 = e64Stale[0] ? e32[0].p : nullptr;
+    a.t32 = ncols > 1 && e64Stale[1] ? e32[1].p : nullptr;
     a.tconst = tconst;
     a.pairSrc = wPairS.p;
     a.pairTrgt = wPairT.p;
@@ -1310,8 +1339,12 @@ void Graph::solve_ratio(int K) {
     {
         std::vector<float> mean((size_t)n);
         std::vector<int> cnt((size_t)n);
-        PGC_CUDA(launch_layer1_mean(e64[0].p, T.layerStride(), T.entries[INTER], n, T.nslices, dSp[INTER].p,
-                                    dSp[INTRA].p, dSrc[INTER].p, dSrc[INTRA].p, wMean.p, wCandStat.p, stream));
+        if (e64Stale[0])
+            PGC_CUDA(launch_layer1_mean(e32[0].p, T.layerStride(), T.entries[INTER], n, T.nslices, dSp[INTER].p,
+                                        dSp[INTRA].p, dSrc[INTER].p, dSrc[INTRA].p, wMean.p, wCandStat.p, stream));
+        else
+            PGC_CUDA(launch_layer1_mean(e64[0].p, T.layerStride(), T.entries[INTER], n, T.nslices, dSp[INTER].p,
+                                        dSp[INTRA].p, dSrc[INTER].p, dSrc[INTRA].p, wMean.p, wCandStat.p, stream));
         stats.launches++;
         d2h(mean.data(), wMean.p, sizeof(float) * n);
         d2h(cnt.data(), wCandStat.p, sizeof(int) * n);
@@ -1688,6 +1721,7 @@ void Graph::cost_vector(double* out) {
     const long long total = (long long)(T.nY + 1) * stride;
     DBuf<double> tmp;
     tmp.alloc((size_t)(rows * ncols));
+    for (int c = 0; c < ncols; ++c) ensure_e64(c);
     for (int c = 0; c < ncols; ++c)
         PGC_CUDA(launch_export(e64[c].p, tmp.p, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
                                dTedge[INTER].p, dTedge[INTRA].p, stream));
@@ -1722,6 +1756,7 @@ void Graph::cost_vector_noalloc(double* out) {
     double* scratch = noalloc_scratch_for(device);
     const long long stride = T.layerStride();
     const long long total = (long long)(T.nY + 1) * stride;
+    for (int c = 0; c < ncols; ++c) ensure_e64(c);
     for (int c = 0; c < ncols; ++c)
         PGC_CUDA(launch_export(e64[c].p, scratch, ncols, c, total, stride, T.entries[INTER], T.nY, T.eBlock,
                                dTedge[INTER].p, dTedge[INTRA].p, stream));
