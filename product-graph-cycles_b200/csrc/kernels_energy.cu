@@ -307,30 +307,39 @@ __device__ double4 frame_quaternion(const double v2[3], const double n2[3], cons
                       {Szx - Sxz, Sxy + Syx, -Sxx + Syy - Szz, Syz + Szy},
                       {Sxy - Syx, Szx + Sxz, Syz + Szy, -Sxx - Syy + Szz}};
     double V[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+    // every loop below is unrolled, so A and V stay in registers (a run-time
+    // index would place them in local memory)
     for (int sweep = 0; sweep < 50; ++sweep) {
         double off = 0.0, diag = 0.0;
+#pragma unroll
         for (int i = 0; i < 4; ++i) {
             diag += A[i][i] * A[i][i];
+#pragma unroll
             for (int j = i + 1; j < 4; ++j) off += A[i][j] * A[i][j];
         }
         if (off <= 1e-32 * (diag + 1e-300)) break;
+#pragma unroll
         for (int pp = 0; pp < 3; ++pp)
+#pragma unroll
             for (int q = pp + 1; q < 4; ++q) {
                 const double apq = A[pp][q];
                 if (fabs(apq) < 1e-300) continue;
                 const double theta = (A[q][q] - A[pp][pp]) / (2.0 * apq);
                 const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
                 const double c = 1.0 / sqrt(tt * tt + 1.0), s = tt * c;
+#pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const double akp = A[k][pp], akq = A[k][q];
                     A[k][pp] = c * akp - s * akq;
                     A[k][q] = s * akp + c * akq;
                 }
+#pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const double apk = A[pp][k], aqk = A[q][k];
                     A[pp][k] = c * apk - s * aqk;
                     A[q][k] = s * apk + c * aqk;
                 }
+#pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const double vkp = V[k][pp], vkq = V[k][q];
                     V[k][pp] = c * vkp - s * vkq;
@@ -338,10 +347,16 @@ __device__ double4 frame_quaternion(const double v2[3], const double n2[3], cons
                 }
             }
     }
-    int best = 0;
-    for (int i = 1; i < 4; ++i)
-        if (A[i][i] > A[best][best]) best = i;
-    double q[4] = {V[0][best], V[1][best], V[2][best], V[3][best]};
+    // the column of the largest eigenvalue (first index among equals)
+    double q[4] = {V[0][0], V[1][0], V[2][0], V[3][0]};
+    double bestVal = A[0][0];
+#pragma unroll
+    for (int i = 1; i < 4; ++i) {
+        const bool take = A[i][i] > bestVal;
+        bestVal = take ? A[i][i] : bestVal;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) q[k] = take ? V[k][i] : q[k];
+    }
     const double nq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
     return make_double4(q[0] / nq, q[1] / nq, q[2] / nq, q[3] / nq);
 }
