@@ -412,6 +412,14 @@ __device__ __forceinline__ long long quat_index(const EnergyArgs& a, int i, int 
     return (long long)i2 * a.quatEX + e3;
 }
 
+// Work item: one block of template positions x a chunk of layers.  A thread
+// keeps its position -- template edge, Y pattern, X columns, frame indices,
+// the X half of the line integral -- and walks the chunk's layers, so per
+// layer it reads only the layer's Y edge and the fd entry; the stores of a
+// warp stay 32 consecutive entries of one layer.  Every value is computed
+// with the same operations in the same order as per entry.
+constexpr int kHoLayerChunk = 16;
+
 __global__ void ho_energy_kernel(EnergyArgs a) {
     extern __shared__ unsigned int topSh[];  // [2][kTopBins] when a.hist0
     DigitRun r0, r1;
@@ -422,69 +430,113 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
     // Without quaternions every SO(3) distance is 0: its robust loss is the
     // same number for every edge, computed once per thread by the same code.
     const double rl0 = robust_loss(a, 0.0);
-    for_stream_layers(a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
-                      [&](long long idx, int l, long long pos, int t, bool inRange) {
-        if (!inRange) return;
+    const int stride = (int)a.layerStride, inter = (int)a.interEntries, layers = a.nY + 1;
+    const int posBlocks = (stride + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int chunks = (layers + kHoLayerChunk - 1) / kHoLayerChunk;
+    const long long items = (long long)posBlocks * chunks;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int lc = (int)(it / posBlocks);
+        const int pos = (int)(it - (long long)lc * posBlocks) * (int)blockDim.x + (int)threadIdx.x;
+        if (pos >= stride) continue;
+        const int l0 = lc * kHoLayerChunk, l1 = min(l0 + kHoLayerChunk, layers);
+        const bool isInter = pos < inter;
+        const int t = isInter ? __ldg(a.tedgeInter + pos) : __ldg(a.tedgeIntra + (pos - inter));
         if (t < 0) {
-            a.out0[idx] = nan;
-            if (a.out1) a.out1[idx] = nan;
-            return;
+            for (int l = l0; l < l1; ++l) {
+                const long long idx = (long long)l * stride + pos;
+                a.out0[idx] = nan;
+                if (a.out1) a.out1[idx] = nan;
+            }
+            continue;
         }
-        const int b = pos < a.interEntries ? l - 1 : l;
-        const int s2 = __ldg(a.EY + 2 * b), m2 = __ldg(a.EY + 2 * b + 1);
-        const int t2 = __ldg(a.EY + 2 * ((b + 1) % a.nY) + 1);
-        int y0, y1, y2;
-        switch (__ldg(a.eY + t)) {
-            case 2: y0 = s2; y1 = s2; y2 = s2; break;
-            case 3: y0 = s2; y1 = s2; y2 = m2; break;
-            case 4: y0 = s2; y1 = m2; y2 = t2; break;
-            default: y0 = s2; y1 = m2; y2 = m2; break;
-        }
+        const int pat = __ldg(a.eY + t);
         const int x0 = __ldg(a.eX + 3 * t), x1 = __ldg(a.eX + 3 * t + 1), x2 = __ldg(a.eX + 3 * t + 2);
-        double so3 = 0.0;
+        double dxx[3] = {0.0, 0.0, 0.0};
+        if (needLi) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double dx = __ldg(a.VX + 3 * x0 + j) - __ldg(a.VX + 3 * x1 + j);
+                dxx[j] = dx * dx;
+            }
+        }
+        int eSrc = 0, eTrgt = 0, eNext = 0;
         if (a.quat) {
-            const long long q0 = quat_index(a, b, __ldg(a.eSrc + t));
-            const long long q1 = quat_index(a, (b + __ldg(a.eNext + t)) % a.nY, __ldg(a.eTrgt + t));
-            so3 = so3_distance(ldg_quat(a.quat + q0), ldg_quat(a.quat + q1));
+            eSrc = __ldg(a.eSrc + t);
+            eTrgt = __ldg(a.eTrgt + t);
+            eNext = __ldg(a.eNext + t);
         }
-        const double rl = a.quat ? robust_loss(a, so3) : rl0;
-        const double fd = __ldg(a.FD + (long long)x2 * a.nvy + y2);
-        const double li = needLi ? line_integral(a, y0, y1, x0, x1) : 0.0;
-        const bool degenerate = (y2 == y1 || x2 == x1);
-        const int cm = a.costMode, tm = a.timeMode;
-        double c0 = 0, c1 = 0;
-        if (cm == VANILLA && tm == VANILLA) {
-            c0 = rl + fd;
-        } else if (cm == VANILLA && tm == LENGTH) {
-            c0 = rl + fd;
-            c1 = li;
-        } else if (cm == LENGTH && tm == VANILLA) {
-            c0 = li;
-        } else if (cm == VANILLA && tm == PENALISE_DEGENERATE) {
-            c0 = rl + fd;
-            c1 = degenerate ? 0.1 : 1;
-        } else if (cm == PENALISE_DEGENERATE && tm == VANILLA) {
-            c0 = degenerate ? 0.1 : 1;
-        } else if (cm == FEATURE && tm == SO3_PLAIN) {
-            c0 = fd;
-            c1 = fmax(0.0, twoPi - so3);
-        } else if (cm == FEATURE && tm == SO3_ROBUST) {
-            c0 = fd;
-            c1 = fmax(0.0, a.maxSO3 - rl);
-        } else if (cm == SO3_ROBUST && tm == FEATURE) {
-            c0 = rl;
-            c1 = fmax(0.0, a.maxFd - fd);
-        } else {  // SO3_PLAIN, FEATURE
-            c0 = so3;
-            c1 = fmax(0.0, a.maxFd - fd);
+        const double* fdRow = a.FD + (long long)x2 * a.nvy;
+        for (int l = l0; l < l1; ++l) {
+            const long long idx = (long long)l * stride + pos;
+            if (isInter ? l < 1 : l >= a.nY) {  // no edge in this layer's slot
+                a.out0[idx] = nan;
+                if (a.out1) a.out1[idx] = nan;
+                continue;
+            }
+            const int b = isInter ? l - 1 : l;
+            const int s2 = __ldg(a.EY + 2 * b), m2 = __ldg(a.EY + 2 * b + 1);
+            const int t2 = __ldg(a.EY + 2 * ((b + 1) % a.nY) + 1);
+            int y0, y1, y2;
+            switch (pat) {
+                case 2: y0 = s2; y1 = s2; y2 = s2; break;
+                case 3: y0 = s2; y1 = s2; y2 = m2; break;
+                case 4: y0 = s2; y1 = m2; y2 = t2; break;
+                default: y0 = s2; y1 = m2; y2 = m2; break;
+            }
+            double so3 = 0.0;
+            if (a.quat) {
+                const long long q0 = quat_index(a, b, eSrc);
+                const long long q1 = quat_index(a, (b + eNext) % a.nY, eTrgt);
+                so3 = so3_distance(ldg_quat(a.quat + q0), ldg_quat(a.quat + q1));
+            }
+            const double rl = a.quat ? robust_loss(a, so3) : rl0;
+            const double fd = __ldg(fdRow + y2);
+            double li = 0.0;
+            if (needLi) {  // line_integral's sum, in its order
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double dy = __ldg(a.VY + 3 * y0 + j) - __ldg(a.VY + 3 * y1 + j);
+                    li = li + dy * dy;
+                    li = li + dxx[j];
+                }
+                li = sqrt(li);
+            }
+            const bool degenerate = (y2 == y1 || x2 == x1);
+            const int cm = a.costMode, tm = a.timeMode;
+            double c0 = 0, c1 = 0;
+            if (cm == VANILLA && tm == VANILLA) {
+                c0 = rl + fd;
+            } else if (cm == VANILLA && tm == LENGTH) {
+                c0 = rl + fd;
+                c1 = li;
+            } else if (cm == LENGTH && tm == VANILLA) {
+                c0 = li;
+            } else if (cm == VANILLA && tm == PENALISE_DEGENERATE) {
+                c0 = rl + fd;
+                c1 = degenerate ? 0.1 : 1;
+            } else if (cm == PENALISE_DEGENERATE && tm == VANILLA) {
+                c0 = degenerate ? 0.1 : 1;
+            } else if (cm == FEATURE && tm == SO3_PLAIN) {
+                c0 = fd;
+                c1 = fmax(0.0, twoPi - so3);
+            } else if (cm == FEATURE && tm == SO3_ROBUST) {
+                c0 = fd;
+                c1 = fmax(0.0, a.maxSO3 - rl);
+            } else if (cm == SO3_ROBUST && tm == FEATURE) {
+                c0 = rl;
+                c1 = fmax(0.0, a.maxFd - fd);
+            } else {  // SO3_PLAIN, FEATURE
+                c0 = so3;
+                c1 = fmax(0.0, a.maxFd - fd);
+            }
+            a.out0[idx] = c0;
+            if (a.out1) a.out1[idx] = c1;
+            if (a.hist0) {
+                count_top_digit(topSh, r0, c0);
+                if (a.hist1) count_top_digit(topSh + kTopBins, r1, c1);
+            }
         }
-        a.out0[idx] = c0;
-        if (a.out1) a.out1[idx] = c1;
-        if (a.hist0) {
-            count_top_digit(topSh, r0, c0);
-            if (a.hist1) count_top_digit(topSh + kTopBins, r1, c1);
-        }
-    });
+    }
     top_digit_end(a, topSh, r0, r1);
 }
 
