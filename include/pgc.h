@@ -143,6 +143,12 @@ int pgc_set_feat_diff(pgc_graph* g, const double* feat_diff, int64_t rows, int64
  * slower per solve but leaves the rest of the GPU to other graphs. */
 int pgc_set_team_cap(pgc_graph* g, int max_ctas);
 
+/* No reference counterpart.  The Bellman-Ford team of this graph: ctas CTAs
+ * of threads_per_cta threads (a multiple of 32 in [32, 640]); 0 leaves
+ * either automatic.  Set by the autotuner (cyclic_product_graphs.autotune);
+ * results do not depend on it. */
+int pgc_set_team_shape(pgc_graph* g, int ctas, int threads_per_cta);
+
 /* No reference counterpart.  Solves `count` graphs concurrently: each one as
  * pgc_solve_with_cost_time_ratio (solver "lawlercpu"/"lawlergpu") or
  * pgc_solve_with_minimum_cost (any other name) would, on its own stream with

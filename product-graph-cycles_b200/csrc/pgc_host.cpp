@@ -323,6 +323,9 @@ class Graph {
     int wsK = -1;
     int ctlEpoch = 0, ctlWalkId = 0;
     int teamCap = 0;  // most CTAs of a Bellman-Ford launch (0: as many as help)
+    // team shape chosen for this graph (pgc_set_team_shape; 0: automatic);
+    // the PGC_BF_BLOCKS / PGC_BF_THREADS environment overrides take precedence
+    int shapeBlocks = 0, shapeThreads = 0;
     bool workspaceFresh = false;
 
     // last result
@@ -833,7 +836,9 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
         return bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(rowCap, costBytes, timeBytes);
     };
     const size_t tables = bf_shared_table_bytes(T.n, r.Kp);
-    const int envBlocks = env_int("PGC_BF_BLOCKS", 0), envThreads = env_int("PGC_BF_THREADS", 0);
+    int envBlocks = env_int("PGC_BF_BLOCKS", 0), envThreads = env_int("PGC_BF_THREADS", 0);
+    if (!envBlocks) envBlocks = shapeBlocks;
+    if (!envThreads) envThreads = shapeThreads;
     if (envThreads && (envThreads < 32 || envThreads > kBfThreads || envThreads % 32 != 0))
         throw Failure(PGC_ERR_ARG, "PGC_BF_THREADS must be a multiple of 32 in [32, 640]");
     int maxSl = 0, rowCap = 0;
@@ -2110,6 +2115,16 @@ int pgc_set_team_cap(pgc_graph* h, int max_ctas) {
     return guarded([&] {
         if (!h || max_ctas < 0) throw Failure(PGC_ERR_ARG, "max_ctas must be >= 0");
         h->g.teamCap = max_ctas;
+    });
+}
+
+int pgc_set_team_shape(pgc_graph* h, int ctas, int threads_per_cta) {
+    return guarded([&] {
+        if (!h || ctas < 0) throw Failure(PGC_ERR_ARG, "ctas must be >= 0");
+        if (threads_per_cta && (threads_per_cta < 32 || threads_per_cta > pgc::kBfThreads || threads_per_cta % 32 != 0))
+            throw Failure(PGC_ERR_ARG, "threads per CTA must be 0 or a multiple of 32 in [32, 640]");
+        h->g.shapeBlocks = ctas;
+        h->g.shapeThreads = threads_per_cta;
     });
 }
 

@@ -28,7 +28,7 @@ import numpy as np
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
-           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export"]
+           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -70,6 +70,7 @@ _lib.pgc_result_profile.argtypes = [_h, _lp]
 _lib.pgc_result_profile_detail.argtypes = [_h, _lp]
 _lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
 _lib.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
+_lib.pgc_set_team_shape.argtypes = [_h, ctypes.c_int, ctypes.c_int]
 _lib.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
 _lib.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
 _lib.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
@@ -245,6 +246,11 @@ class product_graph_generator:
         """Most CTAs a Bellman-Ford launch of this graph may use (0: no limit)."""
         _check(_lib.pgc_set_team_cap(self._h, int(max_ctas)))
 
+    def set_team_shape(self, ctas: int = 0, threads_per_cta: int = 0):
+        """Bellman-Ford team of this graph: ctas CTAs of threads_per_cta
+        threads (0: automatic).  Results do not depend on it (see autotune)."""
+        _check(_lib.pgc_set_team_shape(self._h, int(ctas), int(threads_per_cta)))
+
     def set_stream(self, cuda_stream: int | None):
         """Issue all device work of this generator on `cuda_stream` (a cudaStream_t as int)."""
         _check(_lib.pgc_set_stream(self._h, ctypes.c_void_p(cuda_stream) if cuda_stream else None))
@@ -288,6 +294,70 @@ def from_export(directory: str = ".", conjugate: bool = False, regularising_cost
     if "NX" in d:
         g.set_normals(d["NX"], d["NY"])
     return g
+
+
+def autotune(gen: "product_graph_generator", max_depth: int | None = None, candidates=None,
+             cache_path: str | None = None, repeats: int = 2) -> dict:
+    """Picks the Bellman-Ford team shape (CTAs, threads per CTA) for the shape
+    bucket of ``gen`` and applies it (no counterpart in the reference).
+
+    The bucket is (nodes per layer rounded up to a power of two, layers
+    rounded up to a power of two, max depth, whether layers have intralayer
+    edges).  A bucket found in the JSON file ``cache_path`` is applied
+    without timing.  Otherwise every candidate (ctas, threads_per_cta) --
+    by default the automatic shape, the automatic CTA count with 320 and 480
+    threads, and a half-size team -- is timed over ``repeats`` ratio solves
+    (costs regenerated before each; the Bellman-Ford device time of the solve
+    is compared), the fastest is applied, and the bucket's entry, with every
+    candidate's time, is written to the cache.  The shape changes the speed
+    only: every solve returns the same result.
+    """
+    import json
+
+    info = gen.graph_info()
+    k = int(max_depth) if max_depth is not None else None
+
+    def p2(x):
+        return 1 << max(0, int(x) - 1).bit_length()
+
+    key = f"n{p2(info['nodes_per_layer'])}-l{p2(info['layers'])}-k{k}-intra{int(info['intra_edges_per_layer'] > 0)}"
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    if key in cache:
+        e = cache[key]
+        gen.set_team_shape(e["ctas"], e["threads_per_cta"])
+        return dict(e, bucket=key, cached=True)
+
+    def timed(shape):
+        gen.set_team_shape(*shape)
+        best = None
+        for _ in range(max(1, repeats)):
+            gen.generate()
+            gen.solve_with_cost_time_ratio("lawlergpu", k)
+            ms = gen.last_stats()["device_us"] / 1000.0
+            best = ms if best is None else min(best, ms)
+        return best, gen.last_profile()
+
+    if candidates is None:
+        _, prof = timed((0, 0))
+        auto = int(prof["ctas"])
+        candidates = [(0, 0), (auto, 320), (auto, 480), (max(1, auto // 2), 640)]
+    results = []
+    for shape in candidates:
+        ms, prof = timed(tuple(shape))
+        results.append({"ctas": int(shape[0]), "threads_per_cta": int(shape[1]), "bf_ms": ms,
+                        "team": [int(prof["ctas"]), int(prof["threads"])]})
+    best = min(results, key=lambda r: r["bf_ms"])
+    entry = {"ctas": best["ctas"], "threads_per_cta": best["threads_per_cta"], "bf_ms": best["bf_ms"],
+             "candidates": results}
+    gen.set_team_shape(best["ctas"], best["threads_per_cta"])
+    if cache_path:
+        cache[key] = entry
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1)
+    return dict(entry, bucket=key, cached=False)
 
 
 def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas_per_graph: int = 0,
