@@ -252,6 +252,18 @@ int env_int(const char* name, int dflt) {
 void* host_buffer_alloc(size_t bytes) { return HostPool::get().allocate(bytes); }
 void host_buffer_free(void* p) { HostPool::get().deallocate(p); }
 
+// dst := src[0, count), copied by the host worker pool in 1 MB parts: the
+// feature-difference matrix of a large pair is tens of MB, and one thread
+// copies about 10 GB/s.
+template <class T>
+void copy_in(RawVec<T>& dst, const T* src, size_t count) {
+    dst.resize(count);
+    T* d = dst.data();
+    host_parallel_for((int64_t)count, (int64_t)((1 << 20) / sizeof(T)), [&](int64_t a, int64_t b) {
+        std::memcpy(d + a, src + a, (size_t)(b - a) * sizeof(T));
+    });
+}
+
 // A closed walk of the product graph as the reference stores it: original
 // node ids (targets in layer 0 that close a lap are written as the closing
 // copy numNodes + v only at the end), plus the edge and its cost/time for
@@ -1832,7 +1844,7 @@ void Graph::set_cost_vector(const double* in, int64_t rows, int64_t cols) {
 // A new feature-difference matrix; the next solve regenerates the costs.
 void Graph::set_feat_diff(const double* fd, int64_t rows, int64_t cols) {
     if (rows != nvx || cols != nvy) throw Failure(PGC_ERR_ARG, "feat_diff must be |VX| x |VY|");
-    FD.assign(fd, fd + rows * cols);
+    copy_in(FD, fd, (size_t)(rows * cols));
     if (templateReady) dFD.upload(FD.data(), FD.size(), stream);
     generated = false;
     adjKind = 0;
@@ -1937,7 +1949,7 @@ int pgc_create(const double* VX, int64_t nvx, const int32_t* EX, int64_t nex, co
         g.EX.assign(EX, EX + 2 * nex);
         g.VY.assign(VY, VY + 3 * nvy);
         g.EY.assign(EY, EY + 2 * ney);
-        g.FD.assign(feat_diff, feat_diff + nvx * nvy);
+        pgc::copy_in(g.FD, feat_diff, (size_t)(nvx * nvy));
         g.conj = use_conjugate_graph != 0;
         g.reg = use_regularising_cost_term != 0;
         g.prune = prune_intralayer != 0;
