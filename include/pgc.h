@@ -208,8 +208,9 @@ int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_
  * the sliced-ELL padding), cost columns]. */
 int pgc_graph_info(pgc_graph* g, int64_t* out8);
 
-/* Returns the device memory cached by the library's allocator to CUDA (no
- * reference counterpart; freed buffers are otherwise kept for reuse). */
+/* Returns the device memory and the pinned host memory cached by the
+ * library's allocators to CUDA (no reference counterpart; freed buffers are
+ * otherwise kept for reuse). */
 int pgc_release_cached_memory(void);
 
 /* Message of the last failing call on this thread ("" if none). */

@@ -106,6 +106,12 @@ class HostPool {
         free_.emplace(it->second, p);
         sizes_.erase(it);
     }
+    // Unpins and frees the cached blocks (live handles keep theirs).
+    void release_cached() {
+        std::lock_guard<std::mutex> lock(mu_);
+        for (auto& b : free_) cudaFreeHost(b.second);
+        free_.clear();
+    }
 
   private:
     std::mutex mu_;
@@ -2359,7 +2365,10 @@ int pgc_graph_info(pgc_graph* h, int64_t* out8) {
 }
 
 int pgc_release_cached_memory(void) {
-    return guarded([&] { pgc::DevicePool::get().release_cached(); });
+    return guarded([&] {
+        pgc::DevicePool::get().release_cached();
+        pgc::HostPool::get().release_cached();
+    });
 }
 
 const char* pgc_last_error(void) { return pgc::g_lastError.c_str(); }

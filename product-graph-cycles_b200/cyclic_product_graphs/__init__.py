@@ -28,7 +28,7 @@ import numpy as np
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
-           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune"]
+           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune", "release_cached_memory"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -261,6 +261,12 @@ class product_graph_generator:
         keys = ["bf_calls", "sweeps", "candidates", "lawler_iters", "branches", "fallback_walks", "device_us",
                 "kernel_launches"]
         return dict(zip(keys, list(buf)))
+
+
+def release_cached_memory():
+    """Returns the device memory and the pinned host memory that the
+    library's allocators keep for reuse (no counterpart in the reference)."""
+    _check(_lib.pgc_release_cached_memory())
 
 
 def load_export(directory: str = ".") -> dict:
