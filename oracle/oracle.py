@@ -136,6 +136,13 @@ class OracleGenerator:
         if lib().orc_set_cost(self._h, E.ctypes.data_as(_dp), E.shape[0], E.shape[1]) != 0:
             raise ValueError("cost vector has the wrong number of rows")
 
+    def product_space_rows(self) -> int:
+        """Number of product edges, without copying the product space."""
+        self._ensure()
+        r, c = _i64(), _i64()
+        lib().orc_ps_shape(self._h, ctypes.byref(r), ctypes.byref(c))
+        return int(r.value)
+
     def get_product_space(self):
         self._ensure()
         r, c = _i64(), _i64()
