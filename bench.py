@@ -441,6 +441,25 @@ def _batch_pair(spec):
     return {k: p[k] for k in ("VX", "EX", "VY", "EY", "feat_diff")}
 
 
+def _batch_config(workload, pairs, world):
+    """The `config` of a batch line, the same in both arms.  A plain block
+    holds 2|EX| + |VX| edges (an intra- and an interlayer copy of every X
+    edge, and the vertical edges), so the total is known from the inputs."""
+    return {"workload": workload, "pairs": len(pairs), "vx_range": BATCHES[workload][1],
+            "vy_range": BATCHES[workload][2], "k": BATCHES[workload][3],
+            "edges_total": int(sum(len(p["EY"]) * (2 * len(p["EX"]) + len(p["VX"])) for p in pairs)),
+            "parallelism": f"one stream + a small CTA team per pair, replicas x{world}",
+            "l2": "inputs larger than L2 (all pairs' cost streams together)"}
+
+
+def _fwdbwd_config(workload, pairs, k, world):
+    """The `config` of a fwd/bwd line, the same in both arms."""
+    return {"workload": workload, "pairs": int(pairs), "vx": FWDBWD[workload][1], "vy": FWDBWD[workload][2],
+            "k": int(k), "feature_dim": FWDBWD[workload][4],
+            "parallelism": f"one stream + a small CTA team per pair, replicas x{world}",
+            "l2": "per-pair streams of all pairs exceed L2"}
+
+
 def _batch_pairs(name, seed):
     """The batch's seeded pairs, built in parallel host processes (spawned, before any GPU work)."""
     import multiprocessing as mp
@@ -540,11 +559,7 @@ def run_batch(args, world, rank):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 (fp32 integer-valued cost streams)", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "pairs": len(pairs), "vx_range": BATCHES[args.workload][1],
-                   "vy_range": BATCHES[args.workload][2], "k": BATCHES[args.workload][3],
-                   "edges_total": sum(i["layers"] * i["edges_per_block"] for i in infos),
-                   "parallelism": f"one stream + a small CTA team per pair, replicas x{world}",
-                   "l2": "inputs larger than L2 (all pairs' cost streams together)"},
+        "config": _batch_config(args.workload, pairs, world),
         "vs_plain_gpu_lawler": {"plain_solves_per_s": seq_value, "ratio": value / seq_value,
                                 "sample": f"all {seq_n} pairs solved one after the other, full-GPU teams"},
         "e2e": {"value": world * len(pairs) / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
@@ -592,7 +607,7 @@ def run_reference_batch(args):
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "pairs": len(specs)},
+            "config": _batch_config(args.workload, pairs, int(os.environ.get("WORLD_SIZE", "1"))),
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
                              "sample": "oracle generate + lawlercpu of one pair of the batch per step "
                                        "(pairs 0..steps-1), median"},
@@ -705,10 +720,7 @@ def run_fwdbwd(args, world, rank):
         "metric": METRIC, "value": value, "unit": "fwd+bwd pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 solve / fp32 features", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "pairs": len(pairs), "vx": FWDBWD[args.workload][1],
-                   "vy": FWDBWD[args.workload][2], "k": k, "feature_dim": FWDBWD[args.workload][4],
-                   "parallelism": f"one stream + a small CTA team per pair, replicas x{world}",
-                   "l2": "per-pair streams of all pairs exceed L2"},
+        "config": _fwdbwd_config(args.workload, len(pairs), k, world),
         "vs_plain_gpu_lawler": {"plain_pairs_per_s": plain_value, "ratio": value / plain_value,
                                 "sample": "the same pairs, forward + backward one after the other, full-GPU teams"},
         "e2e": {"value": world * len(pairs) / e2e_s, "unit": "fwd+bwd pairs/s", "h2d_bytes_per_step": h2d,
@@ -741,7 +753,7 @@ def run_reference_fwdbwd(args):
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": "fwd+bwd pairs/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload},
+            "config": _fwdbwd_config(args.workload, len(specs), specs[0]["k"], int(os.environ.get("WORLD_SIZE", "1"))),
             "cpu_baseline": {"value": value, "unit": "fwd+bwd pairs/s", "cores": os.cpu_count() or 1, "kind": "port",
                              "sample": "oracle generate + lawlercpu of one pair per step (forward only: the "
                                        "reference has no backward), median"},
