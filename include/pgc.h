@@ -197,6 +197,15 @@ int pgc_result_profile_detail(pgc_graph* g, int64_t* out4);
  * V [nv x 3], E [ne x 2] with ne == nv; out [nv x 3]. */
 int pgc_compute_normals_2d(const double* V, int64_t nv, const int32_t* E, int64_t ne, double* out);
 
+/* No reference counterpart.  Sizes of the product graph of X (EX [nex x 2],
+ * |VX| = nvx) with a closed curve of ney edges, built on the host without a
+ * GPU: out6 = {nodes per layer, edges per block (= per Y edge), interlayer
+ * edges per block, intralayer edges per block, 32-node slices, sliced-ELL
+ * rows of both parts}.  The product graph has ney * out6[1] edges, the rows
+ * of the reference's productspace. */
+int pgc_product_graph_sizes(const int32_t* EX, int64_t nex, int64_t nvx, int64_t ney, int conjugate,
+                            int prune_intralayer_edges, int64_t* out6);
+
 /* utils::normals3d (helper/utils.cpp:86-90, bindings.cpp:26): area-weighted
  * vertex normals of a triangle mesh (libigl per_vertex_normals with its
  * default weighting).  V [nv x 3], F [nf x 3]; out [nv x 3]. */

@@ -2261,6 +2261,30 @@ int pgc_result_stats(pgc_graph* h, int64_t* out8) {
 }
 
 // utils::normals2d (helper/utils.cpp:93-157).
+int pgc_product_graph_sizes(const int32_t* EX, int64_t nex, int64_t nvx, int64_t ney, int conjugate,
+                            int prune_intralayer_edges, int64_t* out6) {
+    return guarded([&] {
+        if (!EX || !out6) throw Failure(PGC_ERR_ARG, "null argument");
+        std::vector<int> ey((size_t)(2 * std::max<int64_t>(ney, 0)));
+        for (int64_t i = 0; i < ney; ++i) {
+            ey[(size_t)(2 * i)] = (int)i;
+            ey[(size_t)(2 * i + 1)] = (int)((i + 1) % ney);
+        }
+        pgc::LayerTemplate T;
+        const std::string err = pgc::build_template(EX, nex, ey.data(), ney, nvx, conjugate != 0,
+                                                    prune_intralayer_edges != 0, T);
+        if (!err.empty()) throw Failure(PGC_ERR_ARG, err);
+        int64_t inter = 0;
+        for (int64_t t = 0; t < T.eBlock; ++t) inter += T.eNext[(size_t)t] ? 1 : 0;
+        out6[0] = T.n;
+        out6[1] = T.eBlock;
+        out6[2] = inter;
+        out6[3] = T.eBlock - inter;
+        out6[4] = T.nslices;
+        out6[5] = (T.entries[pgc::INTER] + T.entries[pgc::INTRA]) / 32;
+    });
+}
+
 int pgc_compute_normals_2d(const double* Vin, int64_t nv, const int32_t* E, int64_t ne, double* out) {
     return guarded([&] {
         if (nv != ne) throw Failure(PGC_ERR_ARG, "V.rows() != E.rows()");

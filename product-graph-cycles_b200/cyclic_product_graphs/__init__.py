@@ -28,7 +28,8 @@ import numpy as np
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
-           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune", "release_cached_memory"]
+           "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune", "release_cached_memory",
+           "product_graph_sizes"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -71,6 +72,7 @@ _lib.pgc_result_profile_detail.argtypes = [_h, _lp]
 _lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
 _lib.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
 _lib.pgc_set_team_shape.argtypes = [_h, ctypes.c_int, ctypes.c_int]
+_lib.pgc_product_graph_sizes.argtypes = [_ip, _i64, _i64, _i64, ctypes.c_int, ctypes.c_int, _lp]
 _lib.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
 _lib.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
 _lib.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
@@ -261,6 +263,24 @@ class product_graph_generator:
         keys = ["bf_calls", "sweeps", "candidates", "lawler_iters", "branches", "fallback_walks", "device_us",
                 "kernel_launches"]
         return dict(zip(keys, list(buf)))
+
+
+def product_graph_sizes(EX, n_vertices_x: int, n_edges_y: int, conjugate: bool = False,
+                        prune_intralayer_edges: bool = False) -> dict:
+    """Sizes of the product graph of X and a closed curve with ``n_edges_y``
+    edges, from the layer template built on the host (no GPU needed; no
+    counterpart in the reference)."""
+    EX = np.ascontiguousarray(EX, dtype=np.int32)
+    if EX.ndim != 2 or EX.shape[1] != 2:
+        raise ValueError("EX must be [n x 2]")
+    out = (ctypes.c_int64 * 6)()
+    _check(_lib.pgc_product_graph_sizes(EX.ctypes.data_as(_ip), EX.shape[0], int(n_vertices_x), int(n_edges_y),
+                                        int(bool(conjugate)), int(bool(prune_intralayer_edges)), out))
+    keys = ["nodes_per_layer", "edges_per_block", "inter_edges_per_block", "intra_edges_per_block", "slices",
+            "ell_rows"]
+    d = dict(zip(keys, list(out)))
+    d["edges"] = d["edges_per_block"] * int(n_edges_y)
+    return d
 
 
 def release_cached_memory():
