@@ -109,6 +109,11 @@ std::string build_template(const int* EX, int64_t nEX, const int* EY, int64_t nE
 // process's host worker pool (inline when another job holds the pool).
 void host_parallel_for(int64_t n, int64_t grain, const std::function<void(int64_t, int64_t)>& f);
 
+// Contiguous slice ranges [cut[c], cut[c+1]) of `blocks` CTAs of `warps`
+// warps for the Bellman-Ford team, balanced on the per-step work of their
+// slowest warps; rowsPerBatch[p] = rows a warp gathers per batch in part p.
+std::vector<int> plan_cta_cuts(const LayerTemplate& T, int blocks, int K, int warps, const int rowsPerBatch[2]);
+
 // productspace row of global edge id e (product_space.cpp / conj_product_space.cpp order).
 void product_row(const LayerTemplate& T, const int* EY, int64_t e, int* out);
 

@@ -922,110 +922,17 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     return r;
 }
 
-// Contiguous slice ranges for `blocks` CTAs of `warps` warps with balanced
-// step times.  A warp relaxes the CTA's slices that have rows in the step's
-// part, round-robin, and one slice of one step costs it about (gather
-// batches + 1) memory latencies: the batches of its rows and the epilogue
-// (the winner's record, the stores).  Slices without rows are visited only
-// by two steps per sweep and cost nothing here.
-// Steps are coupled across the team by the hand-offs, so a layer costs the
-// slowest warp of any CTA in the interlayer step plus K - 1 times the
-// slowest in an intralayer step (those run only when the layer has
-// intralayer edges).  The cuts therefore bound the two kinds separately:
-// for bounds (bi, bj) CTAs are filled greedily while their slowest warps
-// stay within both -- optimal for the pair, since a range's costs never grow
-// when it shrinks -- and the pair with the smallest bi + (K - 1) bj that
-// fits in `blocks` CTAs is kept (bj in steps of one latency, bi by binary
-// search).  Costs are in 1/32 of a latency.  Cached per (blocks, K, warps).
+// CTA slice ranges of the team (plan_cta_cuts), cached per (blocks, K,
+// warps).  A warp gathers bf_rows_per_batch(K) interlayer rows per batch
+// (one row when K > 4) and bf_rows_per_batch(1) intralayer rows.
 std::vector<int> Graph::cta_cuts(int blocks, int K, int warps) const {
-    const int ns = T.nslices;
-    std::vector<int> cut((size_t)blocks + 1, ns);
-    cut[0] = 0;
-    if (blocks <= 1 || ns == 0) return cut;
-    warps = std::max(1, warps);
     const std::string key = std::to_string(blocks) + "/" + std::to_string(K) + "/" + std::to_string(warps);
     {
         const auto it = cutCache.find(key);
         if (it != cutCache.end()) return it->second;
     }
-    const bool intra = T.entries[INTRA] > 0 && K > 1;
     const int rb[2] = {K <= 4 ? bf_rows_per_batch(K) : 1, bf_rows_per_batch(1)};
-    std::vector<long long> w[2];
-    long long lo[2] = {0, 0}, hi[2] = {0, 0};
-    for (int p = 0; p < 2; ++p) {
-        w[p].resize((size_t)ns);
-        for (int s = 0; s < ns; ++s) {
-            const int rows = T.sp[p][(size_t)s + 1] - T.sp[p][(size_t)s];
-            w[p][(size_t)s] = (p == 1 && !intra) || rows == 0 ? 0 : 32LL * ((rows + rb[p] - 1) / rb[p] + 1);
-            lo[p] = std::max(lo[p], w[p][(size_t)s]);
-            hi[p] += w[p][(size_t)s];
-        }
-    }
-    std::vector<long long> acc[2] = {std::vector<long long>((size_t)warps), std::vector<long long>((size_t)warps)};
-    // fills CTAs greedily under (bi, bj); returns the CTAs used (cuts in c
-    // when given).  A CTA's warps take its slices with rows in a part
-    // round-robin (a0, a1: the warp that gets the next one); slices without
-    // rows cost nothing.
-    auto fill = [&](long long bi, long long bj, std::vector<int>* c) -> int {
-        int used = 1, start = 0, a0 = 0, a1 = 0;
-        long long* acc0 = acc[0].data();
-        long long* acc1 = acc[1].data();
-        std::fill(acc0, acc0 + warps, 0);
-        std::fill(acc1, acc1 + warps, 0);
-        const long long* w0 = w[0].data();
-        const long long* w1 = w[1].data();
-        for (int s = 0; s < ns; ++s) {
-            const long long x0 = w0[s], x1 = w1[s];
-            if (s > start && ((x0 && acc0[a0] + x0 > bi) || (x1 && acc1[a1] + x1 > bj))) {
-                if (c && used < blocks) (*c)[(size_t)used] = s;
-                if (++used > blocks && !c) return used;
-                start = s;
-                a0 = a1 = 0;
-                std::fill(acc0, acc0 + warps, 0);
-                std::fill(acc1, acc1 + warps, 0);
-            }
-            if (x0) {
-                acc0[a0] += x0;
-                if (++a0 == warps) a0 = 0;
-            }
-            if (x1) {
-                acc1[a1] += x1;
-                if (++a1 == warps) a1 = 0;
-            }
-        }
-        return used;
-    };
-    const long long reps = intra ? K - 1 : 0;
-    // the smallest intralayer bound that fits at all, then up from there
-    long long j0 = lo[1], j1 = hi[1];
-    while (j0 < j1) {
-        const long long mid = j0 + (j1 - j0) / 2;
-        if (fill(hi[0], mid, nullptr) <= blocks) j1 = mid;
-        else j0 = mid + 1;
-    }
-    long long bestI = -1, bestJ = -1, bestCost = 0;
-    for (long long bj = j0, tries = 0; tries < 64; bj += 32, ++tries) {
-        if (bestI >= 0 && reps * bj >= bestCost) break;
-        if (bj > hi[1]) bj = hi[1];
-        if (fill(hi[0], bj, nullptr) <= blocks) {
-            long long a = lo[0], b = hi[0];
-            while (a < b) {
-                const long long mid = a + (b - a) / 2;
-                if (fill(mid, bj, nullptr) <= blocks) b = mid;
-                else a = mid + 1;
-            }
-            const long long cost = a + reps * bj;
-            if (bestI < 0 || cost < bestCost) {
-                bestI = a;
-                bestJ = bj;
-                bestCost = cost;
-            }
-        }
-        if (bj >= hi[1] || !intra) break;
-    }
-    const int used = fill(bestI, bestJ, &cut);
-    // CTAs past the last range keep empty ranges at the end
-    for (int c = used; c < blocks; ++c) cut[(size_t)c] = ns;
+    std::vector<int> cut = plan_cta_cuts(T, blocks, K, warps, rb);
     cutCache[key] = cut;
     return cut;
 }
