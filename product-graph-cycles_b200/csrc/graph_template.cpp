@@ -495,4 +495,51 @@ std::vector<int> plan_cta_cuts(const LayerTemplate& T, int blocks, int K, int wa
     return cut;
 }
 
+// Wait lists of the Bellman-Ford team in CSR form (ptr: blocks + 1 offsets,
+// idx: CTA ids, ascending per list): CTA c lists every other CTA d joined to
+// it by an in-edge of either part, i.e. d owns the slice of a source of one
+// of c's in-edges (c reads d's rows) or c owns the slice of a source of one
+// of d's (d reads c's rows, so d must be done before c overwrites them).
+// CTA c owns the slices [cut[c], cut[c+1]).  The product graph repeats one
+// layer template, so one pass over the template covers every layer; the
+// closing layer's sources are a subset of the interlayer ones.
+void cta_wait_lists(const LayerTemplate& T, const std::vector<int>& cut, std::vector<int>& ptr, std::vector<int>& idx) {
+    const int blocks = (int)cut.size() - 1;
+    std::vector<int> owner((size_t)T.nslices);
+    for (int c = 0; c < blocks; ++c)
+        for (int s = cut[(size_t)c]; s < cut[(size_t)c + 1]; ++s) owner[(size_t)s] = c;
+    // the CTA pairs joined by an in-edge, in parallel over slices (each part
+    // of the range marks its own matrix; the matrices are OR-ed)
+    std::vector<unsigned char> adj((size_t)blocks * blocks, 0);
+    std::mutex adjMu;
+    host_parallel_for(T.nslices, 256, [&](int64_t s0, int64_t s1) {
+        std::vector<unsigned char> mine((size_t)blocks * blocks, 0);
+        for (int p = 0; p < 2; ++p) {
+            for (int64_t s = s0; s < s1; ++s) {
+                const int ct = owner[(size_t)s];
+                int last = ct;
+                for (int j = T.sp[p][(size_t)s]; j < T.sp[p][(size_t)s + 1]; ++j)
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int sv = T.src[p][(size_t)j * 32 + lane];
+                        if (sv < 0) continue;
+                        const int cs = owner[(size_t)(sv >> 5)];
+                        if (cs == ct || cs == last) continue;
+                        last = cs;
+                        mine[(size_t)ct * blocks + cs] = 1;
+                        mine[(size_t)cs * blocks + ct] = 1;
+                    }
+            }
+        }
+        std::lock_guard<std::mutex> lock(adjMu);
+        for (size_t i = 0; i < adj.size(); ++i) adj[i] |= mine[i];
+    });
+    ptr.assign((size_t)blocks + 1, 0);
+    idx.clear();
+    for (int c = 0; c < blocks; ++c) {
+        for (int d = 0; d < blocks; ++d)
+            if (adj[(size_t)c * blocks + d]) idx.push_back(d);
+        ptr[(size_t)c + 1] = (int)idx.size();
+    }
+}
+
 }  // namespace pgc

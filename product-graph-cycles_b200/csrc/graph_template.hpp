@@ -114,6 +114,11 @@ void host_parallel_for(int64_t n, int64_t grain, const std::function<void(int64_
 // slowest warps; rowsPerBatch[p] = rows a warp gathers per batch in part p.
 std::vector<int> plan_cta_cuts(const LayerTemplate& T, int blocks, int K, int warps, const int rowsPerBatch[2]);
 
+// Wait lists of the Bellman-Ford team for the CTA slice ranges `cut`: CTA c
+// lists, in ascending order in idx[ptr[c]..ptr[c+1]), every other CTA joined
+// to it by an in-edge of the layer template in either direction.
+void cta_wait_lists(const LayerTemplate& T, const std::vector<int>& cut, std::vector<int>& ptr, std::vector<int>& idx);
+
 // productspace row of global edge id e (product_space.cpp / conj_product_space.cpp order).
 void product_row(const LayerTemplate& T, const int* EY, int64_t e, int* out);
 

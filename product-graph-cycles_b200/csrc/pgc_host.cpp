@@ -937,49 +937,14 @@ std::vector<int> Graph::cta_cuts(int blocks, int K, int warps) const {
     return cut;
 }
 
-// Slice range of every CTA (cta_cuts), and every CTA's wait list: the CTAs that own a source
-// of one of its in-edges (it reads their rows) or read one of its nodes
-// through an in-edge (they must be done before it overwrites a row).  The
-// product graph repeats one layer template, so one pass over the template
-// covers every layer; the closing layer's sources are a subset of the
-// interlayer ones.
+// Uploads the slice range of every CTA (cta_cuts) and every CTA's wait list
+// (cta_wait_lists: the CTAs whose rows it reads through an in-edge, and the
+// CTAs that read its rows).
 void Graph::upload_cta_slices(const std::vector<int>& cut, int K, int warps) {
     const int blocks = (int)cut.size() - 1;
     if (cutBlocks == blocks && cutK == K && cutWarps == warps && ctaCut == cut) return;
-    std::vector<int> owner((size_t)T.nslices);
-    for (int c = 0; c < blocks; ++c)
-        for (int s = cut[(size_t)c]; s < cut[(size_t)c + 1]; ++s) owner[(size_t)s] = c;
-    // the CTA pairs joined by an in-edge, in parallel over slices (each part
-    // of the range marks its own matrix; the matrices are OR-ed)
-    std::vector<unsigned char> adj((size_t)blocks * blocks, 0);
-    std::mutex adjMu;
-    host_parallel_for(T.nslices, 256, [&](int64_t s0, int64_t s1) {
-        std::vector<unsigned char> mine((size_t)blocks * blocks, 0);
-        for (int p = 0; p < 2; ++p) {
-            for (int64_t s = s0; s < s1; ++s) {
-                const int ct = owner[(size_t)s];
-                int last = ct;
-                for (int j = T.sp[p][(size_t)s]; j < T.sp[p][(size_t)s + 1]; ++j)
-                    for (int lane = 0; lane < 32; ++lane) {
-                        const int sv = T.src[p][(size_t)j * 32 + lane];
-                        if (sv < 0) continue;
-                        const int cs = owner[(size_t)(sv >> 5)];
-                        if (cs == ct || cs == last) continue;
-                        last = cs;
-                        mine[(size_t)ct * blocks + cs] = 1;
-                        mine[(size_t)cs * blocks + ct] = 1;
-                    }
-            }
-        }
-        std::lock_guard<std::mutex> lock(adjMu);
-        for (size_t i = 0; i < adj.size(); ++i) adj[i] |= mine[i];
-    });
-    std::vector<int> ptr((size_t)blocks + 1, 0), idx;
-    for (int c = 0; c < blocks; ++c) {
-        for (int d = 0; d < blocks; ++d)
-            if (adj[(size_t)c * blocks + d]) idx.push_back(d);
-        ptr[(size_t)c + 1] = (int)idx.size();
-    }
+    std::vector<int> ptr, idx;
+    cta_wait_lists(T, cut, ptr, idx);
     wCtaSlice.upload(cut.data(), cut.size(), stream);
     wWaitPtr.upload(ptr.data(), ptr.size(), stream);
     if (idx.empty()) idx.push_back(0);  // keep a valid pointer; ptr says the lists are empty

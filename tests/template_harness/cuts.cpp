@@ -9,6 +9,10 @@
 // The exact search takes every intralayer cost a range can have as the
 // bound, finds by dynamic programming the partition whose ranges all stay
 // within it with the smallest interlayer maximum, and keeps the best sum.
+// For the planned ranges and for equal slice counts it also checks the
+// team's wait lists (cta_wait_lists) against the ones that follow from the
+// template's edge list: every template edge joins the CTA that owns its
+// target's slice and the one that owns its source's slice, both ways.
 // Usage: cuts EX.bin nVX conj prune nY
 #include "graph_template.hpp"
 
@@ -101,6 +105,34 @@ struct Model {
     }
 };
 
+// wait lists that follow from the template's edges (CSR, ascending)
+void edge_wait_lists(const LayerTemplate& T, const std::vector<int>& cut, std::vector<int>& ptr,
+                     std::vector<int>& idx) {
+    const int blocks = (int)cut.size() - 1;
+    std::vector<int> owner((size_t)T.nslices);
+    for (int c = 0; c < blocks; ++c)
+        for (int s = cut[(size_t)c]; s < cut[(size_t)c + 1]; ++s) owner[(size_t)s] = c;
+    std::vector<char> adj((size_t)blocks * blocks, 0);
+    for (int64_t t = 0; t < T.eBlock; ++t) {
+        const int a = owner[(size_t)(T.eSrc[(size_t)t] >> 5)], b = owner[(size_t)(T.eTrgt[(size_t)t] >> 5)];
+        if (a != b) adj[(size_t)a * blocks + b] = adj[(size_t)b * blocks + a] = 1;
+    }
+    ptr.assign((size_t)blocks + 1, 0);
+    idx.clear();
+    for (int c = 0; c < blocks; ++c) {
+        for (int d = 0; d < blocks; ++d)
+            if (adj[(size_t)c * blocks + d]) idx.push_back(d);
+        ptr[(size_t)c + 1] = (int)idx.size();
+    }
+}
+
+bool same_wait_lists(const LayerTemplate& T, const std::vector<int>& cut) {
+    std::vector<int> p0, i0, p1, i1;
+    cta_wait_lists(T, cut, p0, i0);
+    edge_wait_lists(T, cut, p1, i1);
+    return p0 == p1 && i0 == i1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -125,7 +157,7 @@ int main(int argc, char** argv) {
         std::printf("error %s\n", err.c_str());
         return 1;
     }
-    int cases = 0, bad = 0;
+    int cases = 0, bad = 0, badWait = 0;
     for (int K = 1; K <= 6; ++K)
         for (int warps : {1, 2, 3, 20})
             for (int blocks : {1, 2, 3, 5, 8, 13}) {
@@ -136,6 +168,10 @@ int main(int argc, char** argv) {
                 for (int i = 0; ok && i < blocks; ++i) ok = cut[(size_t)i] <= cut[(size_t)i + 1];
                 const ll got = ok ? m.objective(cut) : -1, want = m.best(blocks);
                 ++cases;
+                if (ok && !same_wait_lists(T, cut)) {
+                    ++badWait;
+                    if (badWait <= 10) std::printf("K=%d warps=%d blocks=%d: wait lists differ\n", K, warps, blocks);
+                }
                 if (!ok || got != want) {
                     ++bad;
                     if (bad <= 10)
@@ -143,7 +179,17 @@ int main(int argc, char** argv) {
                                     want, ok ? "" : " (malformed cuts)");
                 }
             }
-    std::printf("%d of %d plans differ from the best (slices %d, intralayer entries %lld)\n", bad, cases, T.nslices,
-                (long long)T.entries[INTRA]);
-    return bad ? 1 : 0;
+    // equal slice counts, as many CTAs as slices at most
+    for (int blocks : {2, 7, 64, 148}) {
+        std::vector<int> cut((size_t)blocks + 1);
+        for (int c = 0; c <= blocks; ++c) cut[(size_t)c] = (int)((long long)T.nslices * c / blocks);
+        ++cases;
+        if (!same_wait_lists(T, cut)) {
+            ++badWait;
+            std::printf("equal cuts, blocks=%d: wait lists differ\n", blocks);
+        }
+    }
+    std::printf("%d of %d plans differ from the best, %d wait lists differ (slices %d, intralayer entries %lld)\n",
+                bad, cases - 4, badWait, T.nslices, (long long)T.entries[INTRA]);
+    return bad || badWait ? 1 : 0;
 }

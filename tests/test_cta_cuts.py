@@ -2,7 +2,8 @@
 (K, warps, blocks) of a grid, the planner's contiguous ranges reach the
 smallest step cost that any partition of the template's slices into at most
 `blocks` ranges has under the same cost model (exact search by dynamic
-programming over every intralayer bound)."""
+programming over every intralayer bound), and the team's wait lists equal
+the CTA pairs that the template's edges join."""
 import os
 import subprocess
 
@@ -33,4 +34,4 @@ def test_cuts_reach_the_best_partition(cuts, tmp_path, n_vertices, conj, prune):
     r = subprocess.run([cuts, str(ex), str(len(p["VX"])), str(int(conj)), str(int(prune)), "5"],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.startswith("0 of 144 plans differ")
+    assert r.stdout.startswith("0 of 144 plans differ from the best, 0 wait lists differ")
