@@ -29,7 +29,7 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
            "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune", "release_cached_memory",
-           "product_graph_sizes"]
+           "product_graph_sizes", "vertex_correspondences"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -406,6 +406,27 @@ def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas
     _check(_lib.pgc_solve_batch(arr, len(gens), str(solver_name).encode(), -1 if max_depth is None else int(max_depth),
                                 int(ctas_per_graph), int(workers), int(bool(regenerate)), status))
     return [g._result() for g in gens]
+
+
+def vertex_correspondences(matching, conjugate: bool | None = None) -> np.ndarray:
+    """Vertex correspondences of a returned matching: one [x, y] row per
+    matching row, in the matching's cycle order (int32, L x 2).
+
+    This is the step after the solve in the reference's usage example
+    (README.md:79-85): column 0 of a matching row is the Y vertex it starts
+    at, and the X vertex is column 2 of a plain row [y0, y1, x0, x1] or
+    column 3 of a conjugate row [y0, y1, y2, x0, x1, x2].  `conjugate` None
+    takes the graph kind from the column count (4 plain, 6 conjugate).
+    """
+    m = np.asarray(matching)
+    if m.ndim != 2 or m.shape[1] not in (4, 6):
+        raise ValueError(f"a matching has 4 (plain) or 6 (conjugate) columns, got shape {m.shape}")
+    if conjugate is None:
+        conjugate = m.shape[1] == 6
+    if m.shape[1] != (6 if conjugate else 4):
+        raise ValueError(f"a {'conjugate' if conjugate else 'plain'} matching has {6 if conjugate else 4} columns, "
+                         f"got {m.shape[1]}")
+    return np.column_stack((m[:, 3 if conjugate else 2], m[:, 0])).astype(np.int32, copy=False)
 
 
 def compute_normals_2d(V, E) -> np.ndarray:
