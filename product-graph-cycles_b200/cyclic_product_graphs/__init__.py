@@ -335,8 +335,8 @@ def autotune(gen: "product_graph_generator", max_depth: int | None = None, candi
     threads, and a half-size team -- is timed over ``repeats`` ratio solves
     (costs regenerated before each; the Bellman-Ford device time of the solve
     is compared), the fastest is applied, and the bucket's entry, with every
-    candidate's time, is written to the cache.  The shape changes the speed
-    only: every solve returns the same result.
+    candidate's time, is merged into the cache file as it is then.  The
+    shape changes the speed only: every solve returns the same result.
     """
     import json
 
@@ -380,9 +380,16 @@ def autotune(gen: "product_graph_generator", max_depth: int | None = None, candi
              "candidates": results}
     gen.set_team_shape(best["ctas"], best["threads_per_cta"])
     if cache_path:
+        # buckets another tuner wrote meanwhile are kept; the file is
+        # replaced in one rename, so a reader never sees half of it
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                cache = json.load(f)
         cache[key] = entry
-        with open(cache_path, "w") as f:
+        tmp = f"{cache_path}.{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
             json.dump(cache, f, indent=1)
+        os.replace(tmp, cache_path)
     return dict(entry, bucket=key, cached=False)
 
 
