@@ -1257,6 +1257,25 @@ void Graph::solve_ratio(int K) {
         currentRatio = 10;
         const double ub = (double)std::numeric_limits<float>::infinity();
         const Control c = launch_bf_call(r, params(r, 1, 0, currentRatio, ub));
+        if (c.status == BF_LAYER_UNREACHED) {
+            // The sweep from the start node reached no node of some layer: a
+            // 2D-degenerate node of a conjugate graph with K = 1, whose
+            // out-edges are all intralayer.  The reference then rates its
+            // empty cycle (cost_time_ratio_solver.cpp:357-365, :686-697): the
+            // bound is 0/0 = NaN, every Bellman-Ford call at lambda = NaN
+            // stops at layer 1 on the empty cycle (a zero cycle, :574-577),
+            // the branch is pushed and popped as valid (:809-815, :834-838),
+            // and the solve returns (true, NaN, no rows) (:855-862).  That
+            // result is set here without those launches.  It has no cycle
+            // to differentiate.
+            stats.lawlerIters = 0;
+            resPasses = true;
+            resObjective = std::numeric_limits<float>::quiet_NaN();
+            rows_for_edges({});
+            adjKind = 0;
+            adjT = 0;
+            return;
+        }
         if (c.status != BF_UB_DONE)
             throw Failure(PGC_ERR_INTERNAL, "no closed path through the upper-bound start node");
         numNodesInBranch = c.numInBranch;

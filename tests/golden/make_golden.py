@@ -8,10 +8,29 @@ vertex -- the reference's product_space.cpp generation order), the costs are
 round(1e5 / (2 * median) * c) clipped at 1e7 (times 5e4 in mean mode), and
 the optima come from exact enumeration (tests/bruteforce.py).
 
+tests/golden/conj_cases.json holds the same kind of answers for tiny
+conjugate product graphs (conj_product_space.cpp:70-174), plain and with
+intralayer edges pruned, on a given cost/time matrix (the reference's
+set_cost_vector) so that no energy is involved:
+
+* SHA-256 digests of the product space rows and of SRC, TRGT;
+* the exact minimum cost cycle on the raw costs, and on the costs as the
+  ratio solve leaves them (each column rescaled in place);
+* the exact minimum cost/time ratio.  The reference's ratio solver is not
+  exact on these graphs: its Bellman-Ford verdict looks only at the cycle of
+  the best candidate (cost_time_ratio_solver.cpp:443-489), so Lawler can stop
+  above the optimum.  The answer bounds its result from below;
+* the node that the reference's initial-upper-bound rule starts from
+  (cost_time_ratio_solver.cpp:652-707: the layer-1 node with the lowest mean
+  incoming rescaled cost among those with more than 3 in-edges).  With K = 1
+  a 2D-degenerate start node has no usable out-edge (all of them are
+  intralayer), the bound's cycle is empty and its ratio 0/0.
+
 Run:  python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import os
 import sys
@@ -88,6 +107,108 @@ def case(mesh, ny, K, seed):
     }
 
 
+def conj_product(EX, EY, prune):
+    """Conjugate product space in the reference's generation order
+    (conj_product_space.cpp:70-174).  Nodes of layer i: i*3|EX| + j for the
+    non-degenerate node of X edge j, + |EX| + j for its 2D-degenerate node,
+    + |EX| (pruned) or 2|EX| (not pruned) + j for its 3D-degenerate node.
+    Outgoing edges of an X vertex are taken in ascending edge id."""
+    nEX, nEY = len(EX), len(EY)
+    out = {}
+    for j, (a, _) in enumerate(EX):
+        out.setdefault(int(a), []).append(j)
+    deg2 = nEX
+    deg3 = nEX if prune else 2 * nEX
+    rows, src, trgt = [], [], []
+
+    def add(row, s, t):
+        rows.append(row); src.append(s); trgt.append(t)
+
+    for i in range(nEY):
+        nx = (i + 1) % nEY
+        cur, nxt = i * 3 * nEX, nx * 3 * nEX
+        s2, m2, t2 = int(EY[i, 0]), int(EY[i, 1]), int(EY[nx, 1])
+        if not prune:  # intralayer: deg2d -> deg2d, deg2d -> non-deg
+            for j, (s3, m3) in enumerate(EX):
+                for it in sorted(out.get(int(m3), [])):
+                    t3 = int(EX[it, 1])
+                    if t3 == s3:
+                        continue
+                    add((s2, s2, s2, s3, m3, t3), cur + deg2 + j, cur + deg2 + it)
+                    add((s2, s2, m2, s3, m3, t3), cur + deg2 + j, cur + it)
+        for j, (s3, m3) in enumerate(EX):  # interlayer
+            for it in sorted(out.get(int(m3), [])):
+                t3 = int(EX[it, 1])
+                if t3 == s3:
+                    continue
+                add((s2, m2, t2, s3, m3, t3), cur + j, nxt + it)
+                if not prune:
+                    add((s2, m2, m2, s3, m3, t3), cur + j, nxt + deg2 + it)
+                add((s2, m2, t2, m3, m3, t3), cur + deg3 + j, nxt + it)
+            add((s2, m2, t2, s3, m3, m3), cur + j, nxt + deg3 + j)
+            add((s2, m2, t2, m3, m3, m3), cur + deg3 + j, nxt + deg3 + j)
+    return np.array(rows, dtype=np.int32), src, trgt
+
+
+def digest(*arrays):
+    """SHA-256 of the arrays as little-endian int32, one after the other."""
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(np.asarray(a, dtype="<i4")).tobytes())
+    return h.hexdigest()
+
+
+def upper_bound_start(trgt, cost_scaled, n):
+    """The reference's initial-upper-bound start node: the first layer-1 node
+    with the lowest float mean of its incoming costs among nodes with more
+    than 3 in-edges (summed in edge order in float32)."""
+    trgt = np.asarray(trgt)
+    c32 = cost_scaled.astype(np.float32)
+    best, where = np.float32(np.inf), 0
+    for v in range(n):
+        e = np.nonzero(trgt == n + v)[0]
+        if len(e) == 0:
+            continue
+        mean = np.float32(0)
+        for x in e:
+            mean = np.float32(mean + c32[x])
+        mean = np.float32(mean / np.float32(len(e)))
+        if mean < best and len(e) > 3:
+            best, where = mean, v
+    return where
+
+
+def conj_case(mesh, ny, K, seed, prune):
+    VX, und = MESHES[mesh]
+    EX = directed(und)
+    t = np.linspace(0, 2 * np.pi, ny, endpoint=False)
+    VY = np.stack([np.cos(t), np.sin(t), np.zeros(ny)], axis=1)
+    EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
+    rows, src, trgt = conj_product(EX, EY, prune)
+    rng = np.random.default_rng(100 + seed)
+    raw_e4 = rng.integers(1000, 20001, size=(len(rows), 2))
+    raw = raw_e4 / 1e4
+    cost_scaled, time_scaled = rescale(raw[:, 0]), rescale(raw[:, 1])
+    n = 3 * len(EX)
+    lam, (_, opt_ratio) = bruteforce.min_ratio_cycle(src, trgt, cost_scaled, time_scaled, n, ny, K)
+    mc_scaled, (_, opt_cost_scaled) = bruteforce.min_cost_cycle(src, trgt, cost_scaled, n, ny, K)
+    mc_raw, (_, opt_cost_raw) = bruteforce.min_cost_cycle(src, trgt, raw[:, 0], n, ny, K)
+    ub = upper_bound_start(trgt, cost_scaled, n)
+    ub_kind = "nondegenerate" if ub < len(EX) else "degenerate2d" if (ub < 2 * len(EX) and not prune) else "degenerate3d"
+    return {
+        "name": f"conj_{mesh}_ny{ny}_k{K}_s{seed}{'_prune' if prune else ''}", "K": K, "prune": prune,
+        "VX": VX.tolist(), "EX": EX.tolist(), "VY": VY.tolist(), "EY": EY.tolist(),
+        "cost_time_e4": raw_e4.tolist(),
+        "product_rows": len(rows), "rows_digest": digest(rows), "src_trgt_digest": digest(src, trgt),
+        "ratio_optimum": [lam.numerator, lam.denominator],
+        "ratio_upper_bound_start": [int(ub), ub_kind],
+        "min_cost_after_ratio": float(mc_scaled),
+        "min_cost_after_ratio_cycles": [sorted(p) for p in opt_cost_scaled],
+        "min_cost_raw": [Fraction(mc_raw).numerator, Fraction(mc_raw).denominator],
+        "min_cost_raw_cycles": [sorted(p) for p in opt_cost_raw],
+    }
+
+
 def main():
     cases = []
     for mesh in ("tetrahedron", "octahedron"):
@@ -107,6 +228,17 @@ def main():
     with open(os.path.join(HERE, "toy_cases.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": cases}, f, separators=(",", ":"))
     print(f"wrote {len(cases)} cases")
+    conj = []
+    # seed 2 draws costs on which the reference's Lawler stops above the
+    # optimum in most cases, seed 0 costs on which it reaches it
+    for seed in (0, 2):
+        for mesh in ("tetrahedron", "octahedron"):
+            for ny, K in ((3, 1), (4, 1), (4, 2), (4, 3)):  # odd nY with K >= 2: Q1, as above
+                for prune in (False, True):
+                    conj.append(conj_case(mesh, ny, K, seed, prune))
+    with open(os.path.join(HERE, "conj_cases.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": conj}, f, separators=(",", ":"))
+    print(f"wrote {len(conj)} conjugate cases")
 
 
 if __name__ == "__main__":

@@ -1,7 +1,8 @@
-"""The sm_100a solvers against exact known answers (tests/golden/toy_cases.json)."""
+"""The sm_100a solvers against exact known answers (tests/golden/toy_cases.json,
+tests/golden/conj_cases.json)."""
 import pytest
 
-from test_oracle_golden import CASES, check_case
+from test_oracle_golden import CASES, CONJ_CASES, check_case, check_conj_case
 
 pytestmark = pytest.mark.gpu
 
@@ -9,3 +10,8 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
 def test_gpu_matches_known_answers(cpg, c):
     check_case(lambda *a: cpg.product_graph_generator(*a, False, False), c)
+
+
+@pytest.mark.parametrize("c", CONJ_CASES, ids=[c["name"] for c in CONJ_CASES])
+def test_gpu_matches_conjugate_known_answers(cpg, c):
+    check_conj_case(cpg.product_graph_generator, c)

@@ -1,9 +1,11 @@
-"""Pins the CPU oracle against exact known answers (tests/golden/toy_cases.json).
+"""Pins the CPU oracle against exact known answers (tests/golden/toy_cases.json,
+tests/golden/conj_cases.json).
 
 The fixtures come from tests/golden/make_golden.py, which builds the toy
 product graphs, their costs and the rescale from their definitions and finds
 the optima by exact enumeration -- independently of the oracle.
 """
+import hashlib
 import json
 import os
 from fractions import Fraction
@@ -14,6 +16,8 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 with open(os.path.join(HERE, "golden", "toy_cases.json")) as f:
     CASES = json.load(f)["cases"]
+with open(os.path.join(HERE, "golden", "conj_cases.json")) as f:
+    CONJ_CASES = json.load(f)["cases"]
 
 
 def _arrays(c):
@@ -65,3 +69,71 @@ def test_fixture_product_space_matches_oracle(oracle):
     assert np.array_equal(o.get_product_space(), ps)
     s2, t2 = o.get_src_trgt()
     assert np.array_equal(s2, np.array(src)) and np.array_equal(t2, np.array(trgt))
+
+
+def _digest(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(np.asarray(a, dtype="<i4")).tobytes())
+    return h.hexdigest()
+
+
+def conj_generator(make, c):
+    """A conjugate generator on the case's graph with its cost/time matrix set
+    (feature differences and normals are placeholders: no energy is used)."""
+    VX, EX, VY = np.array(c["VX"]), np.array(c["EX"], dtype=np.int32), np.array(c["VY"])
+    EY = np.array(c["EY"], dtype=np.int32)
+    g = make(VX, EX, VY, EY, np.ones((len(VX), len(VY))), True, False, c["prune"])
+    g.set_normals(VX / np.linalg.norm(VX, axis=1, keepdims=True), np.tile([0.0, 0.0, 1.0], (len(VY), 1)))
+    g.set_cost_time_ratio_mode("vanilla", "lengthnormalisation")
+    g.set_cost_vector(np.array(c["cost_time_e4"]) / 1e4)
+    return g
+
+
+def check_conj_case(make, c):
+    """Product space digest, then the bounds the reference's solvers keep on a
+    conjugate graph.  Neither solver is exact there: Lawler stops when the
+    cycle of the best Bellman-Ford candidate is not negative
+    (cost_time_ratio_solver.cpp:443-489), and the minimum-cost branch and
+    bound returns the first branch popped with a valid bound even after a
+    cheaper cycle was found past the first candidate of another branch
+    (dijkstra_solver.cpp:455-461, :361-371).  So each objective is checked
+    against its own cycle and against the exact optimum from below; with
+    K = 1 a 2D-degenerate upper-bound start gives a 0/0 ratio and no cycle."""
+    g = conj_generator(make, c)
+    ps = g.get_product_space()
+    assert ps.shape == (c["product_rows"], 6)
+    assert _digest(ps) == c["rows_digest"]
+    raw = np.array(c["cost_time_e4"]) / 1e4
+
+    passes, obj, m = g.solve_with_cost_time_ratio("lawlercpu", c["K"])
+    assert passes
+    start, kind = c["ratio_upper_bound_start"]
+    scaled = g.get_cost_vector()  # rescaled in place by the ratio solve
+    if c["K"] == 1 and kind == "degenerate2d":
+        assert np.isnan(obj) and m.shape[0] == 0
+    else:
+        e = g.last_cycle_edges()
+        assert m.shape == (len(e), 6) and np.array_equal(m, ps[e])
+        assert obj == pytest.approx(scaled[e, 0].sum() / scaled[e, 1].sum(), rel=1e-6)
+        assert obj >= np.float32(float(Fraction(*c["ratio_optimum"]))) * (1 - 1e-6)
+
+    passes, obj, m = g.solve_with_minimum_cost("dijkstracpu", c["K"])
+    e = g.last_cycle_edges()
+    assert passes and m.shape == (len(e), 6) and np.array_equal(m, ps[e])
+    assert obj == pytest.approx(scaled[e, 0].sum(), rel=1e-6)
+    assert obj >= np.float32(c["min_cost_after_ratio"])
+
+    g2 = conj_generator(make, c)
+    passes, obj, m = g2.solve_with_minimum_cost("dijkstracpu", c["K"])
+    e = g2.last_cycle_edges()
+    assert passes and m.shape == (len(e), 6) and np.array_equal(m, ps[e])
+    assert obj == pytest.approx(raw[e, 0].sum(), rel=1e-6)
+    assert obj >= np.float32(float(Fraction(*c["min_cost_raw"]))) * (1 - 1e-6)
+
+
+@pytest.mark.parametrize("c", CONJ_CASES, ids=[c["name"] for c in CONJ_CASES])
+def test_oracle_matches_conjugate_known_answers(oracle, c):
+    check_conj_case(oracle.OracleGenerator, c)
+    s, t = conj_generator(oracle.OracleGenerator, c).get_src_trgt()
+    assert _digest(s, t) == c["src_trgt_digest"]
