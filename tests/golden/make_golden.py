@@ -8,6 +8,11 @@ vertex -- the reference's product_space.cpp generation order), the costs are
 round(1e5 / (2 * median) * c) clipped at 1e7 (times 5e4 in mean mode), and
 the optima come from exact enumeration (tests/bruteforce.py).
 
+tests/golden/pruned_cases.json holds them for the plain graph with its
+intralayer edges pruned (product_space.cpp:44-52, :122-133), with digests of
+its product space.  There the reference's ratio solver can stop above the
+optimum (see below), so its answer bounds the result from below.
+
 tests/golden/conj_cases.json holds the same kind of answers for tiny
 conjugate product graphs (conj_product_space.cpp:70-174), plain and with
 intralayer edges pruned, on a given cost/time matrix (the reference's
@@ -55,13 +60,14 @@ def directed(undirected):
     return np.array(sorted(both), dtype=np.int32)
 
 
-def plain_product(EX, EY, nvx):
+def plain_product(EX, EY, nvx, prune=False):
     src, trgt, rows = [], [], []
     nEY = EY.shape[0]
     for i in range(nEY):
         nxt = (i + 1) % nEY
         for a, b in EX:
-            rows.append((EY[i, 0], EY[i, 0], a, b)); src.append(i * nvx + a); trgt.append(i * nvx + b)
+            if not prune:
+                rows.append((EY[i, 0], EY[i, 0], a, b)); src.append(i * nvx + a); trgt.append(i * nvx + b)
             rows.append((EY[i, 0], EY[i, 1], a, b)); src.append(i * nvx + a); trgt.append(nxt * nvx + b)
         for x in range(nvx):
             rows.append((EY[i, 0], EY[i, 1], x, x)); src.append(i * nvx + x); trgt.append(nxt * nvx + x)
@@ -79,7 +85,7 @@ def rescale(col):
     return np.minimum(x, 1e7)
 
 
-def case(mesh, ny, K, seed):
+def case(mesh, ny, K, seed, prune=False):
     VX, und = MESHES[mesh]
     EX = directed(und)
     nvx = VX.shape[0]
@@ -88,15 +94,15 @@ def case(mesh, ny, K, seed):
     VY = np.stack([np.cos(t), np.sin(t), np.zeros(ny)], axis=1)
     EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
     fd = rng.uniform(0.1, 2.0, size=(nvx, ny))
-    ps, src, trgt = plain_product(EX, EY, nvx)
+    ps, src, trgt = plain_product(EX, EY, nvx, prune)
     raw = 0.5 * (fd[ps[:, 2], ps[:, 0]] + fd[ps[:, 3], ps[:, 1]])
     cost_scaled = rescale(raw)
     time = np.full_like(cost_scaled, 50000.0)
     lam, (u, opt_ratio) = bruteforce.min_ratio_cycle(src, trgt, cost_scaled, time, nvx, ny, K)
     mc_scaled, (_, opt_cost_scaled) = bruteforce.min_cost_cycle(src, trgt, cost_scaled, nvx, ny, K)
     mc_raw, (_, opt_cost_raw) = bruteforce.min_cost_cycle(src, trgt, raw, nvx, ny, K)
-    return {
-        "name": f"{mesh}_ny{ny}_k{K}_s{seed}", "K": K,
+    out = {
+        "name": f"{mesh}_ny{ny}_k{K}_s{seed}{'_prune' if prune else ''}", "K": K,
         "VX": VX.tolist(), "EX": EX.tolist(), "VY": VY.tolist(), "EY": EY.tolist(), "feat_diff": fd.tolist(),
         "ratio": [lam.numerator, lam.denominator],
         "ratio_cycles": [sorted(p) for p in opt_ratio],
@@ -105,6 +111,9 @@ def case(mesh, ny, K, seed):
         "min_cost_raw": [Fraction(mc_raw).numerator, Fraction(mc_raw).denominator],
         "min_cost_raw_cycles": [sorted(p) for p in opt_cost_raw],
     }
+    if prune:
+        out.update({"prune": True, "rows_digest": digest(ps), "src_trgt_digest": digest(src, trgt)})
+    return out
 
 
 def conj_product(EX, EY, prune):
@@ -236,6 +245,14 @@ def main():
             for ny, K in ((3, 1), (4, 1), (4, 2), (4, 3)):  # odd nY with K >= 2: Q1, as above
                 for prune in (False, True):
                     conj.append(conj_case(mesh, ny, K, seed, prune))
+    pruned = []
+    for mesh in ("tetrahedron", "octahedron"):
+        for ny, K in ((3, 1), (4, 1), (4, 2), (6, 1), (6, 2)):
+            for seed in (0, 1, 2):
+                pruned.append(case(mesh, ny, K, seed, prune=True))
+    with open(os.path.join(HERE, "pruned_cases.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": pruned}, f, separators=(",", ":"))
+    print(f"wrote {len(pruned)} pruned plain cases")
     with open(os.path.join(HERE, "conj_cases.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": conj}, f, separators=(",", ":"))
     print(f"wrote {len(conj)} conjugate cases")

@@ -1,5 +1,5 @@
 """Pins the CPU oracle against exact known answers (tests/golden/toy_cases.json,
-tests/golden/conj_cases.json).
+tests/golden/pruned_cases.json, tests/golden/conj_cases.json).
 
 The fixtures come from tests/golden/make_golden.py, which builds the toy
 product graphs, their costs and the rescale from their definitions and finds
@@ -18,6 +18,8 @@ with open(os.path.join(HERE, "golden", "toy_cases.json")) as f:
     CASES = json.load(f)["cases"]
 with open(os.path.join(HERE, "golden", "conj_cases.json")) as f:
     CONJ_CASES = json.load(f)["cases"]
+with open(os.path.join(HERE, "golden", "pruned_cases.json")) as f:
+    PRUNED_CASES = json.load(f)["cases"]
 
 
 def _arrays(c):
@@ -69,6 +71,44 @@ def test_fixture_product_space_matches_oracle(oracle):
     assert np.array_equal(o.get_product_space(), ps)
     s2, t2 = o.get_src_trgt()
     assert np.array_equal(s2, np.array(src)) and np.array_equal(t2, np.array(trgt))
+
+
+def check_pruned_case(make, c):
+    """Plain graph with pruned intralayer edges: product space digest; the
+    ratio against its own cycle and, from below, against the optimum (the
+    reference's Lawler can stop above it, as on conjugate graphs); the exact
+    minimum cost on the rescaled and on the raw costs."""
+    VX, EX, VY, EY, fd = _arrays(c)
+    g = make(VX, EX, VY, EY, fd, False, False, True)
+    ps = g.get_product_space()
+    assert _digest(ps) == c["rows_digest"]
+    g.set_cost_time_ratio_mode("vanilla", "nomode")
+    passes, obj, m = g.solve_with_cost_time_ratio("lawlercpu", c["K"])
+    assert passes
+    e = g.last_cycle_edges()
+    assert m.shape == (len(e), 4) and np.array_equal(m, ps[e])
+    scaled = g.get_cost_vector()[:, 0]
+    assert obj == pytest.approx(scaled[e].sum() / (50000.0 * len(e)), rel=1e-6)
+    assert obj >= np.float32(float(Fraction(*c["ratio"]))) * (1 - 1e-6)
+
+    passes, obj, m = g.solve_with_minimum_cost("dijkstracpu", c["K"])
+    assert passes
+    assert obj == np.float32(c["min_cost_after_ratio"])
+    assert sorted(g.last_cycle_edges().tolist()) in c["min_cost_after_ratio_cycles"]
+
+    g2 = make(VX, EX, VY, EY, fd, False, False, True)
+    passes, obj, m = g2.solve_with_minimum_cost("dijkstracpu", c["K"])
+    assert passes
+    assert obj == np.float32(float(Fraction(*c["min_cost_raw"])))
+    assert sorted(g2.last_cycle_edges().tolist()) in c["min_cost_raw_cycles"]
+
+
+@pytest.mark.parametrize("c", PRUNED_CASES, ids=[c["name"] for c in PRUNED_CASES])
+def test_oracle_matches_pruned_known_answers(oracle, c):
+    check_pruned_case(oracle.OracleGenerator, c)
+    VX, EX, VY, EY, fd = _arrays(c)
+    s_, t_ = oracle.OracleGenerator(VX, EX, VY, EY, fd, False, False, True).get_src_trgt()
+    assert _digest(s_, t_) == c["src_trgt_digest"]
 
 
 def _digest(*arrays):
