@@ -10,7 +10,8 @@
  *  - Matrices are dense, row-major (C order); indices are 0-based int32.
  *  - Every function returns PGC_OK (0) or a negative PGC_ERR_* code; the
  *    message of the last failure of the calling thread is pgc_last_error().
- *    Nothing calls exit().
+ *    Nothing calls exit().  A null handle, or a null pointer where an array
+ *    is read or written, returns PGC_ERR_ARG.
  *  - A handle is not thread-safe; distinct handles may be used from
  *    distinct threads.  All device work of a handle runs on one CUDA stream
  *    of the device that was current when the handle was created.

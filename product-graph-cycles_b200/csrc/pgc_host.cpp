@@ -1862,6 +1862,7 @@ void pgc_destroy(pgc_graph* g) { delete g; }
 int pgc_set_normals(pgc_graph* h, const double* NX, int64_t rx, int64_t cx, const double* NY, int64_t ry,
                     int64_t cy) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         Graph& g = h->g;
         if (rx != g.nvx || cx != 3)
             throw Failure(PGC_ERR_ARG,
@@ -1869,6 +1870,7 @@ int pgc_set_normals(pgc_graph* h, const double* NX, int64_t rx, int64_t cx, cons
         if (ry != g.nvy || cy != 3)
             throw Failure(PGC_ERR_ARG,
                           "normals for shape Y do not contain as many entries as expected. Assumed shape = |VY| x 3");
+        if (!NX || !NY) throw Failure(PGC_ERR_ARG, "null normals");
         g.NX.assign(NX, NX + 3 * rx);
         g.NY.assign(NY, NY + 3 * ry);
         g.normalsGiven = true;
@@ -1876,11 +1878,15 @@ int pgc_set_normals(pgc_graph* h, const double* NX, int64_t rx, int64_t cx, cons
 }
 
 int pgc_set_max_depth(pgc_graph* h, int k) {
-    return guarded([&] { h->g.maxDepth = k; });
+    return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        h->g.maxDepth = k;
+    });
 }
 
 int pgc_set_cost_time_ratio_mode(pgc_graph* h, const char* cost, const char* time) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         h->g.costName = cost ? cost : "";
         h->g.timeName = time ? time : "";
     });
@@ -1888,6 +1894,7 @@ int pgc_set_cost_time_ratio_mode(pgc_graph* h, const char* cost, const char* tim
 
 int pgc_update_robust_loss_params(pgc_graph* h, double alpha, double c, double pwr) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         Graph& g = h->g;
         if (!g.conj) return;
         if (g.generated) throw Failure(PGC_ERR_STATE, "cannot update robust loss params after model has been generated");
@@ -1899,6 +1906,7 @@ int pgc_update_robust_loss_params(pgc_graph* h, double alpha, double c, double p
 
 int pgc_set_stream(pgc_graph* h, void* cuda_stream) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         Graph& g = h->g;
         PGC_CUDA(cudaStreamSynchronize(g.stream));
         g.stream = cuda_stream ? (cudaStream_t)cuda_stream : g.ownStream;
@@ -1907,6 +1915,7 @@ int pgc_set_stream(pgc_graph* h, void* cuda_stream) {
 
 int pgc_generate(pgc_graph* h) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.generate();
     });
@@ -1914,6 +1923,8 @@ int pgc_generate(pgc_graph* h) {
 
 int pgc_cost_vector_shape(pgc_graph* h, int64_t* rows, int64_t* cols) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!rows || !cols) throw Failure(PGC_ERR_ARG, "null output");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.ensure_generated();
         *rows = (int64_t)h->g.T.nY * h->g.T.eBlock;
@@ -1923,6 +1934,8 @@ int pgc_cost_vector_shape(pgc_graph* h, int64_t* rows, int64_t* cols) {
 
 int pgc_get_cost_vector(pgc_graph* h, double* out) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!out) throw Failure(PGC_ERR_ARG, "null output");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.cost_vector(out);
     });
@@ -1938,6 +1951,8 @@ int pgc_get_cost_vector_noalloc(pgc_graph* h, double* out) {
 
 int pgc_product_space_shape(pgc_graph* h, int64_t* rows, int64_t* cols) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!rows || !cols) throw Failure(PGC_ERR_ARG, "null output");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.ensure_generated();
         *rows = (int64_t)h->g.T.nY * h->g.T.eBlock;
@@ -1947,6 +1962,8 @@ int pgc_product_space_shape(pgc_graph* h, int64_t* rows, int64_t* cols) {
 
 int pgc_get_product_space(pgc_graph* h, int32_t* out) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!out) throw Failure(PGC_ERR_ARG, "null output");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.product_space(out);
     });
@@ -1954,6 +1971,7 @@ int pgc_get_product_space(pgc_graph* h, int32_t* out) {
 
 int pgc_solve_with_cost_time_ratio(pgc_graph* h, const char* solver, int max_depth) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         Graph& g = h->g;
         const std::string name = solver ? solver : "";
         const int K = max_depth >= 1 ? max_depth : g.maxDepth;
@@ -1977,6 +1995,7 @@ int pgc_solve_with_cost_time_ratio(pgc_graph* h, const char* solver, int max_dep
 
 int pgc_solve_with_minimum_cost(pgc_graph* h, const char* solver, int max_depth) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         Graph& g = h->g;
         const std::string name = solver ? solver : "";
         const int K = max_depth >= 1 ? max_depth : g.maxDepth;
@@ -2022,14 +2041,16 @@ int pgc_set_feat_diff(pgc_graph* h, const double* feat_diff, int64_t rows, int64
 
 int pgc_set_team_cap(pgc_graph* h, int max_ctas) {
     return guarded([&] {
-        if (!h || max_ctas < 0) throw Failure(PGC_ERR_ARG, "max_ctas must be >= 0");
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (max_ctas < 0) throw Failure(PGC_ERR_ARG, "max_ctas must be >= 0");
         h->g.teamCap = max_ctas;
     });
 }
 
 int pgc_set_team_shape(pgc_graph* h, int ctas, int threads_per_cta) {
     return guarded([&] {
-        if (!h || ctas < 0) throw Failure(PGC_ERR_ARG, "ctas must be >= 0");
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (ctas < 0) throw Failure(PGC_ERR_ARG, "ctas must be >= 0");
         if (threads_per_cta && (threads_per_cta < 32 || threads_per_cta > pgc::kBfThreads || threads_per_cta % 32 != 0))
             throw Failure(PGC_ERR_ARG, "threads per CTA must be 0 or a multiple of 32 in [32, 640]");
         h->g.shapeBlocks = ctas;
@@ -2088,6 +2109,7 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
 
 int pgc_result(pgc_graph* h, int* passes, float* objective, int64_t* rows, int64_t* cols) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         const Graph& g = h->g;
         if (passes) *passes = g.resPasses ? 1 : 0;
         if (objective) *objective = g.resObjective;
@@ -2098,14 +2120,18 @@ int pgc_result(pgc_graph* h, int* passes, float* objective, int64_t* rows, int64
 
 int pgc_result_matching(pgc_graph* h, int32_t* out) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         const Graph& g = h->g;
-        std::memcpy(out, g.resMatching.data(), sizeof(int32_t) * g.resMatching.size());
+        if (!out && !g.resMatching.empty()) throw Failure(PGC_ERR_ARG, "null output");
+        if (!g.resMatching.empty()) std::memcpy(out, g.resMatching.data(), sizeof(int32_t) * g.resMatching.size());
     });
 }
 
 int pgc_result_cycle_edges(pgc_graph* h, int64_t* out, int64_t capacity, int64_t* count) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         const Graph& g = h->g;
+        if (!count || (!out && capacity > 0)) throw Failure(PGC_ERR_ARG, "null output");
         *count = (int64_t)g.resEdges.size();
         for (int64_t i = 0; i < *count && i < capacity; ++i) out[i] = g.resEdges[(size_t)i];
     });
@@ -2113,6 +2139,7 @@ int pgc_result_cycle_edges(pgc_graph* h, int64_t* out, int64_t capacity, int64_t
 
 int pgc_result_profile(pgc_graph* h, int64_t* out8) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         if (!out8) throw pgc::Failure(PGC_ERR_ARG, "null output");
         const pgc::Stats& s = h->g.stats;
         out8[0] = (int64_t)s.cycA;
@@ -2128,6 +2155,7 @@ int pgc_result_profile(pgc_graph* h, int64_t* out8) {
 
 int pgc_result_profile_detail(pgc_graph* h, int64_t* out4) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
         if (!out4) throw pgc::Failure(PGC_ERR_ARG, "null output");
         const pgc::Stats& s = h->g.stats;
         out4[0] = (int64_t)s.cycStage;
@@ -2139,6 +2167,8 @@ int pgc_result_profile_detail(pgc_graph* h, int64_t* out4) {
 
 int pgc_result_stats(pgc_graph* h, int64_t* out8) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!out8) throw Failure(PGC_ERR_ARG, "null output");
         const pgc::Stats& s = h->g.stats;
         out8[0] = s.bfCalls;
         out8[1] = s.sweeps;
@@ -2178,6 +2208,7 @@ int pgc_product_graph_sizes(const int32_t* EX, int64_t nex, int64_t nvx, int64_t
 
 int pgc_compute_normals_2d(const double* Vin, int64_t nv, const int32_t* E, int64_t ne, double* out) {
     return guarded([&] {
+        if (nv < 0 || (nv > 0 && (!Vin || !E || !out))) throw Failure(PGC_ERR_ARG, "null argument");
         if (nv != ne) throw Failure(PGC_ERR_ARG, "V.rows() != E.rows()");
         std::vector<double> V(Vin, Vin + 3 * nv);
         int zero = -1;
@@ -2235,6 +2266,7 @@ int pgc_compute_normals_2d(const double* Vin, int64_t nv, const int32_t* E, int6
 // normals weighted by twice their area, i.e. of their edge cross products.
 int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_t nf, double* out) {
     return guarded([&] {
+        if (nv < 0 || nf < 0 || (nv > 0 && (!V || !out)) || (nf > 0 && !F)) throw Failure(PGC_ERR_ARG, "null argument");
         for (int64_t i = 0; i < 3 * nv; ++i) out[i] = 0.0;
         for (int64_t f = 0; f < nf; ++f) {
             const int a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
@@ -2263,6 +2295,8 @@ int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_
 
 int pgc_graph_info(pgc_graph* h, int64_t* out8) {
     return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!out8) throw Failure(PGC_ERR_ARG, "null output");
         Graph& g = h->g;
         PGC_CUDA(cudaSetDevice(g.device));
         g.ensure_generated();
