@@ -177,3 +177,33 @@ def test_oracle_matches_conjugate_known_answers(oracle, c):
     check_conj_case(oracle.OracleGenerator, c)
     s, t = conj_generator(oracle.OracleGenerator, c).get_src_trgt()
     assert _digest(s, t) == c["src_trgt_digest"]
+
+
+@pytest.mark.parametrize("ny", [2, 3, 5])
+@pytest.mark.parametrize("kind", ["plain", "plain_pruned", "conj", "conj_pruned"])
+@pytest.mark.parametrize("mesh", ["tetrahedron", "octahedron"])
+def test_fixture_generators_match_oracle_product_spaces(oracle, mesh, kind, ny):
+    """The fixture script's product spaces (restated from product_space.cpp
+    and conj_product_space.cpp) equal the oracle's, rows and SRC/TRGT, also
+    for layer counts the fixtures do not hold (two layers included)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden
+
+    VX, und = make_golden.MESHES[mesh]
+    EX = make_golden.directed(und)
+    t = np.linspace(0, 2 * np.pi, ny, endpoint=False)
+    VY = np.stack([np.cos(t), np.sin(t), np.zeros(ny)], axis=1)
+    EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
+    conj, prune = kind.startswith("conj"), kind.endswith("pruned")
+    if conj:
+        ps, src, trgt = make_golden.conj_product(EX, EY, prune)
+    else:
+        ps, src, trgt = make_golden.plain_product(EX, EY, len(VX), prune)
+    o = oracle.OracleGenerator(VX, EX, VY, EY, np.ones((len(VX), ny)), conj, False, prune)
+    if conj:
+        o.set_normals(VX / np.linalg.norm(VX, axis=1, keepdims=True), np.tile([0.0, 0.0, 1.0], (ny, 1)))
+    assert np.array_equal(o.get_product_space(), ps)
+    s_, t_ = o.get_src_trgt()
+    assert np.array_equal(s_, np.array(src)) and np.array_equal(t_, np.array(trgt))
