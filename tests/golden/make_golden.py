@@ -8,6 +8,10 @@ vertex -- the reference's product_space.cpp generation order), the costs are
 round(1e5 / (2 * median) * c) clipped at 1e7 (times 5e4 in mean mode), and
 the optima come from exact enumeration (tests/bruteforce.py).
 
+tests/golden/mesh_cases.json holds them for plain graphs on icospheres of
+12 and 42 vertices.  There the reference's ratio solver can stop above the
+optimum with K >= 2 (see below), so its answer bounds the result from below.
+
 tests/golden/pruned_cases.json holds them for the plain graph with its
 intralayer edges pruned (product_space.cpp:44-52, :122-133), with digests of
 its product space.  There the reference's ratio solver can stop above the
@@ -55,6 +59,38 @@ MESHES = {
 }
 
 
+def icosphere(level):
+    """Vertices and undirected edges of an icosahedron subdivided `level`
+    times, new vertices at the edge midpoints pushed onto the unit sphere."""
+    g = (1 + 5 ** 0.5) / 2
+    V = [(-1, g, 0), (1, g, 0), (-1, -g, 0), (1, -g, 0), (0, -1, g), (0, 1, g), (0, -1, -g), (0, 1, -g),
+         (g, 0, -1), (g, 0, 1), (-g, 0, -1), (-g, 0, 1)]
+    V = [tuple(np.array(v) / np.linalg.norm(v)) for v in V]
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        mid, nf = {}, []
+
+        def m(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                x = (np.array(V[a]) + np.array(V[b])) / 2
+                V.append(tuple(x / np.linalg.norm(x)))
+                mid[key] = len(V) - 1
+            return mid[key]
+
+        for a, b, c in F:
+            ab, bc, ca = m(a, b), m(b, c), m(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        F = nf
+    und = sorted({(min(a, b), max(a, b)) for f in F for a, b in ((f[0], f[1]), (f[1], f[2]), (f[2], f[0]))})
+    return np.array(V, dtype=np.float64), und
+
+
+ICOSPHERES = {f"icosphere{level}": icosphere(level) for level in (0, 1)}
+
+
 def directed(undirected):
     both = [(a, b) for a, b in undirected] + [(b, a) for a, b in undirected]
     return np.array(sorted(both), dtype=np.int32)
@@ -85,8 +121,8 @@ def rescale(col):
     return np.minimum(x, 1e7)
 
 
-def case(mesh, ny, K, seed, prune=False):
-    VX, und = MESHES[mesh]
+def case(mesh, ny, K, seed, prune=False, digests=False):
+    VX, und = MESHES[mesh] if mesh in MESHES else ICOSPHERES[mesh]
     EX = directed(und)
     nvx = VX.shape[0]
     rng = np.random.default_rng(seed)
@@ -112,7 +148,9 @@ def case(mesh, ny, K, seed, prune=False):
         "min_cost_raw_cycles": [sorted(p) for p in opt_cost_raw],
     }
     if prune:
-        out.update({"prune": True, "rows_digest": digest(ps), "src_trgt_digest": digest(src, trgt)})
+        out["prune"] = True
+    if prune or digests:
+        out.update({"rows_digest": digest(ps), "src_trgt_digest": digest(src, trgt)})
     return out
 
 
@@ -250,6 +288,14 @@ def main():
         for ny, K in ((3, 1), (4, 1), (4, 2), (6, 1), (6, 2)):
             for seed in (0, 1, 2):
                 pruned.append(case(mesh, ny, K, seed, prune=True))
+    irregular = []
+    for mesh, seeds in (("icosphere0", (0, 1, 2, 3)), ("icosphere1", (0, 1))):
+        for ny, K in ((4, 1), (4, 2), (6, 2), (4, 3)):
+            for seed in seeds:
+                irregular.append(case(mesh, ny, K, seed, digests=True))
+    with open(os.path.join(HERE, "mesh_cases.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": irregular}, f, separators=(",", ":"))
+    print(f"wrote {len(irregular)} icosphere cases")
     with open(os.path.join(HERE, "pruned_cases.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": pruned}, f, separators=(",", ":"))
     print(f"wrote {len(pruned)} pruned plain cases")

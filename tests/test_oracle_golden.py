@@ -1,5 +1,6 @@
 """Pins the CPU oracle against exact known answers (tests/golden/toy_cases.json,
-tests/golden/pruned_cases.json, tests/golden/conj_cases.json).
+tests/golden/mesh_cases.json, tests/golden/pruned_cases.json,
+tests/golden/conj_cases.json).
 
 The fixtures come from tests/golden/make_golden.py, which builds the toy
 product graphs, their costs and the rescale from their definitions and finds
@@ -20,6 +21,8 @@ with open(os.path.join(HERE, "golden", "conj_cases.json")) as f:
     CONJ_CASES = json.load(f)["cases"]
 with open(os.path.join(HERE, "golden", "pruned_cases.json")) as f:
     PRUNED_CASES = json.load(f)["cases"]
+with open(os.path.join(HERE, "golden", "mesh_cases.json")) as f:
+    MESH_CASES = json.load(f)["cases"]
 
 
 def _arrays(c):
@@ -73,13 +76,14 @@ def test_fixture_product_space_matches_oracle(oracle):
     assert np.array_equal(s2, np.array(src)) and np.array_equal(t2, np.array(trgt))
 
 
-def check_pruned_case(make, c):
-    """Plain graph with pruned intralayer edges: product space digest; the
+def check_bounded_plain_case(make, c):
+    """Plain graph (pruned or on an icosphere): product space digest; the
     ratio against its own cycle and, from below, against the optimum (the
-    reference's Lawler can stop above it, as on conjugate graphs); the exact
-    minimum cost on the rescaled and on the raw costs."""
+    reference's Lawler can stop above it); the exact minimum cost on the
+    rescaled and on the raw costs."""
     VX, EX, VY, EY, fd = _arrays(c)
-    g = make(VX, EX, VY, EY, fd, False, False, True)
+    prune = c.get("prune", False)
+    g = make(VX, EX, VY, EY, fd, False, False, prune)
     ps = g.get_product_space()
     assert _digest(ps) == c["rows_digest"]
     g.set_cost_time_ratio_mode("vanilla", "nomode")
@@ -96,18 +100,21 @@ def check_pruned_case(make, c):
     assert obj == np.float32(c["min_cost_after_ratio"])
     assert sorted(g.last_cycle_edges().tolist()) in c["min_cost_after_ratio_cycles"]
 
-    g2 = make(VX, EX, VY, EY, fd, False, False, True)
+    g2 = make(VX, EX, VY, EY, fd, False, False, prune)
     passes, obj, m = g2.solve_with_minimum_cost("dijkstracpu", c["K"])
     assert passes
     assert obj == np.float32(float(Fraction(*c["min_cost_raw"])))
     assert sorted(g2.last_cycle_edges().tolist()) in c["min_cost_raw_cycles"]
 
 
-@pytest.mark.parametrize("c", PRUNED_CASES, ids=[c["name"] for c in PRUNED_CASES])
-def test_oracle_matches_pruned_known_answers(oracle, c):
-    check_pruned_case(oracle.OracleGenerator, c)
+BOUNDED_PLAIN_CASES = MESH_CASES + PRUNED_CASES
+
+
+@pytest.mark.parametrize("c", BOUNDED_PLAIN_CASES, ids=[c["name"] for c in BOUNDED_PLAIN_CASES])
+def test_oracle_matches_bounded_plain_known_answers(oracle, c):
+    check_bounded_plain_case(oracle.OracleGenerator, c)
     VX, EX, VY, EY, fd = _arrays(c)
-    s_, t_ = oracle.OracleGenerator(VX, EX, VY, EY, fd, False, False, True).get_src_trgt()
+    s_, t_ = oracle.OracleGenerator(VX, EX, VY, EY, fd, False, False, c.get("prune", False)).get_src_trgt()
     assert _digest(s_, t_) == c["src_trgt_digest"]
 
 
