@@ -2,7 +2,8 @@
 // list: every template edge sits exactly once in its target node's list of
 // the right part (interlayer when its target is in the next layer), with its
 // source node; every node's entries form a prefix of its slots, in ascending
-// edge id (the relaxation's tie order); padding slots hold -1 in both arrays.
+// edge id (the relaxation's tie order); padding slots hold -1 in both arrays;
+// the closing layer's source list follows the reference's dummy-edge rule.
 // Usage: ell EX.bin EY.bin nVX conj prune
 #include "graph_template.hpp"
 
@@ -73,6 +74,21 @@ int main(int argc, char** argv) {
     }
     for (long long t = 0; t < T.eBlock; ++t)
         if (seen[(size_t)t] != 1) fail("edge listed a number of times other than once", t, seen[(size_t)t]);
+    // The closing layer's sources: an interlayer edge of block nY-1 reaches
+    // the closing layer only when its global source id (nY-1)*n + src is
+    // strictly greater than n (cost_time_ratio_solver.cpp:56).  The list is
+    // stored only where that drops something, i.e. with two layers.
+    if (T.nY == 2) {
+        if (T.srcDummy.size() != T.src[INTER].size()) fail("closing-layer list size", (long long)T.srcDummy.size(), 0);
+        else
+            for (size_t at = 0; at < T.srcDummy.size(); ++at) {
+                const int sv = T.src[INTER][at];
+                const int want = sv >= 0 && (long long)(T.nY - 1) * T.n + sv > T.n ? sv : -1;
+                if (T.srcDummy[at] != want) fail("closing-layer source", (long long)at, T.srcDummy[at]);
+            }
+    } else if (!T.srcDummy.empty()) {
+        fail("closing-layer list stored although nothing is dropped", T.nY, (long long)T.srcDummy.size());
+    }
     std::printf("%lld problems (%lld template edges, %d slices)\n", bad, (long long)T.eBlock, T.nslices);
     return bad ? 1 : 0;
 }
