@@ -214,3 +214,53 @@ def test_fixture_generators_match_oracle_product_spaces(oracle, mesh, kind, ny):
     assert np.array_equal(o.get_product_space(), ps)
     s_, t_ = o.get_src_trgt()
     assert np.array_equal(s_, np.array(src)) and np.array_equal(t_, np.array(trgt))
+
+
+def _plain_energy(VX, VY, fd, ps, reg, cost, time):
+    """deformationEnergy.cpp:11-78 restated in numpy, in its operation order:
+    L = sqrt of the squared coordinate differences summed per axis, the Y
+    one before the X one (1 without the regulariser unless the mode needs
+    it); one column 0.5 * (fd0 + fd1) * L, or for ("feature",
+    "lengthnormalisation") the two columns fd0 + fd1 and L."""
+    y0, y1, x0, x1 = ps[:, 0], ps[:, 1], ps[:, 2], ps[:, 3]
+    two = cost == "feature" and time == "lengthnormalisation"
+    if reg or two:
+        L = np.zeros(len(ps))
+        for j in range(3):
+            dy = VY[y0, j] - VY[y1, j]
+            dx = VX[x0, j] - VX[x1, j]
+            L = L + dy * dy
+            L = L + dx * dx
+        L = np.sqrt(L)
+    else:
+        L = np.ones(len(ps))
+    f = fd[x0, y0] + fd[x1, y1]
+    return np.stack([f, L], axis=1) if two else ((0.5 * f) * L)[:, None]
+
+
+@pytest.mark.parametrize("prune", [False, True])
+@pytest.mark.parametrize("reg", [False, True])
+@pytest.mark.parametrize("cost,time", [("vanilla", "nomode"), ("feature", "lengthnormalisation"),
+                                       ("vanilla", "lengthnormalisation"), ("feature", "")])
+def test_oracle_plain_energy_matches_the_restatement(oracle, cost, time, reg, prune):
+    """The oracle's plain-graph costs equal deformationEnergy.cpp restated
+    here, bit for bit, on a perturbed octahedron."""
+    rng = np.random.default_rng(7)
+    V, und = MESHES_FOR_ENERGY
+    VX = V * (1 + 0.2 * rng.random((len(V), 1)))
+    EX = np.array(sorted([(a, b) for a, b in und] + [(b, a) for a, b in und]), dtype=np.int32)
+    ny = 5
+    t = np.linspace(0, 2 * np.pi, ny, endpoint=False)
+    VY = np.stack([np.cos(t), np.sin(t), 0.3 * rng.random(ny)], axis=1)
+    EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
+    fd = rng.uniform(0.1, 2.0, size=(len(VX), ny))
+    o = oracle.OracleGenerator(VX, EX, VY, EY, fd, False, reg, prune)
+    o.set_cost_time_ratio_mode(cost, time)
+    got = o.get_cost_vector()
+    want = _plain_energy(VX, VY, fd, o.get_product_space(), reg, cost, time)
+    assert got.shape == want.shape
+    assert np.array_equal(got, want)
+
+
+MESHES_FOR_ENERGY = (np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], dtype=np.float64),
+                     [(0, 2), (0, 3), (0, 4), (0, 5), (1, 2), (1, 3), (1, 4), (1, 5), (2, 4), (2, 5), (3, 4), (3, 5)])
