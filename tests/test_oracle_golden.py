@@ -8,6 +8,7 @@ the optima by exact enumeration -- independently of the oracle.
 """
 import hashlib
 import json
+import math
 import os
 from fractions import Fraction
 
@@ -264,3 +265,82 @@ def test_oracle_plain_energy_matches_the_restatement(oracle, cost, time, reg, pr
 
 MESHES_FOR_ENERGY = (np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], dtype=np.float64),
                      [(0, 2), (0, 3), (0, 4), (0, 5), (1, 2), (1, 3), (1, 4), (1, 5), (2, 4), (2, 5), (3, 4), (3, 5)])
+
+
+def _mode(name):
+    """stringToMode (higherOrderDeformationEnergy.cpp:396-412), with its
+    missing `== 0`: "penalisedegenerate" maps to vanilla and every unknown
+    name to penalise-degenerate."""
+    known = {"nomode": "nomode", "vanilla": "vanilla", "feature": "feature", "lengthnormalisation": "length",
+             "plainso3": "so3plain", "robustso3": "so3robust"}
+    if name in known:
+        return known[name]
+    return "vanilla" if name == "penalisedegenerate" else "penalise"
+
+
+def _robust(x, alpha=0.7, c=0.6, pwr=4.0):
+    """robustSO3Dif (higherOrderDeformationEnergy.cpp:55-63), same operations."""
+    a2 = abs(alpha - 2)
+    return a2 / alpha * (math.pow(math.pow(x / c, pwr) / a2 + 1, 0.5 * alpha) - 1)
+
+
+def _conj_energy_without_so3(VX, VY, fd, ps, cost, time):
+    """higherOrderDeformationEnergy.cpp:209-339 without the regulariser (the
+    SO(3) distance is 0, and so is its robust loss).  The column-1 writes of
+    the one-column modes fall outside the matrix in the reference; they are
+    left out."""
+    cm, tm = _mode(cost), _mode(time)
+    y0, y1, y2, x0, x1, x2 = (ps[:, i] for i in range(6))
+    f = fd[x2, y2]
+    L = np.zeros(len(ps))
+    for j in range(3):
+        dy = VY[y0, j] - VY[y1, j]
+        dx = VX[x0, j] - VX[x1, j]
+        L = L + dy * dy
+        L = L + dx * dx
+    L = np.sqrt(L)
+    so3 = _robust(0.0)
+    deg = np.where((y2 == y1) | (x2 == x1), 0.1, 1.0)
+    two_pi = 2 * math.pi
+    maxso3 = float(np.float32(_robust(two_pi)))
+    maxfd = float(np.float32(fd.max()))
+    table = {
+        ("vanilla", "vanilla"): [so3 + f],
+        ("vanilla", "length"): [so3 + f, L],
+        ("length", "vanilla"): [L],
+        ("vanilla", "penalise"): [so3 + f, deg],
+        ("penalise", "vanilla"): [deg],
+        ("feature", "so3plain"): [f, np.maximum(0.0, two_pi - 0.0) + 0 * f],
+        ("feature", "so3robust"): [f, np.maximum(0.0, maxso3 - so3) + 0 * f],
+        ("so3robust", "feature"): [so3 + 0 * f, np.maximum(0.0, maxfd - f)],
+        ("so3plain", "feature"): [0.0 * f, np.maximum(0.0, maxfd - f)],
+    }
+    return np.stack(table[(cm, tm)], axis=1)
+
+
+@pytest.mark.parametrize("prune", [False, True])
+@pytest.mark.parametrize("cost,time", [("vanilla", "vanilla"), ("vanilla", "lengthnormalisation"),
+                                       ("lengthnormalisation", "vanilla"), ("vanilla", ""),
+                                       ("", "vanilla"), ("penalisedegenerate", "vanilla"),
+                                       ("feature", "plainso3"), ("feature", "robustso3"),
+                                       ("robustso3", "feature"), ("plainso3", "feature")])
+def test_oracle_conjugate_energy_matches_the_restatement(oracle, cost, time, prune):
+    """The oracle's conjugate-graph costs without the regulariser equal
+    higherOrderDeformationEnergy.cpp restated here, bit for bit, on a
+    perturbed octahedron."""
+    rng = np.random.default_rng(11)
+    V, und = MESHES_FOR_ENERGY
+    VX = V * (1 + 0.2 * rng.random((len(V), 1)))
+    EX = np.array(sorted([(a, b) for a, b in und] + [(b, a) for a, b in und]), dtype=np.int32)
+    ny = 5
+    t = np.linspace(0, 2 * np.pi, ny, endpoint=False)
+    VY = np.stack([np.cos(t), np.sin(t), 0.3 * rng.random(ny)], axis=1)
+    EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
+    fd = rng.uniform(0.1, 2.0, size=(len(VX), ny))
+    o = oracle.OracleGenerator(VX, EX, VY, EY, fd, True, False, prune)
+    o.set_normals(VX / np.linalg.norm(VX, axis=1, keepdims=True), np.tile([0.0, 0.0, 1.0], (ny, 1)))
+    o.set_cost_time_ratio_mode(cost, time)
+    got = o.get_cost_vector()
+    want = _conj_energy_without_so3(VX, VY, fd, o.get_product_space(), cost, time)
+    assert got.shape == want.shape
+    assert np.array_equal(got, want)
