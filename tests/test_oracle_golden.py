@@ -344,3 +344,103 @@ def test_oracle_conjugate_energy_matches_the_restatement(oracle, cost, time, pru
     want = _conj_energy_without_so3(VX, VY, fd, o.get_product_space(), cost, time)
     assert got.shape == want.shape
     assert np.array_equal(got, want)
+
+
+def _rotation_quaternion(R):
+    """Unit quaternion (w, x, y, z) of a rotation matrix, from whichever of
+    the trace and the diagonal entries is largest (sign is irrelevant here)."""
+    t = np.trace(R)
+    if t > max(R[0, 0], R[1, 1], R[2, 2]):
+        w = math.sqrt(1 + t) / 2
+        return np.array([w, (R[2, 1] - R[1, 2]) / (4 * w), (R[0, 2] - R[2, 0]) / (4 * w), (R[1, 0] - R[0, 1]) / (4 * w)])
+    i = int(np.argmax(np.diag(R)))
+    j, k = (i + 1) % 3, (i + 2) % 3
+    s = math.sqrt(1 + R[i, i] - R[j, j] - R[k, k]) * 2
+    q = np.empty(4)
+    q[0] = (R[k, j] - R[j, k]) / s
+    q[1 + i] = s / 4
+    q[1 + j] = (R[j, i] + R[i, j]) / s
+    q[1 + k] = (R[k, i] + R[i, k]) / s
+    return q
+
+
+def _node_quaternions(VX, EX, NX, VY, EY, NY, prune):
+    """precomputeAllQuaternionds with the MATLAB convention
+    (higherOrderDeformationEnergy.cpp:95-134) and precomputeRotation
+    (:16-53): one rotation per product node, aligning the curve frame [n, e,
+    e x n] of its Y edge (the previous one for a 2D-degenerate node) with the
+    mesh frame of its X edge (normal: mean of the endpoint normals), taken
+    as U diag(1, 1, det(U V^T)) V^T from the SVD of X^T Y (numpy's LAPACK
+    SVD here)."""
+    nEX, nEY = len(EX), len(EY)
+    eX = VX[EX[:, 1]] - VX[EX[:, 0]]
+    eY = VY[EY[:, 1]] - VY[EY[:, 0]]
+    unit = lambda v: v / np.linalg.norm(v)
+    out = []
+    for i in range(nEY):
+        for j in range(3 * nEX):
+            jj = j % nEX
+            iy = (i + nEY - 1) % nEY if (nEX <= j < 2 * nEX and not prune) else i
+            e2, n2 = eY[iy], NY[EY[iy, 0]]
+            e3, n3 = eX[jj], (NX[EX[jj, 0]] + NX[EX[jj, 1]]) / 2
+            X = np.stack([unit(n2), unit(e2), unit(np.cross(e2, n2))])
+            Y = np.stack([unit(n3), unit(e3), unit(np.cross(e3, n3))])
+            U, _, Vt = np.linalg.svd(X.T @ Y)
+            d = np.linalg.det(U @ Vt)
+            out.append(_rotation_quaternion(U @ np.diag([1.0, 1.0, d]) @ Vt))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("prune", [False, True])
+@pytest.mark.parametrize("cost,time", [("vanilla", "vanilla"), ("vanilla", "lengthnormalisation"),
+                                       ("vanilla", ""), ("feature", "plainso3"), ("feature", "robustso3"),
+                                       ("robustso3", "feature"), ("plainso3", "feature")])
+def test_oracle_so3_energy_matches_the_restatement(oracle, cost, time, prune):
+    """The oracle's conjugate-graph costs with the regulariser (the SO(3)
+    distance 2 acos|q0 . q1| between the rotations of an edge's two nodes)
+    against the restatement above, within 1e-9: the oracle takes its SVD by
+    one-sided Jacobi rotations, numpy by LAPACK."""
+    rng = np.random.default_rng(13)
+    V, und = MESHES_FOR_ENERGY
+    VX = V * (1 + 0.2 * rng.random((len(V), 1)))
+    EX = np.array(sorted([(a, b) for a, b in und] + [(b, a) for a, b in und]), dtype=np.int32)
+    NX = VX / np.linalg.norm(VX, axis=1, keepdims=True)
+    ny = 5
+    t = np.linspace(0, 2 * np.pi, ny, endpoint=False)
+    VY = np.stack([np.cos(t), np.sin(t), 0.3 * rng.random(ny)], axis=1)
+    EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
+    NY = np.tile([0.0, 0.0, 1.0], (ny, 1))
+    fd = rng.uniform(0.1, 2.0, size=(len(VX), ny))
+    o = oracle.OracleGenerator(VX, EX, VY, EY, fd, True, True, prune)
+    o.set_normals(NX, NY)
+    o.set_cost_time_ratio_mode(cost, time)
+    got = o.get_cost_vector()
+    ps = o.get_product_space()
+    src, trgt = o.get_src_trgt()
+    q = _node_quaternions(VX, EX, NX, VY, EY, NY, prune)
+    dot = np.minimum(np.abs(np.sum(q[src] * q[trgt], axis=1)), 1.0)
+    dist = 2 * np.arccos(dot)
+    robust = np.array([_robust(x) for x in dist])
+    f = fd[ps[:, 5], ps[:, 2]]
+    L = np.zeros(len(ps))
+    for j in range(3):
+        dy = VY[ps[:, 0], j] - VY[ps[:, 1], j]
+        dx = VX[ps[:, 3], j] - VX[ps[:, 4], j]
+        L = L + dy * dy + dx * dx
+    L = np.sqrt(L)
+    deg = np.where((ps[:, 2] == ps[:, 1]) | (ps[:, 5] == ps[:, 4]), 0.1, 1.0)
+    maxso3 = float(np.float32(_robust(2 * math.pi)))
+    maxfd = float(np.float32(fd.max()))
+    want = {
+        ("vanilla", "vanilla"): [robust + f],
+        ("vanilla", "lengthnormalisation"): [robust + f, L],
+        ("vanilla", ""): [robust + f, deg],
+        ("feature", "plainso3"): [f, np.maximum(0.0, 2 * math.pi - dist)],
+        ("feature", "robustso3"): [f, np.maximum(0.0, maxso3 - robust)],
+        ("robustso3", "feature"): [robust, np.maximum(0.0, maxfd - f)],
+        ("plainso3", "feature"): [dist, np.maximum(0.0, maxfd - f)],
+    }[(cost, time)]
+    want = np.stack(want, axis=1)
+    assert got.shape == want.shape
+    np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-9)
+    assert dist.max() > 0.1  # the frames do differ
