@@ -444,3 +444,53 @@ def test_oracle_so3_energy_matches_the_restatement(oracle, cost, time, prune):
     assert got.shape == want.shape
     np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-9)
     assert dist.max() > 0.1  # the frames do differ
+
+
+@pytest.mark.parametrize("ny", [4, 5])
+@pytest.mark.parametrize("column", ["halves", "tiny", "outliers", "random"])
+def test_oracle_rescale_matches_the_restatement(oracle, column, ny):
+    """The ratio solve's in-place rescale (cost_time_ratio_solver.cpp:709-721,
+    utils.hpp:196-209) against tests/golden/make_golden.py's restatement, bit
+    for bit, per column: halves that round away from zero (numpy's rounding
+    would take them to even), a median below 0.001, outliers clipped at 1e7,
+    and column lengths of both parities."""
+    import sys
+
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden
+
+    if ny == 5:  # a square pyramid: 5 vertices, 8 edges, 37 rows per layer, an odd count
+        V = np.array([[1, 1, 0], [-1, 1, 0], [-1, -1, 0], [1, -1, 0], [0, 0, 1]], dtype=np.float64)
+        und = [(0, 1), (1, 2), (2, 3), (0, 3), (0, 4), (1, 4), (2, 4), (3, 4)]
+    else:
+        V, und = MESHES_FOR_ENERGY
+    EX = np.array(sorted([(a, b) for a, b in und] + [(b, a) for a, b in und]), dtype=np.int32)
+    t = np.linspace(0, 2 * np.pi, ny, endpoint=False)
+    VY = np.stack([np.cos(t), np.sin(t), np.zeros(ny)], axis=1)
+    EY = np.stack([np.arange(ny), (np.arange(ny) + 1) % ny], axis=1).astype(np.int32)
+    o = oracle.OracleGenerator(V, EX, VY, EY, np.ones((len(V), ny)), False, False)
+    rows = o.product_space_rows()
+    assert rows % 2 == (ny % 2)
+    rng = np.random.default_rng(ny)
+    if column == "halves":  # median 5e4 makes the scale factor exactly 1
+        c = np.full(rows, 5e4)
+        c[: rows // 3] = rng.integers(1, 1000, rows // 3) + 0.5
+    elif column == "tiny":
+        c = rng.uniform(1e-6, 1e-5, rows)
+    elif column == "outliers":
+        c = rng.uniform(1.0, 2.0, rows)
+        c[::7] *= 1e4
+    else:
+        c = rng.uniform(0.1, 2.0, rows)
+    E = np.stack([c, rng.uniform(0.5, 1.5, rows)], axis=1)
+    o.set_cost_vector(E)
+    o.solve_with_cost_time_ratio("lawlercpu", 2)
+    got = o.get_cost_vector()
+    want = np.stack([make_golden.rescale(E[:, 0]), make_golden.rescale(E[:, 1])], axis=1)
+    assert np.array_equal(got, want)
+    if column == "halves":
+        assert not np.array_equal(want[:, 0], np.minimum(np.round(E[:, 0]), 1e7))
+    if column == "outliers":
+        assert (want[:, 0] == 1e7).any()
+    if column == "tiny":
+        assert float(np.median(c)) < 0.001
