@@ -304,7 +304,7 @@ static ProductGraph conj_product_graph(const IMat& EX, const IMat& EY, bool prun
     g.ps.rows = (i64)g.src.size();
     g.ps.cols = 6;
     g.ps.v = std::move(rows);
-    // conj_product_space.cpp:222-270
+    // conj_product_space.cpp:177-225
     std::vector<std::set<long>> bg((size_t)n);
     for (int j = 0; j < nEX; ++j) {
         bg[j].insert(j + nEX);

@@ -1415,8 +1415,10 @@ void Graph::solve_min_cost(int K) {
     const long long nn = numNodes();
 
     // branch graph: the reference's branchGraph when it exists (conjugate
-    // graph, or plain graph with pruning), else the in-edge sets of layer 0.
-    // Entries are used as edge ids (SRCIds(e)), exactly as the reference does.
+    // graph, conj_product_space.cpp:177-225; plain graph with pruning,
+    // product_space.cpp:122-131), else the in-edge sets of layer 0
+    // (dijkstra_solver.cpp:93-94).  Entries are used as edge ids
+    // (SRCIds(e)), exactly as the reference does (dijkstra_solver.cpp:137-139).
     std::vector<std::vector<long>> bg;
     const bool haveBranchGraph = conj || prune;
     if (haveBranchGraph) {
