@@ -1,23 +1,34 @@
 """Benchmark of the cycle-search hot path on B200.
 
-Workload (default): one shape pair on the GPU -- a perturbed genus-0 mesh X
-with 5,000 vertices (both orientations of its ~30k edges) and normals, a
-200-point closed silhouette curve Y with in-plane normals, 64-d float32
-features -> feat_diff; conjugate product graph, k = 3, cost/time mode
-("vanilla", "lengthnormalisation") [cost = feature difference, time = edge
-length].  Inputs are seeded synthetic data of that shape (no dataset).
+The default run measures the whole metric ("ratio-cycle solves/s + fwd/bwd
+pairs/s, 1 B200, vs plain GPU Lawler; BF HBM GB/s") and prints ONE JSON line:
 
-One step = recompute the edge costs on the device (generate) + one minimum
-cost/time-ratio cycle solve (lawlergpu).  `value` is solves/s with the inputs
-resident in HBM, timed with CUDA events on the solver's stream; `e2e` is the
-same solve through the public API from host arrays (handle creation, host ->
-device copies, template build, solve, matching read back).
+* top level -- the single-pair GPU configuration: a perturbed genus-0 mesh X
+  with 5,000 vertices (both orientations of its ~30k edges) and normals, a
+  200-point closed silhouette curve Y with in-plane normals, 64-d float32
+  features -> feat_diff; conjugate product graph, k = 3, cost/time mode
+  ("vanilla", "lengthnormalisation").  One step = recompute the edge costs on
+  the device (generate) + one minimum cost/time-ratio cycle solve
+  (lawlergpu).  Its "dijkstragpu" sub-object times the minimum-cost solve of
+  the same graph (generate + dijkstragpu per step).
+* "configs" -- the other GPU configurations, each with its own value, e2e,
+  roofline and (where the metric asks for it) vs_plain_gpu_lawler:
+  batched serving of 256 uneven plain pairs, forward + backward on 32 plain
+  pairs, and the large pruned conjugate pair (20k vertices x 500 curve
+  points, k = 4).
+
+`value` is throughput with the inputs resident in HBM, timed with CUDA
+events on the solver's stream; `e2e` is the same work through the public API
+from host arrays (handle creation, host -> device copies, template build,
+solve, results back).  Inputs are seeded synthetic data of the stated shapes
+(no dataset).  --workload NAME measures one configuration alone.
 
 --impl reference times the reference algorithm's CPU implementation (the
 restatement under oracle/; the reference itself cannot be compiled in this
-environment) on the host cores: a full lawlercpu solve during warm-up gives
-the sweep count, each timed step times a bounded sample (one Bellman-Ford
-sweep), and solves/s = 1 / (energy + rescale + in-edge sets + sweeps x sweep).
+environment) on all host cores, on the same configuration: every timed step
+is one complete lawlercpu solve (energies recomputed on the product graph,
+in-place rescale, in-edge sets, branch and bound), as many as fit a fixed
+time budget; the line's `steps` is the number actually timed.
 
 Multi-GPU: the path does not shard within a pair; --gpus N runs N independent
 replicas (one pair per rank, seed = rank), value = total solves / max time.
@@ -25,11 +36,6 @@ replicas (one pair per rank, seed = rank), value = total solves / max time.
 from __future__ import annotations
 
 import os
-
-# before anything starts CUDA: 32 host work queues let batched solves (one
-# stream per pair) run side by side; the default of 8 serialises them
-os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
-
 import argparse
 import gc
 import json
@@ -200,15 +206,122 @@ def algorithmic_bytes_per_sweep(info, k, ratio_mode):
     return (4 + 4 * c) * (e_inter + (k - 1) * e_intra) + 8 * depths * nodes
 
 
-def run_ours(args, world, rank):
+def host_cpu():
+    """The host's CPU model and the cores this process may use (lscpu's model name and affinity)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    return {"model": model, "usable_cores": usable, "logical_cpus": os.cpu_count() or 1}
+
+
+def _solve_once(g, solver, k):
+    return g.solve_with_cost_time_ratio("lawlergpu", k) if solver == "ratio" else \
+        g.solve_with_minimum_cost("dijkstragpu", k)
+
+
+def _time_pair_steps(g, stream, solver, k, steps, warmup, info, world):
+    """Warm-up, then `steps` timed steps of generate + solve on `stream`
+    (CUDA events around each step); the L2 is flushed between timed steps
+    when the cost streams fit in it.  Returns the timing and counters."""
+    import torch
+
+    def step():
+        g.generate()
+        return _solve_once(g, solver, k)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    sweeps = bf_us = launches = 0
+    result = st = prof = None
+    edges = info["layers"] * info["edges_per_block"]
+    flush = torch.empty(1 << 25, dtype=torch.float64, device="cuda") if 8 * edges < L2_BYTES else None
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.fill_(float(i))
+            ev[i][0].record(stream)
+            result = step()
+            ev[i][1].record(stream)
+            st = g.last_stats()
+            prof = g.last_profile()
+            sweeps += st["sweeps"]
+            bf_us += st["device_us"]
+            launches += st["kernel_launches"] + 1  # + the energy kernel of generate()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    return dict(total_ms=max_over_ranks(sum(step_ms), world, "cuda"), sweeps=sweeps, bf_us=bf_us,
+                launches=launches, result=result, stats=st, profile=prof, clocks=clocks.summary(), wall=wall)
+
+
+def _e2e_pair(cpg, hargs, pair, cfg, solver, steps, world):
+    """The same solve end to end from host arrays: one fresh handle per
+    request (created after the timed handle was released, as in a serving
+    process), normals and modes set, solved, the matching read back."""
     import numpy as np
+    import torch
+
+    h2d = sum(int(np.asarray(pair[key]).nbytes) for key in ("VX", "EX", "VY", "EY", "feat_diff"))
+    if cfg["conj"]:
+        h2d += int(pair["NX"].nbytes + pair["NY"].nbytes)
+    d2h = 0
+    for it in range(steps + 1):  # the first pass is an untimed warm-up (module loading, first allocations)
+        if it == 1:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+        ge = cpg.product_graph_generator(*hargs)
+        if cfg["conj"]:
+            ge.set_normals(pair["NX"], pair["NY"])
+        ge.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+        out = _solve_once(ge, solver, cfg["k"])
+        d2h = int(out[2].nbytes) + 8
+        del ge
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    return {"value": world * steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps}
+
+
+def _traffic(workload):
+    """DRAM bytes of one Bellman-Ford launch of `workload` from its ncu summary under profiles/, and how it was got."""
+    tpath = os.path.join(ROOT, "profiles", f"bf_kernel_{workload}.json")
+    if not os.path.exists(tpath):
+        return None, None
+    try:
+        with open(tpath) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch"), d.get("kind", "measured") + ": " + d.get("source", "")
+    except Exception:
+        return None, None
+
+
+def measure_pair(args, world, rank, workload, steps, warmup, e2e_steps, with_min_cost=False, with_cpu=False):
+    """One shape pair: ratio solves (and optionally min-cost solves) timed on
+    the device, end to end through the public API, roofline of the
+    Bellman-Ford kernel, and optionally the CPU baseline."""
     import torch
 
     import cyclic_product_graphs as cpg
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    dev = torch.cuda.current_device()
-    pair, cfg = _make_pair(args.workload, seed=args.seed + rank)
+    pair, cfg = _make_pair(workload, seed=args.seed + rank)
     k = cfg["k"]
     hargs = (pair["VX"], pair["EX"], pair["VY"], pair["EY"], pair["feat_diff"], cfg["conj"], cfg["reg"], cfg["prune"])
 
@@ -220,153 +333,115 @@ def run_ours(args, world, rank):
     g.set_stream(stream.cuda_stream)
     g.generate()
     info = g.graph_info()
-
-    def step():
-        g.generate()
-        return g.solve_with_cost_time_ratio("lawlergpu", k)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    sweeps = bf_us = launches = 0
-    result = None
-    # cost streams smaller than L2 (126 MB): flush L2 between the timed steps
-    # with a 256 MB write on the solver's stream, outside the steps' events
-    edges = info["layers"] * info["edges_per_block"]
-    flush = torch.empty(1 << 25, dtype=torch.float64, device="cuda") if 8 * edges < L2_BYTES else None
-    with ClockSampler(dev) as clocks:
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for i in range(args.steps):
-            if flush is not None:
-                with torch.cuda.stream(stream):
-                    flush.fill_(float(i))
-            ev[i][0].record(stream)
-            result = step()
-            ev[i][1].record(stream)
-            st = g.last_stats()
-            prof = g.last_profile()
-            last_sweeps = st["sweeps"]
-            sweeps += st["sweeps"]
-            bf_us += st["device_us"]
-            launches += st["kernel_launches"] + 1  # + the energy kernel of generate()
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = max_over_ranks(sum(step_ms), world, "cuda")
-    ms_per_step = total_ms / args.steps
-    value = replica_throughput(args.steps, world, total_ms)
-
-    # roofline of the dominant kernel (the Bellman-Ford launch)
     peak, peak_kind = _peaks()
-    b_sweep = algorithmic_bytes_per_sweep(info, k, True)
-    achieved = (b_sweep * sweeps) / (bf_us * 1e-6) / 1e9 if bf_us else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"bf_kernel_{args.workload}.json")
-    if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
 
-    # End to end through the public API from host buffers, as a serving
-    # process runs it: one fresh handle per request, created after the timed
-    # handle has been released (as in the batch and fwd/bwd workloads; a live
-    # second handle made each request ~4 ms slower on the host).
-    del g
-    gc.collect()
-    torch.cuda.synchronize()
-    e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    h2d = sum(int(np.asarray(pair[key]).nbytes) for key in ("VX", "EX", "VY", "EY", "feat_diff"))
-    if cfg["conj"]:
-        h2d += int(pair["NX"].nbytes + pair["NY"].nbytes)
-    d2h = 0
-    for it in range(e2e_steps + 1):  # the first pass is an untimed warm-up (module loading, first allocations)
-        if it == 1:
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-        ge = cpg.product_graph_generator(*hargs)
-        if cfg["conj"]:
-            ge.set_normals(pair["NX"], pair["NY"])
-        ge.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
-        out = ge.solve_with_cost_time_ratio("lawlergpu", k)
-        d2h = int(out[2].nbytes) + 8
-        del ge
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_value = world * e2e_steps / e2e_s
+    def roofline(t, ratio_mode, steps_done):
+        b_sweep = algorithmic_bytes_per_sweep(info, k, ratio_mode)
+        achieved = (b_sweep * t["sweeps"]) / (t["bf_us"] * 1e-6) / 1e9 if t["bf_us"] else None
+        r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+             "frac": (achieved / peak) if achieved else None, "traffic": None,
+             "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_kernel",
+             "algorithmic_bytes_per_sweep": b_sweep, "sweeps_per_solve": t["sweeps"] / steps_done,
+             "bf_ms_per_solve": t["bf_us"] / 1000.0 / steps_done}
+        if ratio_mode:
+            r["traffic"], r["traffic_source"] = _traffic(workload)
+        return r
 
+    t = _time_pair_steps(g, stream, "ratio", k, steps, warmup, info, world)
+    prof, st = t["profile"], t["stats"]
     line = {
         "metric": METRIC,
-        "value": value,
+        "value": replica_throughput(steps, world, t["total_ms"]),
         "unit": "solves/s",
         "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": t["total_ms"] / steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64 (fp32 integer-valued cost streams)",
         "data": "synthetic (seeded)",
-        "config": _pair_config(args.workload, cfg, info["nodes_per_layer"], info["layers"],
+        "config": _pair_config(workload, cfg, info["nodes_per_layer"], info["layers"],
                                info["layers"] * info["edges_per_block"], world),
-        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps},
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_kernel",
-                     "algorithmic_bytes_per_sweep": b_sweep, "sweeps_per_solve": sweeps / args.steps,
-                     "bf_ms_per_solve": bf_us / 1000.0 / args.steps},
+        "gpu_launches": t["launches"],
+        "roofline": roofline(t, True, steps),
         "bf_team": {"ctas": prof["ctas"], "threads": prof["threads"], "wait_list_entries": prof["wait_entries"],
                     "cycles_per_step": {key[7:]: round(prof[key] / max(1, prof["steps"]), 1)
                                         for key in ("cycles_relax", "cycles_stage_wait", "cycles_handoff",
                                                     "cycles_bookkeeping", "cycles_sweep_tail")},
-                    "tail_cycles_per_sweep": {key[12:]: round(prof[key] / max(1, last_sweeps), 1)
+                    "tail_cycles_per_sweep": {key[12:]: round(prof[key] / max(1, st["sweeps"]), 1)
                                               for key in ("cycles_tail_wrap", "cycles_tail_candidates",
                                                           "cycles_tail_lead")},
                     "last_solve": {key: st[key] for key in ("bf_calls", "sweeps", "candidates", "fallback_walks",
                                                             "lawler_iters")}},
-        "clocks": clocks.summary(),
-        "result": {"objective": result[1], "cycle_edges": int(result[2].shape[0])},
-        "wall_s": wall,
+        "clocks": t["clocks"],
+        "result": {"objective": t["result"][1], "cycle_edges": int(t["result"][2].shape[0])},
+        "wall_s": t["wall"],
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(pair, cfg, sweeps / args.steps, args.cpu_sweeps)
+    if with_min_cost:
+        tm = _time_pair_steps(g, stream, "min_cost", k, steps, warmup, info, world)
+        line["dijkstragpu"] = {
+            "value": replica_throughput(steps, world, tm["total_ms"]), "unit": "solves/s",
+            "ms_per_step": tm["total_ms"] / steps, "steps": steps, "warmup": warmup,
+            "gpu_launches": tm["launches"], "roofline": roofline(tm, False, steps), "clocks": tm["clocks"],
+            "result": {"objective": tm["result"][1], "cycle_edges": int(tm["result"][2].shape[0]),
+                       "bf_calls": tm["stats"]["bf_calls"], "branches": tm["stats"]["branches"]},
+        }
+    del g
+    gc.collect()
+    torch.cuda.synchronize()
+    line["e2e"] = _e2e_pair(cpg, hargs, pair, cfg, "ratio", max(1, min(steps, e2e_steps)), world)
+    if with_min_cost:
+        line["dijkstragpu"]["e2e"] = _e2e_pair(cpg, hargs, pair, cfg, "min_cost", max(1, min(steps, e2e_steps)),
+                                               world)
+    cpg.release_cached_memory()
+    if with_cpu and rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(pair, cfg)
     return line
 
 
-def cpu_baseline(pair, cfg, sweeps_per_solve, sample_sweeps):
-    """The reference algorithm on the host cores: measured phases of one ratio
-    solve, with `sample_sweeps` Bellman-Ford sweeps timed and scaled to the
-    solve's sweep count."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
-
-    cores = os.cpu_count() or 1
-    orc.set_threads(cores)
+def _oracle_pair(orc, pair, cfg):
     hargs = (pair["VX"], pair["EX"], pair["VY"], pair["EY"], pair["feat_diff"], cfg["conj"], cfg["reg"], cfg["prune"])
     o = orc.OracleGenerator(*hargs)
     if cfg["conj"]:
         o.set_normals(pair["NX"], pair["NY"])
     o.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+    return o
+
+
+def _oracle_step(o, solver, k):
+    """One complete CPU step, the counterpart of the device's generate + solve:
+    the energies recomputed on the product graph already built, then the
+    whole lawlercpu (rescale, in-edge sets, branch and bound) or dijkstracpu
+    solve."""
+    t0 = time.perf_counter()
+    o.recompute_energy()
+    res = o.solve_with_cost_time_ratio("lawlercpu", k) if solver == "ratio" else \
+        o.solve_with_minimum_cost("dijkstracpu", k)
+    return time.perf_counter() - t0, res
+
+
+def cpu_baseline(pair, cfg):
+    """The reference algorithm on the host cores: one complete ratio step
+    (energies + lawlercpu solve), timed once."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+
+    cpu = host_cpu()
+    orc.set_threads(cpu["usable_cores"])
+    o = _oracle_pair(orc, pair, cfg)
     t0 = time.perf_counter()
     o.generate()
-    t_gen = time.perf_counter() - t0
-    ph = o.time_phases(cfg["k"], 0.3, sample_sweeps)
-    t_solve = ph["energy_s"] + ph["rescale_s"] + ph["in_graph_s"] + sweeps_per_solve * ph["sweep_s"]
-    return {"value": 1.0 / t_solve, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": (f"oracle lawlercpu restatement, OpenMP x{cores}: energy {ph['energy_s']:.2f}s + rescale "
-                       f"{ph['rescale_s']:.2f}s + in-edge sets {ph['in_graph_s']:.2f}s measured, "
-                       f"{sample_sweeps} Bellman-Ford sweeps timed ({ph['sweep_s']:.3f}s each) and scaled to "
-                       f"{sweeps_per_solve:.1f} sweeps/solve; product-graph build {t_gen:.1f}s not counted"),
-            "phases_s": ph}
+    t_graph = time.perf_counter() - t0
+    secs, res = _oracle_step(o, "ratio", cfg["k"])
+    return {"value": 1.0 / secs, "unit": "solves/s", "cores": cpu["usable_cores"], "kind": "port",
+            "cpu": cpu,
+            "sample": (f"one complete step of the oracle's lawlercpu restatement, OpenMP x{cpu['usable_cores']}: "
+                       f"energies recomputed + rescale + in-edge sets + branch and bound, {secs:.1f}s "
+                       f"({o.last_stats()['sweeps']} sweeps); the product graph, built once before "
+                       f"({t_graph:.1f}s), is not counted, as the device keeps its layer template"),
+            "result": {"objective": res[1], "cycle_edges": int(res[2].shape[0])}}
 
 
 def _pair_config(workload, cfg, nodes_per_layer, layers, edges, world):
@@ -378,49 +453,52 @@ def _pair_config(workload, cfg, nodes_per_layer, layers, edges, world):
             "l2": l2}
 
 
-def run_reference(args):
+REFERENCE_BUDGET_S = 120.0  # timed CPU work of the reference arm's main configuration
+
+
+def run_reference(args, workload, with_min_cost=False):
+    """The oracle's lawlercpu on the host cores: after one untimed warm-up
+    step, complete steps are timed until the budget is spent (at least one,
+    at most --steps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
 
-    pair, cfg = _make_pair(args.workload, seed=args.seed)
-    cores = os.cpu_count() or 1
+    pair, cfg = _make_pair(workload, seed=args.seed)
+    cpu = host_cpu()
+    cores = cpu["usable_cores"]
     orc.set_threads(cores)
-    hargs = (pair["VX"], pair["EX"], pair["VY"], pair["EY"], pair["feat_diff"], cfg["conj"], cfg["reg"], cfg["prune"])
-    o = orc.OracleGenerator(*hargs)
-    if cfg["conj"]:
-        o.set_normals(pair["NX"], pair["NY"])
-    o.set_cost_time_ratio_mode(cfg["cost"], cfg["time"])
+    o = _oracle_pair(orc, pair, cfg)
     o.generate()
-    # warm-up: one full solve fixes the sweep count of a solve, one timed
-    # pass of the per-solve phases (energy, rescale, in-edge sets) their cost
-    t0 = time.perf_counter()
-    res = o.solve_with_cost_time_ratio("lawlercpu", cfg["k"])
-    t_full = time.perf_counter() - t0
-    stats = o.last_stats()
-    sweeps = stats["sweeps"]
-    ph = o.time_phases(cfg["k"], 0.3, 1)
-    fixed = ph["energy_s"] + ph["rescale_s"] + ph["in_graph_s"]
-    for _ in range(max(0, args.warmup - 1)):
-        o.time_sweeps(cfg["k"], 0.3, 1)
-    # timed steps: one Bellman-Ford sweep each (the bounded sample)
-    samples = [o.time_sweeps(cfg["k"], 0.3, 1) for _ in range(args.steps)]
-    sweep_s = statistics.median(samples)
-    t_solve = fixed + sweeps * sweep_s
-    value = 1.0 / t_solve
-    return {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000.0 * t_solve, "higher_is_better": True,
+    warm_s, _ = _oracle_step(o, "ratio", cfg["k"])
+    n = max(1, min(args.steps, int(REFERENCE_BUDGET_S // max(warm_s, 1e-9))))
+    samples, res = [], None
+    for _ in range(n):
+        secs, res = _oracle_step(o, "ratio", cfg["k"])
+        samples.append(secs)
+    mean_s = sum(samples) / len(samples)
+    value = 1.0 / mean_s
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": n,
+        "warmup": 1, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": 1000.0 * mean_s, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": _pair_config(args.workload, cfg, 3 * len(pair["EX"]) if cfg["conj"] else len(pair["VX"]),
+        "config": _pair_config(workload, cfg, 3 * len(pair["EX"]) if cfg["conj"] else len(pair["VX"]),
                                len(pair["EY"]), o.product_space_rows(), int(os.environ.get("WORLD_SIZE", "1"))),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": f"one Bellman-Ford sweep per step (median {sweep_s:.3f}s) scaled to {sweeps} "
-                                   f"sweeps/solve, plus energy {ph['energy_s']:.2f}s + rescale {ph['rescale_s']:.2f}s "
-                                   f"+ in-edge sets {ph['in_graph_s']:.2f}s timed once; a full warm-up solve took "
-                                   f"{t_full:.1f}s"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "cpu": cpu,
+                         "sample": (f"{n} complete steps of the oracle's lawlercpu restatement (energies "
+                                    f"recomputed + rescale + in-edge sets + branch and bound), OpenMP x{cores}, "
+                                    f"after one untimed warm-up step ({warm_s:.1f}s); steps timed until a "
+                                    f"{REFERENCE_BUDGET_S:.0f}s budget, each {min(samples):.1f}-{max(samples):.1f}s")},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "full_solve_s": t_full, "result": {"objective": res[1], "cycle_edges": int(res[2].shape[0])},
+        "step_s": samples, "result": {"objective": res[1], "cycle_edges": int(res[2].shape[0])},
     }
+    if with_min_cost:
+        secs, mres = _oracle_step(o, "min_cost", cfg["k"])
+        line["dijkstracpu"] = {"value": 1.0 / secs, "unit": "solves/s", "steps": 1, "ms_per_step": 1000.0 * secs,
+                               "sample": "one complete dijkstracpu step (energies recomputed + solve), "
+                                         f"OpenMP x{cores}",
+                               "result": {"objective": mres[1], "cycle_edges": int(mres[2].shape[0])}}
+    return line
 
 
 def _batch_specs(name, seed):
@@ -686,6 +764,8 @@ def run_fwdbwd(args, world, rank):
             torch.cuda.synchronize()
     total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
     value = replica_throughput(len(gens) * args.steps, world, total_ms)
+    # per pair and step: the solve's launches, the energy kernel and the adjoint kernel
+    launches = args.steps * sum(g.last_stats()["kernel_launches"] + 2 for g in gens)
     grads_ok = all(t.grad is not None and bool(torch.isfinite(t.grad).all()) for t in fX)
 
     step_plain()
@@ -727,7 +807,7 @@ def run_fwdbwd(args, world, rank):
                 "d2h_bytes_per_step": d2h, "steps": 1},
         "gradients_finite": grads_ok,
         "mean_objective": mean_objective,
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
 
@@ -760,28 +840,101 @@ def run_reference_fwdbwd(args):
             "e2e": {"value": value, "unit": "fwd+bwd pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+SUB_CONFIGS = ("batch_256_plain_1k8k", "fwdbwd_32_plain_2k_100_k2", "conj_prune_20k_500_k4")
+
+
+def _sub_args(args, workload, steps, warmup):
+    import argparse
+
+    sub = argparse.Namespace(**vars(args))
+    sub.workload, sub.steps, sub.warmup = workload, steps, warmup
+    return sub
+
+
+def full_metric_line(args, world, rank):
+    """The default line: the single-pair configuration at the top level, with
+    its dijkstragpu timing and the CPU baseline, and the batched, fwd/bwd and
+    large-pair configurations under "configs"."""
+    import torch
+
+    import cyclic_product_graphs as cpg
+
+    line = measure_pair(args, world, rank, DEFAULT_WORKLOAD, args.steps, args.warmup, args.e2e_steps,
+                        with_min_cost=True, with_cpu=not args.no_cpu_baseline)
+    sub_steps, sub_warmup = max(1, min(args.steps, args.sub_steps)), max(3, min(args.warmup, 3))
+    configs = {}
+    for name in SUB_CONFIGS:
+        sub = _sub_args(args, name, sub_steps, sub_warmup)
+        if name in BATCHES:
+            configs[name] = run_batch(sub, world, rank)
+        elif name in FWDBWD:
+            configs[name] = run_fwdbwd(sub, world, rank)
+        else:
+            configs[name] = measure_pair(sub, world, rank, name, sub_steps, sub_warmup, 2)
+        for key in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+            configs[name].pop(key, None)
+        torch.cuda.synchronize()
+        gc.collect()
+        cpg.release_cached_memory()
+    line["configs"] = configs
+    return line
+
+
+def full_reference_line(args):
+    """The reference arm of the default line: complete lawlercpu steps of the
+    single-pair configuration, one dijkstracpu step, and CPU samples of the
+    batched and fwd/bwd configurations."""
+    line = run_reference(args, DEFAULT_WORKLOAD, with_min_cost=True)
+    configs = {}
+    for name in SUB_CONFIGS:
+        sub = _sub_args(args, name, 2, 1)
+        if name in BATCHES:
+            configs[name] = run_reference_batch(sub)
+        elif name in FWDBWD:
+            configs[name] = run_reference_fwdbwd(sub)
+        else:
+            configs[name] = {"impl": "reference", "unavailable": (
+                "not timed on the CPU within the bench's budget: the oracle builds and holds the full product "
+                "graph (721 M edges; about 30 GB of host memory with its costs and in-edge sets) and spends "
+                "minutes per solve")}
+        for key in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+            configs[name].pop(key, None)
+    line["configs"] = configs
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(FWDBWD),
-                    default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCHES) + sorted(FWDBWD), default=None,
+                    help="measure one configuration alone (default: the whole metric)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-sweeps", type=int, default=3)
+    ap.add_argument("--sub-steps", type=int, default=5, help="timed steps of each configuration under 'configs'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world, rank, local = _dist_env()
 
     if args.impl == "reference":
         if rank == 0:
-            fn = run_reference_batch if args.workload in BATCHES else run_reference_fwdbwd \
-                if args.workload in FWDBWD else run_reference
-            print(json.dumps(fn(args)), flush=True)
+            if args.workload is None:
+                line = full_reference_line(args)
+            elif args.workload in BATCHES:
+                line = run_reference_batch(args)
+            elif args.workload in FWDBWD:
+                line = run_reference_fwdbwd(args)
+            else:
+                line = run_reference(args, args.workload)
+            print(json.dumps(line), flush=True)
         return
 
+    # 32 host work queues let batched solves (one stream per pair) run side
+    # by side; CUDA's default of 8 serialises them.  Read when CUDA starts,
+    # so it is set before anything touches the device.
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if world > 1:
         import datetime
 
@@ -789,12 +942,15 @@ def main():
 
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if args.workload in BATCHES:
+    if args.workload is None:
+        line = full_metric_line(args, world, rank)
+    elif args.workload in BATCHES:
         line = run_batch(args, world, rank)
     elif args.workload in FWDBWD:
         line = run_fwdbwd(args, world, rank)
     else:
-        line = run_ours(args, world, rank)
+        line = measure_pair(args, world, rank, args.workload, args.steps, args.warmup, args.e2e_steps,
+                            with_min_cost=False, with_cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

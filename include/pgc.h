@@ -96,9 +96,12 @@ int pgc_get_cost_vector(pgc_graph* g, double* out);
  * and rows x cols must be at most 2^21 (PGC_ERR_ARG otherwise).  Nothing
  * needs clearing first: the export writes every value.  The first call on a
  * device takes the scratch's device address (cudaGetSymbolAddress, that
- * device current); make that first call before any stream capture.  Every
- * call shares the one scratch of its device, so calls that overlap on the GPU
- * race on it. */
+ * device current) and keeps it for the life of the process; make that first
+ * call before any stream capture.  A device reset (cudaDeviceReset, or
+ * anything else that destroys the device's primary context) invalidates that
+ * address: do not call this entry point on a device after resetting it in the
+ * same process.  Every call shares the one scratch of its device, so calls
+ * that overlap on the GPU race on it. */
 int pgc_get_cost_vector_noalloc(pgc_graph* g, double* out);
 
 /* getProductSpace() -- product_graph_generators.cpp:173-178, bindings.cpp:39.
@@ -217,6 +220,12 @@ int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_
  * layer, interlayer slots per layer, intralayer slots per layer (slots include
  * the sliced-ELL padding), cost columns]. */
 int pgc_graph_info(pgc_graph* g, int64_t* out8);
+
+/* No reference counterpart.  Name of the GPU the handle's device work runs
+ * on (cudaDeviceProp::name), NUL-terminated and cut to capacity - 1 bytes.
+ * The autotuner keys its cache by it, so a cache file written on one GPU type
+ * is not applied on another. */
+int pgc_device_name(pgc_graph* g, char* out, int64_t capacity);
 
 /* Returns the device memory and the pinned host memory cached by the
  * library's allocators to CUDA (no reference counterpart; freed buffers are

@@ -44,6 +44,7 @@ def lib():
         L.orc_set_robust_loss.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.orc_generate.argtypes = [ctypes.c_void_p]
         L.orc_ensure_generated.argtypes = [ctypes.c_void_p]
+        L.orc_recompute_energy.argtypes = [ctypes.c_void_p]
         L.orc_cost_shape.argtypes = [ctypes.c_void_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]
         L.orc_get_cost.argtypes = [ctypes.c_void_p, _dp]
         L.orc_set_cost.argtypes = [ctypes.c_void_p, _dp, _i64, _i64]
@@ -114,6 +115,11 @@ class OracleGenerator:
 
     def generate(self):
         if lib().orc_generate(self._h) != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def recompute_energy(self):
+        """The edge costs again on the product graph already built (a first call generates)."""
+        if lib().orc_recompute_energy(self._h) != 0:
             raise RuntimeError(lib().orc_last_error().decode())
 
     def _ensure(self):

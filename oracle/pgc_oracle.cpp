@@ -1443,6 +1443,21 @@ struct Generator {
         }
         generated = true;
     }
+    // The energies again on the product graph already built: what a second
+    // generate() recomputes when its graph is kept (product_graph_generators.cpp:
+    // 44-47, :81-85), and what the device's generate() does with its cached
+    // layer template.
+    void recompute_energy() {
+        if (!generated) {
+            generate();
+            return;
+        }
+        if (conj)
+            energy = ho_energy(VX, EX, NX, VY, EY, NY, g, FD, reg, RobustLoss{rlAlpha, rlC, rlPwr}, prune, costName,
+                               timeName);
+        else
+            energy = plain_energy(VX, VY, g.ps, FD, reg, costName, timeName);
+    }
 };
 
 }  // namespace orc
@@ -1497,6 +1512,10 @@ void orc_set_robust_loss(void* h, double a, double c, double p) {
 }
 int orc_generate(void* h) {
     try { ((Generator*)h)->generate(); return 0; }
+    catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
+int orc_recompute_energy(void* h) {
+    try { ((Generator*)h)->recompute_energy(); return 0; }
     catch (const std::exception& e) { g_err = e.what(); return -1; }
 }
 int orc_ensure_generated(void* h) {

@@ -2315,6 +2315,18 @@ int pgc_graph_info(pgc_graph* h, int64_t* out8) {
     });
 }
 
+int pgc_device_name(pgc_graph* h, char* out, int64_t capacity) {
+    return guarded([&] {
+        if (!h) throw Failure(PGC_ERR_ARG, "null handle");
+        if (!out || capacity < 1) throw Failure(PGC_ERR_ARG, "null or empty output buffer");
+        cudaDeviceProp prop{};
+        PGC_CUDA(cudaGetDeviceProperties(&prop, h->g.device));
+        const size_t len = std::min(std::strlen(prop.name), (size_t)capacity - 1);
+        std::memcpy(out, prop.name, len);
+        out[len] = '\0';
+    });
+}
+
 int pgc_release_cached_memory(void) {
     return guarded([&] {
         pgc::DevicePool::get().release_cached();

@@ -11,21 +11,18 @@ matching: int32 ndarray)``.
 
 Everything runs through the C ABI of ``lib/libpgc.so`` (include/pgc.h); the
 solvers execute on the GPU.  There is no CPU fallback: importing this module
-without the built library raises ImportError.
+without the built library raises ImportError.  The library is opened on the
+first call that needs it, so importing the package (or its ``synthetic``
+data module) changes nothing in the process: no library is mapped and no
+environment variable is set.
 """
 from __future__ import annotations
 
 import ctypes
 import os
+import threading
 
 import numpy as np
-
-# Batched solves run one CUDA stream per graph; the device runs them side by
-# side only as far as it has host work queues, 8 by default.  32 (the most)
-# triples batched throughput.  The driver reads this when the process's CUDA
-# context is created, so it takes effect only if nothing has used CUDA yet;
-# a value the user set is kept.
-os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
            "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune", "release_cached_memory",
@@ -38,48 +35,77 @@ if not os.path.exists(library_path):
     raise ImportError(f"cyclic_product_graphs: {library_path} is missing; build it with "
                       "`python -c 'import __graft_entry__ as g; g.build()'` (or make -C product-graph-cycles_b200/csrc)")
 
-_lib = ctypes.CDLL(library_path)
 _i64 = ctypes.c_int64
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
 _lp = ctypes.POINTER(ctypes.c_int64)
 _h = ctypes.c_void_p
 
-_lib.pgc_create.argtypes = [_dp, _i64, _ip, _i64, _dp, _i64, _ip, _i64, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                            ctypes.POINTER(_h)]
-_lib.pgc_destroy.argtypes = [_h]
-_lib.pgc_destroy.restype = None
-_lib.pgc_set_normals.argtypes = [_h, _dp, _i64, _i64, _dp, _i64, _i64]
-_lib.pgc_set_max_depth.argtypes = [_h, ctypes.c_int]
-_lib.pgc_set_cost_time_ratio_mode.argtypes = [_h, ctypes.c_char_p, ctypes.c_char_p]
-_lib.pgc_update_robust_loss_params.argtypes = [_h, ctypes.c_double, ctypes.c_double, ctypes.c_double]
-_lib.pgc_generate.argtypes = [_h]
-_lib.pgc_cost_vector_shape.argtypes = [_h, _lp, _lp]
-_lib.pgc_get_cost_vector.argtypes = [_h, _dp]
-_lib.pgc_product_space_shape.argtypes = [_h, _lp, _lp]
-_lib.pgc_get_product_space.argtypes = [_h, _ip]
-_lib.pgc_solve_with_cost_time_ratio.argtypes = [_h, ctypes.c_char_p, ctypes.c_int]
-_lib.pgc_solve_with_minimum_cost.argtypes = [_h, ctypes.c_char_p, ctypes.c_int]
-_lib.pgc_result.argtypes = [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), _lp, _lp]
-_lib.pgc_result_matching.argtypes = [_h, _ip]
-_lib.pgc_result_cycle_edges.argtypes = [_h, _lp, _i64, _lp]
-_lib.pgc_result_stats.argtypes = [_h, _lp]
-_lib.pgc_compute_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
-_lib.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
-_lib.pgc_graph_info.argtypes = [_h, _lp]
-_lib.pgc_result_profile.argtypes = [_h, _lp]
-_lib.pgc_result_profile_detail.argtypes = [_h, _lp]
-_lib.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
-_lib.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
-_lib.pgc_set_team_shape.argtypes = [_h, ctypes.c_int, ctypes.c_int]
-_lib.pgc_product_graph_sizes.argtypes = [_ip, _i64, _i64, _i64, ctypes.c_int, ctypes.c_int, _lp]
-_lib.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
-_lib.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
-_lib.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
-_lib.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                 ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
-_lib.pgc_last_error.restype = ctypes.c_char_p
-_lib.pgc_version.restype = ctypes.c_char_p
+
+def _declare(L):
+    """Argument and result types of every C entry point the package calls."""
+    L.pgc_create.argtypes = [_dp, _i64, _ip, _i64, _dp, _i64, _ip, _i64, _dp, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_int, ctypes.POINTER(_h)]
+    L.pgc_destroy.argtypes = [_h]
+    L.pgc_destroy.restype = None
+    L.pgc_set_normals.argtypes = [_h, _dp, _i64, _i64, _dp, _i64, _i64]
+    L.pgc_set_max_depth.argtypes = [_h, ctypes.c_int]
+    L.pgc_set_cost_time_ratio_mode.argtypes = [_h, ctypes.c_char_p, ctypes.c_char_p]
+    L.pgc_update_robust_loss_params.argtypes = [_h, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.pgc_generate.argtypes = [_h]
+    L.pgc_cost_vector_shape.argtypes = [_h, _lp, _lp]
+    L.pgc_get_cost_vector.argtypes = [_h, _dp]
+    L.pgc_product_space_shape.argtypes = [_h, _lp, _lp]
+    L.pgc_get_product_space.argtypes = [_h, _ip]
+    L.pgc_solve_with_cost_time_ratio.argtypes = [_h, ctypes.c_char_p, ctypes.c_int]
+    L.pgc_solve_with_minimum_cost.argtypes = [_h, ctypes.c_char_p, ctypes.c_int]
+    L.pgc_result.argtypes = [_h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), _lp, _lp]
+    L.pgc_result_matching.argtypes = [_h, _ip]
+    L.pgc_result_cycle_edges.argtypes = [_h, _lp, _i64, _lp]
+    L.pgc_result_stats.argtypes = [_h, _lp]
+    L.pgc_compute_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
+    L.pgc_compute_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
+    L.pgc_graph_info.argtypes = [_h, _lp]
+    L.pgc_result_profile.argtypes = [_h, _lp]
+    L.pgc_result_profile_detail.argtypes = [_h, _lp]
+    L.pgc_set_stream.argtypes = [_h, ctypes.c_void_p]
+    L.pgc_set_team_cap.argtypes = [_h, ctypes.c_int]
+    L.pgc_set_team_shape.argtypes = [_h, ctypes.c_int, ctypes.c_int]
+    L.pgc_product_graph_sizes.argtypes = [_ip, _i64, _i64, _i64, ctypes.c_int, ctypes.c_int, _lp]
+    L.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
+    L.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
+    L.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
+    L.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.pgc_device_name.argtypes = [_h, ctypes.c_char_p, _i64]
+    L.pgc_last_error.restype = ctypes.c_char_p
+    L.pgc_version.restype = ctypes.c_char_p
+
+
+class _Library:
+    """libpgc.so, opened with its entry points declared on first attribute access."""
+
+    def __init__(self):
+        self._cdll = None
+        self._mutex = threading.Lock()
+
+    def __getattr__(self, name):
+        cdll = self._cdll
+        if cdll is None:
+            with self._mutex:
+                if self._cdll is None:
+                    L = ctypes.CDLL(library_path)
+                    _declare(L)
+                    self._cdll = L
+                cdll = self._cdll
+        return getattr(cdll, name)
+
+    @property
+    def loaded(self) -> bool:
+        return self._cdll is not None
+
+
+_lib = _Library()
 
 
 class PGCError(RuntimeError):
@@ -257,6 +283,12 @@ class product_graph_generator:
         """Issue all device work of this generator on `cuda_stream` (a cudaStream_t as int)."""
         _check(_lib.pgc_set_stream(self._h, ctypes.c_void_p(cuda_stream) if cuda_stream else None))
 
+    def device_name(self) -> str:
+        """Name of the GPU this generator's device work runs on (C: pgc_device_name)."""
+        buf = ctypes.create_string_buffer(256)
+        _check(_lib.pgc_device_name(self._h, buf, len(buf)))
+        return buf.value.decode(errors="replace")
+
     def last_stats(self) -> dict:
         buf = (ctypes.c_int64 * 8)()
         _check(_lib.pgc_result_stats(self._h, buf))
@@ -327,9 +359,10 @@ def autotune(gen: "product_graph_generator", max_depth: int | None = None, candi
     """Picks the Bellman-Ford team shape (CTAs, threads per CTA) for the shape
     bucket of ``gen`` and applies it (no counterpart in the reference).
 
-    The bucket is (nodes per layer rounded up to a power of two, layers
-    rounded up to a power of two, max depth, whether layers have intralayer
-    edges).  A bucket found in the JSON file ``cache_path`` is applied
+    The bucket is (the GPU's name, nodes per layer rounded up to a power of
+    two, layers rounded up to a power of two, max depth, whether layers have
+    intralayer edges): a cache file written on one GPU type is not applied
+    on another.  A bucket found in the JSON file ``cache_path`` is applied
     without timing.  Otherwise every candidate (ctas, threads_per_cta) --
     by default the automatic shape, the automatic CTA count with 320 and 480
     threads, and a half-size team -- is timed over ``repeats`` ratio solves
@@ -346,7 +379,8 @@ def autotune(gen: "product_graph_generator", max_depth: int | None = None, candi
     def p2(x):
         return 1 << max(0, int(x) - 1).bit_length()
 
-    key = f"n{p2(info['nodes_per_layer'])}-l{p2(info['layers'])}-k{k}-intra{int(info['intra_edges_per_layer'] > 0)}"
+    key = (f"{gen.device_name()}|n{p2(info['nodes_per_layer'])}-l{p2(info['layers'])}-k{k}"
+           f"-intra{int(info['intra_edges_per_layer'] > 0)}")
     cache = {}
     if cache_path and os.path.exists(cache_path):
         with open(cache_path) as f:
@@ -404,6 +438,13 @@ def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas
     threads (0: 64); with
     ``regenerate`` each first recomputes its edge costs.  Returns the list of
     ``(passes_layers_just_once, final_objective, matching)`` triples.
+
+    The device runs the graphs' streams side by side only as far as it has
+    host work queues: CUDA's default is 8, and a process started with
+    ``CUDA_DEVICE_MAX_CONNECTIONS=32`` (read when CUDA initialises) runs a
+    batch about 3x faster.  The package does not set it: that is the
+    application's choice, since it changes how all of the process's streams
+    share the device.
     """
     gens = list(generators)
     if len(set(id(g) for g in gens)) != len(gens):

@@ -105,7 +105,17 @@ def vertex_normals(V: np.ndarray, F: np.ndarray) -> np.ndarray:
     N = np.zeros_like(V)
     for k in range(3):
         np.add.at(N, F[:, k], fn)
-    return N / np.linalg.norm(N, axis=1, keepdims=True)
+    return _unit_rows(N, "mesh vertex")
+
+
+def _unit_rows(N: np.ndarray, what: str) -> np.ndarray:
+    """Rows of N scaled to unit length; a zero (or non-finite) row has no
+    direction, so it is refused instead of turning into NaN."""
+    length = np.linalg.norm(N, axis=1, keepdims=True)
+    bad = ~(np.isfinite(length[:, 0]) & (length[:, 0] > 1e-300))
+    if bad.any():
+        raise ValueError(f"degenerate input: the {what} normal of row {int(np.flatnonzero(bad)[0])} has no direction")
+    return N / length
 
 
 def normals_2d(V: np.ndarray, E: np.ndarray) -> np.ndarray:
@@ -142,7 +152,7 @@ def normals_2d(V: np.ndarray, E: np.ndarray) -> np.ndarray:
     for i in range(1, m + 1):
         j = i % m
         vn[j] = el[i - 1] * en[i - 1] + el[j] * en[j]
-    return vn / np.linalg.norm(vn, axis=1, keepdims=True)
+    return _unit_rows(vn, "curve vertex")
 
 
 def silhouette_curve(VX: np.ndarray, m: int):
@@ -168,8 +178,14 @@ def silhouette_curve(VX: np.ndarray, m: int):
 
 def make_pair(n_vertices: int = 642, n_curve: int = 60, feat_dim: int = 32, seed: int = 0, amp: float = 0.1,
               feat_noise: float = 0.05, icosphere_level: int | None = None, smooth_iters: int = 4,
-              with_normals: bool = True):
-    """Return a dict with VX, EX, VY, EY, feat_diff (and NX, NY) for one synthetic pair."""
+              with_normals: bool | None = None):
+    """Return a dict with VX, EX, VY, EY, feat_diff (and NX, NY) for one synthetic pair.
+
+    `with_normals` None gives normals when the curve has at least three
+    points: a two-point curve runs back along itself, so its vertex normals
+    cancel and have no direction (asking for them then raises ValueError)."""
+    if with_normals is None:
+        with_normals = n_curve >= 3
     rng = np.random.default_rng(seed)
     if icosphere_level is not None:
         V, F = icosphere(icosphere_level)

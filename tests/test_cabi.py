@@ -120,6 +120,7 @@ _HANDLE_CALLS = [
     ("pgc_result_profile", [ctypes.c_void_p]),
     ("pgc_result_profile_detail", [ctypes.c_void_p]),
     ("pgc_graph_info", [ctypes.c_void_p]),
+    ("pgc_device_name", [ctypes.c_char_p, ctypes.c_int64]),
 ]
 
 

@@ -17,7 +17,11 @@ def test_sizes_match_the_oracle_product_space(cpg, oracle, conj, prune, level, n
     got = cpg.product_graph_sizes(p["EX"], len(p["VX"]), len(p["EY"]), conj, prune)
     o = oracle.OracleGenerator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], conj, False, prune)
     if conj:
-        o.set_normals(p["NX"], p["NY"])
+        # the product space does not read the normals; a two-point curve has
+        # none (its vertex normals cancel), so any unit rows do here
+        nx = p.get("NX", np.tile([0.0, 0.0, 1.0], (len(p["VX"]), 1)))
+        ny_ = p.get("NY", np.tile([1.0, 0.0, 0.0], (len(p["VY"]), 1)))
+        o.set_normals(nx, ny_)
     ps = o.get_product_space()
     assert got["edges"] == ps.shape[0]
     assert got["nodes_per_layer"] == (3 * len(p["EX"]) if conj else len(p["VX"]))

@@ -78,6 +78,37 @@ def test_noalloc_export_matches_existing_entry_point(cpg, conj):
     assert not np.array_equal(before, after)
 
 
+def test_noalloc_export_pruned_graph(cpg):
+    """Pruned graphs have no intralayer edges: the export must still write
+    every value of the smaller edge blocks, into a NaN-filled buffer."""
+    lib = _abi(cpg)
+    from cyclic_product_graphs import synthetic
+
+    for conj in (False, True):
+        p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=5)
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], conj, False, True)
+        if conj:
+            g.set_normals(p["NX"], p["NY"])
+            g.set_cost_time_ratio_mode("vanilla", "lengthnormalisation")
+        g.generate()
+        ref = _check_two_in_a_row(lib, g)
+        assert np.isfinite(ref).all()
+
+
+@pytest.mark.parametrize("conj", [False, True])
+def test_noalloc_export_of_imported_costs(cpg, conj):
+    """Costs set with pgc_set_cost_vector instead of generated: the export
+    returns exactly the imported matrix, every value finite."""
+    lib = _abi(cpg)
+    g = _graph(cpg, conj, seed=7)
+    rows, cols = g.get_cost_vector().shape
+    rng = np.random.default_rng(3)
+    costs = rng.integers(1, 1000, size=(rows, cols)).astype(np.float64)
+    g.set_cost_vector(costs)
+    ref = _check_two_in_a_row(lib, g)
+    assert np.array_equal(ref, costs)
+
+
 def test_noalloc_export_alternates_between_graphs(cpg):
     lib = _abi(cpg)
     a, b = _graph(cpg, False, seed=1), _graph(cpg, True, seed=2)
