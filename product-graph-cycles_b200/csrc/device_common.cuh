@@ -35,7 +35,7 @@ struct Control {
     int epoch;           // monotone sweep counter (improve flags)
     int numInBranch;
     int indexNodeInLayer;
-    int walkId;          // monotone id for visited marks of literal walks
+    int walkRounds;      // rounds of the bounded parallel literal walks (statistics)
     int v0;              // first repeated layer-0 node of the detected cycle
     long long cLength;   // steps the reference's walk needs to detect it
     int cycleLen;        // entries written to the cycle buffer
@@ -44,7 +44,11 @@ struct Control {
     long long candidates;  // candidates decided (for statistics)
     unsigned barCount;
     unsigned barGen;
-    int pad[2];
+    // A word no code writes (the host zeroes it before each launch).  The
+    // wait-timeout test makes one CTA's step hand-off also wait for it to
+    // reach the step number, so that wait runs out.
+    unsigned neverSet;
+    int pad;
     // SM cycles seen by CTA 0's thread 0 (profiling counters): relaxation,
     // sweep bookkeeping, step hand-offs / barriers, sweep tail
     unsigned long long cycPhaseA, cycPhaseB, cycSync, cycTail;
@@ -60,6 +64,16 @@ struct Control {
     double validLb;
     int validV;
     int anyFinite;
+};
+
+// State of one bounded literal walk (the reference's predecessor walk from a
+// candidate, cost_time_ratio_solver.cpp:461-488), advanced a bounded number
+// of predecessor loads per round so that no team barrier waits long.
+struct LiteralWalk {
+    int phase;        // 0 idle/done, 1 cycle length (Brent), 2 offset hare, 3 tail length, 4 first start node
+    int a, b;         // tortoise and hare (expanded node ids)
+    int pad;
+    long long c1, c2, c3;
 };
 
 struct BfParams {
@@ -90,7 +104,7 @@ struct BfParams {
     int stageSrcOnly;              // 1: the buffers hold source indices only (costs, times prefetched to L2)
     int* lapNext;                  // [n]
     int* lapSteps;                 // [n]
-    int* mark;                     // [n] visited marks for literal walks
+    LiteralWalk* walks;            // [n] state of the bounded literal walks
     int* candStat;                 // [n] shortcut verdict per candidate (0 none, 1 cycle, 2 no cycle, 3 undecided)
     int* candV0;                   // [n] first repeated layer-0 node of a candidate's walk
     long long* candSteps;          // [n] predecessor steps that walk needs
@@ -100,6 +114,9 @@ struct BfParams {
     double lambda, ub;
     int mode;                      // 0 ratio, 1 ratio upper-bound search, 2 minimum cost
     int maxSweeps;                 // safety cap on sweeps in one launch (0 = unlimited)
+    unsigned spinLimit;            // polls of any wait before it gives up and raises the error word
+    int stallCta;                  // test hook (-1: none): this CTA's hand-off also waits on ctl->neverSet
+    int literalAll;                // test hook: decide every candidate by the literal walk
     Control* ctl;
     int* cycleBuf;                 // original node ids, walk order (reversed on the host)
     long long cycleCap;
@@ -196,6 +213,10 @@ struct LookupArgs {
 };
 
 constexpr int kStepDoneStride = 8;  // one 32-byte sector per CTA step counter
+// Polls of a device wait before it gives up (~2 s with its back-off).
+constexpr unsigned kDefaultSpinLimit = 1u << 24;
+// Predecessor loads a literal walk advances per round between team barriers.
+constexpr long long kWalkRoundLoads = 4096;
 // Most threads per Bellman-Ford CTA: 20 warps fit the kernel's registers
 // (about 100 per thread) on one SM without spilling the relaxation loop.
 constexpr int kBfThreads = 640;

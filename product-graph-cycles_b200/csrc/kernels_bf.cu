@@ -33,7 +33,10 @@
 // is decided with Brent's cycle-finding algorithm on that lap function; the
 // candidate with the smallest (value, index) whose walk repeats within the
 // reference's step limit wins.  When a lap cannot be derived from the
-// current sweep (a stale predecessor), that candidate is re-walked literally.
+// current sweep (a stale predecessor), that candidate is re-walked literally:
+// all such candidates at once, each by cycle finding on the predecessor
+// function, advanced a bounded number of loads per round between team
+// barriers.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,13 +47,12 @@ namespace pgc {
 
 namespace {
 
-constexpr unsigned kSpinLimit = 1u << 24;  // ~2 s of polling at most
-
 struct Team {
     int cta, ncta;
     unsigned* cnt;
     unsigned* gen;
     int* err;
+    unsigned spin;  // polls of a wait before it gives up
     __device__ long long thread() const { return (long long)cta * blockDim.x + threadIdx.x; }
     __device__ long long nthreads() const { return (long long)ncta * blockDim.x; }
 };
@@ -97,7 +99,7 @@ __device__ int team_sync_or(const Team& t, int flag, bool& ok) {
                 unsigned spins = 0, cur;
                 while ((cur = ld_acquire_u32(t.gen)) == g) {
                     ++spins;
-                    if (spins > kSpinLimit || ((spins & 63u) == 0 && *(volatile int*)t.err)) {
+                    if (spins > t.spin || ((spins & 63u) == 0 && *(volatile int*)t.err)) {
                         atomicExch(t.err, 1);
                         good = 0;
                         break;
@@ -247,8 +249,8 @@ __device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned by
                  : "memory");
 }
 // One bounded wait for the phase with the given parity; true when it completed.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-    for (unsigned spins = 0; spins < kSpinLimit; ++spins) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned limit) {
+    for (unsigned spins = 0; spins < limit; ++spins) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred P;\n\t"
@@ -291,6 +293,7 @@ struct Stage {
     unsigned phase;              // bit b: parity of buffer b's next completion
     unsigned pending;            // bit b: copies issued into buffer b, not yet waited for
     int costBytes, timeBytes;    // bytes per entry of the cost and time streams
+    unsigned spin;               // polls of a copy wait before it gives up
     __device__ const int* spl(int part) const { return part ? splIntra : splInter; }
     __device__ const int* act(int part) const { return part ? actIntra : actInter; }
     __device__ int nAct(int part) const { return part ? nActIntra : nActInter; }
@@ -337,7 +340,7 @@ __device__ void stage_issue(const BfParams& p, Stage& st, int s0, int s1, int b,
 // Wait for buffer b if copies were issued into it (every thread).
 __device__ __forceinline__ bool stage_wait(Stage& st, int b) {
     if (!((st.pending >> b) & 1u)) return true;
-    const bool ok = mbar_wait(st.bar + b, (st.phase >> b) & 1u);
+    const bool ok = mbar_wait(st.bar + b, (st.phase >> b) & 1u, st.spin);
     st.phase ^= 1u << b;
     st.pending &= ~(1u << b);
     return ok;
@@ -576,7 +579,9 @@ __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, i
 // list (the owners of the sources it reads and the readers of the rows it
 // overwrites next) has completed it too.  This replaces a grid-wide barrier:
 // a CTA waits only for its graph neighbours.  Returns false when a wait ran
-// out of iterations or another CTA raised the error word.
+// out of iterations or another CTA raised the error word.  The CTA named by
+// p.stallCta (a test hook; -1 in every solve) also waits for a word that no
+// code writes, so its wait runs out.
 __device__ bool step_handoff(const BfParams& p, const Team& t, unsigned step) {
     __syncthreads();  // the CTA's writes of this step are done
     if (threadIdx.x < 32) {
@@ -585,17 +590,19 @@ __device__ bool step_handoff(const BfParams& p, const Team& t, unsigned step) {
         if (threadIdx.x == 0) st_release_u32(p.stepDone + (size_t)t.cta * kStepDoneStride, step);
         __syncwarp();
         const int w0 = __ldg(p.waitPtr + t.cta), w1 = __ldg(p.waitPtr + t.cta + 1);
+        const bool stall = t.cta == p.stallCta;
         int good = 1;
-        for (int i0 = w0; i0 < w1 && good; i0 += 32) {
+        for (int i0 = w0; i0 < w1 + (stall ? 1 : 0) && good; i0 += 32) {
             const int i = i0 + (int)threadIdx.x;
-            const unsigned* f = i < w1 ? p.stepDone + (size_t)__ldg(p.waitIdx + i) * kStepDoneStride : nullptr;
+            const unsigned* f = i < w1 ? p.stepDone + (size_t)__ldg(p.waitIdx + i) * kStepDoneStride
+                                       : (stall && i == w1) ? &p.ctl->neverSet : nullptr;
             unsigned spins = 0;
             for (;;) {
                 const bool ready = f == nullptr || (int)(ld_acquire_u32(f) - step) >= 0;
                 if (__all_sync(0xffffffffu, ready)) break;
                 ++spins;
                 if ((spins & 63u) == 0 && *(volatile int*)t.err) { good = 0; break; }
-                if (spins > kSpinLimit) {
+                if (spins > t.spin) {
                     if (threadIdx.x == 0) atomicExch(t.err, 1);
                     good = 0;
                     break;
@@ -648,27 +655,106 @@ __device__ int lap_walk(const BfParams& p, int x0, long long limit, int* v0, lon
     return 1;
 }
 
-// The reference's walk (cost_time_ratio_solver.cpp:461-488) for one
-// candidate, marking layer-0 start nodes with a walk id instead of clearing
-// a boolean column.
-__device__ int literal_walk(const BfParams& p, int vi, long long maxLen, int* v0, long long* steps) {
-    const int id = ++p.ctl->walkId;
-    const int n = p.n;
-    const long long total = (long long)n * (p.nY + 1) * p.K;
-    int pr = __ldcg(p.pred + vi);
-    p.mark[vi] = id;
-    long long len = 1;
-    for (long long kk = maxLen - 1; kk > 0; --kk) {
-        if (pr < n && pr >= 0) {
-            if (p.mark[pr] == id) { *v0 = pr; *steps = len; return 1; }
-            p.mark[pr] = id;
-        }
-        if (pr < 0 || pr >= total) return 2;
-        pr = __ldcg(p.pred + pr);
-        if (pr == -1) return 2;
-        ++len;
+// The reference's walk from candidate vi (cost_time_ratio_solver.cpp:461-488):
+// x_0 = vi, x_(j+1) = pred[x_j]; it stops at the first j in [1, maxLen - 1]
+// where x_j is a layer-0 start node (x_j < n) seen before in the walk (vi
+// included), and fails when a predecessor leaves the node range (-1
+// included) or the limit passes.  Since pred is a function, the walk repeats
+// only once it is periodic: with tail mu and cycle length lam, that first
+// repeated start node is x_(mu + lam + d), d the offset of the first start
+// node on the cycle from x_mu.  So the walk is decided by Brent's cycle
+// finding (lam), two pointers lam apart (mu) and a walk round the cycle (d),
+// about (3 mu + 5 lam) loads and no visited marks, so every undecided
+// candidate walks at once.  A walk advances at most `budget` loads per call
+// and keeps its state in p.walks[i]; it returns true once decided, with
+// candStat[i] = 1 (candV0[i] = x_j, candSteps[i] = j) or 2.
+__device__ void walk_start(const BfParams& p, int i) {
+    const long long total = (long long)p.n * (p.nY + 1) * p.K;
+    LiteralWalk w{};
+    w.phase = 1;
+    w.a = i;
+    w.b = __ldcg(p.pred + i);
+    w.c1 = 1;  // power
+    w.c2 = 1;  // lam
+    w.c3 = 1;  // position of the hare
+    if (w.b < 0 || (long long)w.b >= total) {
+        w.phase = 0;
+        p.candStat[i] = 2;
     }
-    return 2;
+    p.walks[i] = w;
+}
+
+__device__ bool walk_advance(const BfParams& p, int i, long long budget) {
+    LiteralWalk w = p.walks[i];
+    if (w.phase == 0) return true;
+    const long long total = (long long)p.n * (p.nY + 1) * p.K;
+    const long long maxLen = p.numNodes;
+    int verdict = 0;  // 1 found, 2 failed
+    while (budget > 0 && verdict == 0) {
+        if (w.phase == 1) {  // Brent: the cycle length lam (c2); c1 power, c3 hare position
+            if (w.a == w.b) {
+                w.phase = 2;
+                w.c1 = w.c2;  // lam
+                w.c2 = w.c2;  // loads left to put the hare lam steps ahead of x_0
+                w.a = i;
+                w.b = i;
+                continue;
+            }
+            if (w.c1 == w.c2) {
+                w.a = w.b;
+                w.c1 <<= 1;
+                w.c2 = 0;
+            }
+            w.b = __ldcg(p.pred + w.b);
+            --budget;
+            ++w.c2;
+            ++w.c3;
+            // out of range: the walk ends without a repeat; past 3 maxLen loads
+            // the tail and cycle exceed maxLen, so no repeat within the limit
+            if (w.b < 0 || (long long)w.b >= total || w.c3 > 3 * maxLen + 8) verdict = 2;
+        } else if (w.phase == 2) {  // hare lam steps ahead of x_0
+            if (w.c2 == 0) {
+                w.phase = 3;
+                continue;  // c2 now counts the tail length mu
+            }
+            w.b = __ldcg(p.pred + w.b);
+            --budget;
+            --w.c2;
+        } else if (w.phase == 3) {  // both pointers until they meet at x_mu
+            if (w.a == w.b) {
+                w.phase = 4;
+                w.c3 = 0;  // d
+                continue;
+            }
+            w.a = __ldcg(p.pred + w.a);
+            w.b = __ldcg(p.pred + w.b);
+            budget -= 2;
+            ++w.c2;
+        } else {  // round the cycle from x_mu to its first start node
+            if (w.a < p.n) {
+                const long long j = w.c2 + w.c1 + w.c3;
+                if (j <= maxLen - 1) {
+                    p.candV0[i] = w.a;
+                    p.candSteps[i] = j;
+                    verdict = 1;
+                } else {
+                    verdict = 2;
+                }
+            } else if (w.c3 + 1 >= w.c1) {
+                verdict = 2;  // no start node on the cycle: no repeat is ever seen
+            } else {
+                w.a = __ldcg(p.pred + w.a);
+                --budget;
+                ++w.c3;
+            }
+        }
+    }
+    if (verdict) {
+        w.phase = 0;
+        p.candStat[i] = verdict;
+    }
+    p.walks[i] = w;
+    return verdict != 0;
 }
 
 // Collects the cycle that closes at v0 (cost_time_ratio_solver.cpp:494-503):
@@ -780,7 +866,7 @@ __device__ int dij_walk_end(const BfParams& p, int v) {
 // ---------------------------------------------------------------------------
 template <class CT, int TK, bool S>
 __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
-    Team t{(int)blockIdx.x, (int)gridDim.x, &p.ctl->barCount, &p.ctl->barGen, &p.ctl->error};
+    Team t{(int)blockIdx.x, (int)gridDim.x, &p.ctl->barCount, &p.ctl->barGen, &p.ctl->error, p.spinLimit};
     const int n = p.n, K = p.K, Kp = p.Kp;
     const long long tid = t.thread(), nth = t.nthreads();
     const bool isLead = (blockIdx.x == 0 && threadIdx.x == 0);
@@ -837,6 +923,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         st.timeBytes = TK == 1 ? 4 : TK == 2 ? 8 : 0;
         st.rowCap = p.rowCap;
         st.srcOnly = p.stageSrcOnly != 0;
+        st.spin = p.spinLimit;
         const size_t bufBytes =
             bf_stage_buffer_bytes(p.rowCap, st.srcOnly ? 0 : st.costBytes, st.srcOnly ? 0 : st.timeBytes);
         st.buf0 = smem + bf_stage_offset(p.maxCtaSlices);
@@ -1090,7 +1177,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                     if (d0 < 0) {
                         int v0 = -1;
                         long long steps = 0;
-                        st = lap_walk(p, (int)i, limit, &v0, &steps);
+                        st = p.literalAll ? 3 : lap_walk(p, (int)i, limit, &v0, &steps);
                         p.candV0[i] = v0;
                         p.candSteps[i] = steps;
                         ++decided;
@@ -1119,54 +1206,85 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         }
         __shared__ int sLaps, sBad;
         __shared__ long long sCycLen;
+        __shared__ Key sOk, sUnk;
         const unsigned long long tCand = isLead ? clock64() : 0;
         if (!team_sync(t)) return;
-        const unsigned long long tLead = isLead ? clock64() : 0;
-        if (isLead) atomicAdd(&p.ctl->cycCand, tLead - tCand);
-        int finished = 0;
-        if (isLead) {
+        // Every CTA reads the team's best decided candidate and its first
+        // undecided one.  Undecided candidates that precede the best decided
+        // one are walked literally, all at once, in bounded rounds; then the
+        // smallest (value, index) candidate whose walk repeats wins, which is
+        // what the reference's walks in ascending order choose.
+        if (threadIdx.x == 0) {
             Key ok{kInfD, 0x7fffffff}, unk{kInfD, 0x7fffffff};
-            long long dec = 0;
             for (int c = 0; c < t.ncta; ++c) {
                 Key a{__ldcg(p.redVal + 2 * c), __ldcg(p.redIdx + 2 * c)};
                 Key b{__ldcg(p.redVal + 2 * c + 1), __ldcg(p.redIdx + 2 * c + 1)};
                 if (key_less(a, ok)) ok = a;
                 if (key_less(b, unk)) unk = b;
-                dec += __ldcg(p.redAux64 + c);
             }
+            sOk = ok;
+            sUnk = unk;
+        }
+        __syncthreads();
+        Key ok = sOk;
+        const Key unk = sUnk;
+        if (unk.i != 0x7fffffff && (ok.i == 0x7fffffff || key_less(unk, ok))) {
+            int started = 0;
+            for (long long i = tid; i < n; i += nth) {
+                if (__ldcg(p.candStat + i) != 3) continue;
+                const Key kk{ldV<S>(p, (size_t)i * Kp), (int)i};
+                if (!key_less(kk, ok)) {
+                    p.candStat[i] = 0;  // follows the best decided candidate: never reached
+                    continue;
+                }
+                walk_start(p, (int)i);
+                ++started;
+            }
+            for (int o = 16; o > 0; o >>= 1) started += __shfl_xor_sync(0xffffffffu, started, o);
+            if ((threadIdx.x & 31) == 0 && started) atomicAdd(&p.ctl->fallbackWalks, started);
+            for (int round = 0;; ++round) {
+                int pending = 0;
+                for (long long i = tid; i < n; i += nth)
+                    if (__ldcg(p.candStat + i) == 3 && !walk_advance(p, (int)i, kWalkRoundLoads)) pending = 1;
+                bool good;
+                pending = team_sync_or(t, pending, good);
+                if (!good) return;
+                if (isLead) p.ctl->walkRounds = round + 1;
+                if (!pending) break;
+            }
+            Key best{kInfD, 0x7fffffff};
+            for (long long i = tid; i < n; i += nth) {
+                if (__ldcg(p.candStat + i) != 1) continue;
+                const Key kk{ldV<S>(p, (size_t)i * Kp), (int)i};
+                if (key_less(kk, best)) best = kk;
+            }
+            best = block_min(best, 0);
+            if (threadIdx.x == 0) {
+                p.redVal[2 * blockIdx.x] = best.v;
+                p.redIdx[2 * blockIdx.x] = best.i;
+            }
+            if (!team_sync(t)) return;
+            if (isLead) {
+                ok = Key{kInfD, 0x7fffffff};
+                for (int c = 0; c < t.ncta; ++c) {
+                    Key a{__ldcg(p.redVal + 2 * c), __ldcg(p.redIdx + 2 * c)};
+                    if (key_less(a, ok)) ok = a;
+                }
+            }
+        }
+        const unsigned long long tLead = isLead ? clock64() : 0;
+        if (isLead) atomicAdd(&p.ctl->cycCand, tLead - tCand);
+        int finished = 0;
+        if (isLead) {
+            long long dec = 0;
+            for (int c = 0; c < t.ncta; ++c) dec += __ldcg(p.redAux64 + c);
             p.ctl->candidates += dec;
             int winner = -1, v0 = -1;
             long long steps = 0;
-            if (ok.i != 0x7fffffff && (unk.i == 0x7fffffff || key_less(ok, unk))) {
+            if (ok.i != 0x7fffffff) {
                 winner = ok.i;
                 v0 = __ldcg(p.candV0 + winner);
                 steps = __ldcg(p.candSteps + winner);
-            } else if (unk.i != 0x7fffffff) {
-                // Resolve in ascending (value, index) order; literal walks only
-                // for the undecidable candidates.
-                Key prev{-kInfD, -1};
-                for (;;) {
-                    Key next{kInfD, 0x7fffffff};
-                    for (int i = 0; i < n; ++i) {
-                        const int st = __ldcg(p.candStat + i);
-                        if (st == 0) continue;
-                        Key kk{ldV<S>(p, (size_t)i * Kp), i};
-                        if (key_less(prev, kk) && key_less(kk, next)) next = kk;
-                    }
-                    if (next.i == 0x7fffffff) break;
-                    prev = next;
-                    const int st = __ldcg(p.candStat + next.i);
-                    if (st == 1) {
-                        winner = next.i;
-                        v0 = __ldcg(p.candV0 + winner);
-                        steps = __ldcg(p.candSteps + winner);
-                        break;
-                    }
-                    if (st == 3) {
-                        p.ctl->fallbackWalks++;
-                        if (literal_walk(p, next.i, numNodes, &v0, &steps) == 1) { winner = next.i; break; }
-                    }
-                }
             }
             sLaps = 0;
             if (winner >= 0) {
@@ -1218,10 +1336,10 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             finished = p.ctl->status != BF_RUNNING;
             atomicAdd(&p.ctl->cycLead, clock64() - tLead);
         }
-        bool ok;
-        finished = team_sync_or(t, finished, ok);
+        bool tailOk;
+        finished = team_sync_or(t, finished, tailOk);
         if (isLead) atomicAdd(&p.ctl->cycTail, clock64() - tTail);
-        if (!ok || finished) return;
+        if (!tailOk || finished) return;
     }
 }
 

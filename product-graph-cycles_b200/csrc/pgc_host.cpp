@@ -333,13 +333,14 @@ class Graph {
     mutable std::map<std::string, std::vector<int>> cutCache;  // cta_cuts per (blocks, K, warps)
     int cutBlocks = -1, cutK = -1, cutWarps = -1;  // the partition ctaCut was made for
     long long waitEntries = 0;  // wait-list entries over all CTAs of the current partition
-    DBuf<int> wPred, wLapNext, wLapSteps, wMark, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
+    DBuf<int> wPred, wLapNext, wLapSteps, wCandStat, wCandV0, wLayerFlag, wBranch, wCycle,
         wRedIdx, wRedAux, wOrigin, wPairS, wPairT, wCount;
+    DBuf<LiteralWalk> wWalks;
     DBuf<long long> wCandSteps, wRedAux64, wEdgeOut;
     DBuf<float> wMean;
     DBuf<Control> wCtl;
     int wsK = -1;
-    int ctlEpoch = 0, ctlWalkId = 0;
+    int ctlEpoch = 0;
     int teamCap = 0;  // most CTAs of a Bellman-Ford launch (0: as many as help)
     // team shape chosen for this graph (pgc_set_team_shape; 0: automatic);
     // the PGC_BF_BLOCKS / PGC_BF_THREADS environment overrides take precedence
@@ -972,9 +973,7 @@ void Graph::ensure_workspace(int K, int blocks) {
         wBak.alloc(n);
         wLapNext.alloc(n);
         wLapSteps.alloc(n);
-        wMark.alloc(n);
-        wMark.zero(stream);
-        ctlWalkId = 0;
+        wWalks.alloc(n);
         wCandStat.alloc(n);
         wCandV0.alloc(n);
         wCandSteps.alloc(n);
@@ -1036,7 +1035,7 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.stageSrcOnly = r.stageSrcOnly;
     p.lapNext = wLapNext.p;
     p.lapSteps = wLapSteps.p;
-    p.mark = wMark.p;
+    p.walks = wWalks.p;
     p.candStat = wCandStat.p;
     p.candV0 = wCandV0.p;
     p.candSteps = wCandSteps.p;
@@ -1047,6 +1046,14 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.ub = ub;
     p.mode = mode;
     p.maxSweeps = 0;
+    // device waits give up after this many polls (PGC_BF_SPIN_LIMIT: tests
+    // of the timeout path use a short one); two test hooks, off in every
+    // solve: PGC_BF_TEST_STALL_CTA makes that CTA's step hand-off also wait
+    // for a word no code writes, and PGC_BF_LITERAL_WALKS=1 decides every
+    // candidate by the literal predecessor walk
+    p.spinLimit = (unsigned)std::max(1, env_int("PGC_BF_SPIN_LIMIT", (int)kDefaultSpinLimit));
+    p.stallCta = env_int("PGC_BF_TEST_STALL_CTA", -1);
+    p.literalAll = env_int("PGC_BF_LITERAL_WALKS", 0) ? 1 : 0;
     p.ctl = wCtl.p;
     p.cycleBuf = wCycle.p;
     p.cycleCap = (long long)wCycle.n;
@@ -1062,7 +1069,6 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
 Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     Control c{};
     c.epoch = ctlEpoch;
-    c.walkId = ctlWalkId;
     PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
     if (!timeEvents[0]) {
         PGC_CUDA(cudaEventCreate(&timeEvents[0]));
@@ -1079,7 +1085,6 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     cudaEventElapsedTime(&ms, e0, e1);
     stats.deviceMs += ms;
     ctlEpoch = c.epoch;
-    ctlWalkId = c.walkId;
     stats.bfCalls++;
     stats.sweeps += c.sweeps;
     stats.candidates += c.candidates;
@@ -1096,7 +1101,16 @@ Control Graph::launch_bf_call(const Run& r, const BfParams& p) {
     stats.ctas = r.blocks;
     stats.threads = r.threads;
     stats.waitEntries = r.blocks > 1 ? waitEntries : 0;
-    if (c.error) throw Failure(PGC_ERR_TIMEOUT, "a wait of the Bellman-Ford kernel (team barrier, step hand-off or staged copy) ran out");
+    if (c.error) {
+        // The launch stopped mid-sweep: layers it stamped carry stamps the
+        // next launch would issue again.  Clear them, so the handle solves
+        // correctly afterwards.
+        wLayerFlag.zero(stream);
+        ctlEpoch = 0;
+        PGC_CUDA(sync_stream());
+        throw Failure(PGC_ERR_TIMEOUT,
+                      "a wait of the Bellman-Ford kernel (team barrier, step hand-off or staged copy) ran out");
+    }
     if (c.status == BF_ERR_EMPTY_BRANCH) throw Failure(PGC_ERR_INTERNAL, "no nodes in branch");
     if (c.status == BF_ERR_CYCLE_CAP) throw Failure(PGC_ERR_INTERNAL, "cycle longer than its buffer");
     if (c.status == BF_ERR_WALK) throw Failure(PGC_ERR_INTERNAL, "predecessor walk left the node range");
@@ -1473,7 +1487,6 @@ void Graph::solve_min_cost(int K) {
         BfParams p = params(r, 2, branchId, 0.0, upperBound);
         Control c{};
         c.epoch = ctlEpoch;
-        c.walkId = ctlWalkId;
         PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
         PGC_CUDA(launch_extract_path(p, v, stream));
         stats.launches++;
