@@ -171,6 +171,15 @@ int pgc_set_team_shape(pgc_graph* g, int ctas, int threads_per_cta);
 int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver_name, int max_depth,
                     int ctas_per_graph, int workers, int regenerate, int* status);
 
+/* No reference counterpart.  Where the calling thread's last
+ * pgc_solve_batch spent its time (host wall clock, ms) when it solved ratio
+ * cycles in one launch: out8 = {costs generated and rescaled, teams
+ * prepared; the launch and its results read back; results taken over or
+ * finished on the host; graphs handed back to the host; graphs solved on the
+ * device; CTAs launched; threads per CTA; dynamic shared memory per CTA}.
+ * All zero after the per-graph-stream route. */
+int pgc_batch_profile(double* out8);
+
 /* The CTR_CYCLE_SOLVER_OUTPUT / DIJKSTRA_SOLVER_OUTPUT tuple
  * (cost_time_ratio_solver.hpp:70, dijkstra_solver.hpp:22) of the last solve. */
 int pgc_result(pgc_graph* g, int* passes_layers_just_once, float* final_objective, int64_t* rows, int64_t* cols);

@@ -45,6 +45,8 @@ def lib():
         L.orc_generate.argtypes = [ctypes.c_void_p]
         L.orc_ensure_generated.argtypes = [ctypes.c_void_p]
         L.orc_recompute_energy.argtypes = [ctypes.c_void_p]
+        L.orc_normals_2d.argtypes = [_dp, _i64, _ip, _i64, _dp]
+        L.orc_normals_3d.argtypes = [_dp, _i64, _ip, _i64, _dp]
         L.orc_cost_shape.argtypes = [ctypes.c_void_p, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]
         L.orc_get_cost.argtypes = [ctypes.c_void_p, _dp]
         L.orc_set_cost.argtypes = [ctypes.c_void_p, _dp, _i64, _i64]
@@ -69,6 +71,29 @@ def lib():
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
+
+
+def normals_2d(V, E):
+    """utils::normals2d restated (helper/utils.cpp:93-157)."""
+    V, E = _d(V), _i(E)
+    out = np.empty_like(V)
+    rc = lib().orc_normals_2d(V.ctypes.data_as(_dp), V.shape[0], E.ctypes.data_as(_ip), E.shape[0],
+                              out.ctypes.data_as(_dp))
+    if rc == -2:
+        raise ValueError("V.rows() != E.rows()")
+    if rc != 0:
+        raise ValueError("points dont lie on xy, xz or yz plane")
+    return out
+
+
+def normals_3d(V, F):
+    """utils::normals3d restated (helper/utils.cpp:86-90, libigl area weighting)."""
+    V, F = _d(V), _i(F)
+    out = np.empty_like(V)
+    if lib().orc_normals_3d(V.ctypes.data_as(_dp), V.shape[0], F.ctypes.data_as(_ip), F.shape[0],
+                            out.ctypes.data_as(_dp)) != 0:
+        raise ValueError("F refers to a vertex outside V")
+    return out
 
 
 def _d(a):

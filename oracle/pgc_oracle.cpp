@@ -1550,6 +1550,92 @@ void orc_get_src_trgt(void* h, int* src, int* trgt) {
     std::memcpy(trgt, G->g.trgt.data(), sizeof(int) * G->g.trgt.size());
 }
 
+// utils::normals2d (helper/utils.cpp:93-157): outward vertex normals of an
+// ordered closed curve in a coordinate plane.  The plane is the first
+// coordinate column whose sum is below 1e-4 in magnitude; edge normals are
+// the edge vectors rotated about z, flipped when the float-rounded test of
+// :120-133 finds them pointing inward; a vertex normal is the length-weighted
+// sum of the normals of the edges ending and starting at it.  Returns 0, or
+// -1 when the points lie in no coordinate plane.
+int orc_normals_2d(const double* Vin, long long nv, const int* E, long long ne, double* out) {
+    if (nv != ne) return -2;
+    std::vector<double> V(Vin, Vin + 3 * nv);
+    int zero = -1;
+    for (int i = 0; i < 3; ++i) {
+        double s = 0;
+        for (long long r = 0; r < nv; ++r) s += V[(size_t)(3 * r + i)];
+        if (std::fabs(s) < 1e-4) { zero = i; break; }
+    }
+    if (zero == -1) return -1;
+    if (zero != 2) {
+        const int order[3] = {zero == 1 ? 0 : 1, 2, zero == 1 ? 1 : 0};
+        std::vector<double> W(V.size());
+        for (long long r = 0; r < nv; ++r)
+            for (int k = 0; k < 3; ++k) W[(size_t)(3 * r + k)] = V[(size_t)(3 * r + order[k])];
+        V.swap(W);
+    }
+    std::vector<double> en((size_t)(3 * ne)), el((size_t)ne);
+    for (long long i = 0; i < ne; ++i) {
+        const int a = E[2 * i], b = E[2 * i + 1];
+        const double ev[3] = {V[(size_t)(3 * a)] - V[(size_t)(3 * b)], V[(size_t)(3 * a + 1)] - V[(size_t)(3 * b + 1)],
+                              V[(size_t)(3 * a + 2)] - V[(size_t)(3 * b + 2)]};
+        el[(size_t)i] = std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
+        const double nrm[3] = {ev[1], -ev[0], ev[2]};  // rotation about z
+        const double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        for (int k = 0; k < 3; ++k) en[(size_t)(3 * i + k)] = len > 0 ? nrm[k] / len : nrm[k];
+    }
+    double mx = -INFINITY, mn = INFINITY, my = -INFINITY, mny = INFINITY;
+    for (long long r = 0; r < nv; ++r) {
+        mx = std::max(mx, V[(size_t)(3 * r)]); mn = std::min(mn, V[(size_t)(3 * r)]);
+        my = std::max(my, V[(size_t)(3 * r + 1)]); mny = std::min(mny, V[(size_t)(3 * r + 1)]);
+    }
+    const float maxX = (float)mx, minX = (float)mn, maxY = (float)my, minY = (float)mny;
+    const float mult = (float)(0.1 * std::min(std::fabs(maxX - minX), std::fabs(maxY - minY)));
+    double mm = -INFINITY;
+    for (long long r = 0; r < nv; ++r) mm = std::max(mm, V[(size_t)(3 * r)] + (double)mult * en[(size_t)(3 * r)]);
+    if ((float)mm < maxX)
+        for (auto& x : en) x = -x;
+    for (long long i = 1; i < nv + 1; ++i) {
+        const long long j = i % nv;
+        double v[3];
+        for (int k = 0; k < 3; ++k)
+            v[k] = el[(size_t)(i - 1)] * en[(size_t)(3 * (i - 1) + k)] + el[(size_t)j] * en[(size_t)(3 * j + k)];
+        const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int k = 0; k < 3; ++k) out[3 * j + k] = len > 0 ? v[k] / len : v[k];
+    }
+    return 0;
+}
+
+// utils::normals3d (helper/utils.cpp:86-90): libigl per_vertex_normals with
+// its default area weighting -- per vertex the sum, in face order, of the
+// incident faces' edge cross products (unit normal times twice the area),
+// then scaled to unit length.  Returns 0, or -1 for an index outside V.
+int orc_normals_3d(const double* V, long long nv, const int* F, long long nf, double* out) {
+    for (long long i = 0; i < 3 * nv; ++i) out[i] = 0.0;
+    for (long long f = 0; f < nf; ++f) {
+        const int a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
+        if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv) return -1;
+        double u[3], w[3];
+        for (int k = 0; k < 3; ++k) {
+            u[k] = V[3 * b + k] - V[3 * a + k];
+            w[k] = V[3 * c + k] - V[3 * a + k];
+        }
+        const double nrm[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+        for (int k = 0; k < 3; ++k) {
+            out[3 * a + k] += nrm[k];
+            out[3 * b + k] += nrm[k];
+            out[3 * c + k] += nrm[k];
+        }
+    }
+    for (long long i = 0; i < nv; ++i) {
+        const double len = std::sqrt(out[3 * i] * out[3 * i] + out[3 * i + 1] * out[3 * i + 1] +
+                                     out[3 * i + 2] * out[3 * i + 2]);
+        if (len > 0)
+            for (int k = 0; k < 3; ++k) out[3 * i + k] /= len;
+    }
+    return 0;
+}
+
 // which: 0 = cost/time ratio (lawlercpu), 1 = minimum cost (dijkstracpu).
 int orc_solve(void* h, int which, int k, int* passes, float* objective) {
     Generator* G = (Generator*)h;

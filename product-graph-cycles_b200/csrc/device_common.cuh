@@ -212,6 +212,49 @@ struct LookupArgs {
     double* tOut;
 };
 
+// One graph of a batched ratio solve (bf_batch_kernel): a CTA takes the job
+// from the queue and runs its whole solve on the device -- the initial upper
+// bound (cost_time_ratio_solver.cpp:652-707), the Lawler iterations
+// (:558-635) and their cycle evaluations (computeRatioForCycle, :88-133) --
+// as long as the first branch's cycle does not wrap; otherwise the host
+// finishes the solve with branch and bound.
+enum PairStatus : int {
+    PAIR_PENDING = 0,
+    PAIR_DONE = 1,       // result written
+    PAIR_NAN = 2,        // the reference's (true, NaN, no rows) result
+    PAIR_HOST = 3,       // the solve needs branch and bound (or a longer cycle record): finish on the host
+    PAIR_ERR_UB = -1,    // no closed path through the upper-bound start node
+    PAIR_ERR_EDGE = -2,  // a cycle edge was not found in the product graph
+    PAIR_ERR_BF = -3,    // a Bellman-Ford call ended in an error status (in bfStatus)
+    PAIR_ERR_WAIT = -4,  // a device wait ran out
+    PAIR_ERR_GUARD = -5, // the upper-bound ratio search did not terminate
+};
+
+struct PairJob {
+    BfParams bf;           // the graph's Bellman-Ford parameters; mode, branch, lambda, ub set per call
+    LookupArgs lk;         // the graph's edge lookup tables (pair arrays unused)
+    int* branchOf;         // == bf.branchOf, written by the solve
+    double tconst;         // time of every edge when there is no time column
+    // two cycle records of capacity `cap`: original node ids (cap + 1), and
+    // per edge its id, cost and time
+    int* recNodes[2];
+    long long* recEdges[2];
+    double* recC[2];
+    double* recT[2];
+    int cap;
+    // outputs
+    int status;            // PairStatus
+    int bfStatus;          // the failing call's status for PAIR_ERR_BF
+    int passes;
+    float objective;
+    int nEdges;            // edges of the returned cycle, in recEdges[rec]
+    int rec;
+    double adjT;           // time sum of the returned cycle (the adjoint's T)
+    double ratio;          // its ratio C / T in double (the adjoint's lambda*)
+    long long cycles;      // SM clock cycles the CTA spent on the graph
+    long long bfCalls, sweeps, lawlerIters, candidates, fallbackWalks;
+};
+
 constexpr int kStepDoneStride = 8;  // one 32-byte sector per CTA step counter
 // Polls of a device wait before it gives up (~2 s with its back-off).
 constexpr unsigned kDefaultSpinLimit = 1u << 24;
@@ -222,6 +265,13 @@ constexpr long long kWalkRoundLoads = 4096;
 constexpr int kBfThreads = 640;
 // Source values a lane gathers before folding them (one batch of rows).
 constexpr int kGather = 20;
+// Threads of a batched-solve CTA and the CTAs an SM should hold: each CTA
+// solves one graph at a time, so CTAs on one SM overlap their latencies.
+constexpr int kBatchThreads = 256;
+// Capacity of a batched solve's cycle records (edges); a longer cycle hands
+// the graph back to the host.
+constexpr long long kBatchCycleCap = 1LL << 16;
+constexpr int kBatchBlocksPerSm = 2;
 // Rows of one gather batch when every row has nk source depths (nk > 0).
 __host__ __device__ constexpr int bf_rows_per_batch(int nk) {
     return kGather / nk < 1 ? 1 : kGather / nk > 8 ? 8 : kGather / nk;
@@ -245,6 +295,11 @@ cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks
                       bool sharedTables, size_t smemBytes, cudaStream_t stream);
 cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream);
+// Batched ratio solves: `count` jobs taken from a queue (*next, zeroed by the
+// caller) by `blocks` CTAs of `threads` threads.
+cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, int costIsF32, int timeKind, int blocks,
+                            int threads, size_t smemBytes, cudaStream_t stream);
+cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);
@@ -273,10 +328,14 @@ cudaError_t noalloc_export_scratch(int device, double** ptr);
 cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
                                         double coef, double* grad, cudaStream_t s);
 cudaError_t launch_conj_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
-                                       double coef, double* grad, cudaStream_t s);
+                                       double coef, double coefT, long long argmax, double* grad, cudaStream_t s);
 cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,
                           long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
                           cudaStream_t s);
+cudaError_t launch_normals_3d(const double* V, long long nv, const int* F, long long nf, double* fn, int* deg,
+                              int* off, int* cursor, int* list, double* out, int* bad, cudaStream_t s);
+cudaError_t launch_normals_2d(const double* Vin, int nv, const int* E, double* V, double* en, double* el, double* out,
+                              int* bad, cudaStream_t s);
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s);

@@ -861,26 +861,18 @@ __device__ int dij_walk_end(const BfParams& p, int v) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// The Bellman-Ford launch.  Every CTA of the grid belongs to one team.
-// Dynamic shared memory: [DP tables + backup row, if S][candidate scratch].
+// One Bellman-Ford call by a team of CTAs, from its set-up to its verdict in
+// p.ctl.  t.cta is the CTA's index in the team: the grid of a single-graph
+// launch, or one CTA of a batched launch that solves many graphs.  `smem` is
+// the dynamic shared memory after the DP tables: [row offsets and lists of
+// slices with rows][two step buffers].
 // ---------------------------------------------------------------------------
 template <class CT, int TK, bool S>
-__global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
-    Team t{(int)blockIdx.x, (int)gridDim.x, &p.ctl->barCount, &p.ctl->barGen, &p.ctl->error, p.spinLimit};
+__device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* smem) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const long long tid = t.thread(), nth = t.nthreads();
-    const bool isLead = (blockIdx.x == 0 && threadIdx.x == 0);
-    extern __shared__ double4 smemRaw[];
-    char* smem = reinterpret_cast<char*>(smemRaw);
-    if constexpr (S) {
-        // single-CTA team: the DP records and the backup row live in shared
-        // memory for the whole launch (layout as in global memory)
-        p.dv = reinterpret_cast<double*>(smem);
-        p.doh = reinterpret_cast<int2*>(smem + (size_t)2 * n * Kp * sizeof(double));
-        p.bak = reinterpret_cast<double*>(smem + (size_t)2 * n * Kp * (sizeof(double) + sizeof(int2)));
-        smem += bf_shared_table_bytes(n, Kp);
-    }
-    const int s0 = __ldg(p.ctaSlice + blockIdx.x), s1 = __ldg(p.ctaSlice + blockIdx.x + 1);
+    const bool isLead = (t.cta == 0 && threadIdx.x == 0);
+    const int s0 = __ldg(p.ctaSlice + t.cta), s1 = __ldg(p.ctaSlice + t.cta + 1);
     const bool handoff = t.ncta > 1 && p.flagSync;
     if (handoff && threadIdx.x == 0) p.stepDone[(size_t)t.cta * kStepDoneStride] = 0;
     // shared memory: [row offsets of both parts][slices with rows, per part]
@@ -961,14 +953,14 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
         Key km{-(double)last, last < 0 ? 0x7fffffff : last};
         if (last < 0) km.v = 1.0;
         km = block_min(km, 0);
-        if (threadIdx.x == 0) p.redIdx[blockIdx.x] = km.i;
+        if (threadIdx.x == 0) p.redIdx[t.cta] = km.i;
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         __shared__ int scnt;
         if (threadIdx.x == 0) scnt = 0;
         __syncthreads();
         if ((threadIdx.x & 31) == 0) atomicAdd(&scnt, cnt);
         __syncthreads();
-        if (threadIdx.x == 0) p.redAux[blockIdx.x] = scnt;
+        if (threadIdx.x == 0) p.redAux[t.cta] = scnt;
     }
     if (!team_sync(t)) return;
     if (isLead) {
@@ -1090,11 +1082,11 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             firstValid = block_min(firstValid, 1);
             anyFinite = __syncthreads_or(anyFinite);
             if (threadIdx.x == 0) {
-                p.redVal[2 * blockIdx.x] = first.v;
-                p.redIdx[2 * blockIdx.x] = first.i;
-                p.redVal[2 * blockIdx.x + 1] = firstValid.v;
-                p.redIdx[2 * blockIdx.x + 1] = firstValid.i;
-                p.redAux[blockIdx.x] = anyFinite;
+                p.redVal[2 * t.cta] = first.v;
+                p.redIdx[2 * t.cta] = first.i;
+                p.redVal[2 * t.cta + 1] = firstValid.v;
+                p.redIdx[2 * t.cta + 1] = firstValid.i;
+                p.redAux[t.cta] = anyFinite;
             }
             if (!team_sync(t)) return;
             if (isLead) {
@@ -1197,11 +1189,11 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             if ((threadIdx.x & 31) == 0) atomicAdd(&sdec, (unsigned long long)decided);
             __syncthreads();
             if (threadIdx.x == 0) {
-                p.redVal[2 * blockIdx.x] = bestOk.v;
-                p.redIdx[2 * blockIdx.x] = bestOk.i;
-                p.redVal[2 * blockIdx.x + 1] = firstUnknown.v;
-                p.redIdx[2 * blockIdx.x + 1] = firstUnknown.i;
-                p.redAux64[blockIdx.x] = (long long)sdec;
+                p.redVal[2 * t.cta] = bestOk.v;
+                p.redIdx[2 * t.cta] = bestOk.i;
+                p.redVal[2 * t.cta + 1] = firstUnknown.v;
+                p.redIdx[2 * t.cta + 1] = firstUnknown.i;
+                p.redAux64[t.cta] = (long long)sdec;
             }
         }
         __shared__ int sLaps, sBad;
@@ -1260,8 +1252,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
             }
             best = block_min(best, 0);
             if (threadIdx.x == 0) {
-                p.redVal[2 * blockIdx.x] = best.v;
-                p.redIdx[2 * blockIdx.x] = best.i;
+                p.redVal[2 * t.cta] = best.v;
+                p.redIdx[2 * t.cta] = best.i;
             }
             if (!team_sync(t)) return;
             if (isLead) {
@@ -1307,7 +1299,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
                 p.ctl->status = BF_MAX_SWEEPS;
             }
         }
-        if (blockIdx.x == 0) {
+        if (t.cta == 0) {
             __syncthreads();
             const int laps = sLaps;
             if (laps > 0) {
@@ -1343,6 +1335,25 @@ __global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
     }
 }
 
+// The Bellman-Ford launch of one graph.  Every CTA of the grid belongs to
+// its team.  Dynamic shared memory: [DP tables + backup row, if S][the
+// body's stage memory].
+template <class CT, int TK, bool S>
+__global__ void __launch_bounds__(kBfThreads, 1) bf_kernel(BfParams p) {
+    const Team t{(int)blockIdx.x, (int)gridDim.x, &p.ctl->barCount, &p.ctl->barGen, &p.ctl->error, p.spinLimit};
+    extern __shared__ double4 smemRaw[];
+    char* smem = reinterpret_cast<char*>(smemRaw);
+    if constexpr (S) {
+        // single-CTA team: the DP records and the backup row live in shared
+        // memory for the whole launch (layout as in global memory)
+        p.dv = reinterpret_cast<double*>(smem);
+        p.doh = reinterpret_cast<int2*>(smem + (size_t)2 * p.n * p.Kp * sizeof(double));
+        p.bak = reinterpret_cast<double*>(smem + (size_t)2 * p.n * p.Kp * (sizeof(double) + sizeof(int2)));
+        smem += bf_shared_table_bytes(p.n, p.Kp);
+    }
+    bf_body<CT, TK, S>(p, t, smem);
+}
+
 // Minimum-cost path extraction (dijkstra_solver.cpp:349-357): from the
 // closing copy of v back to the start node.  Writes original ids in walk
 // order; returns the count through ctl->cycleLen.
@@ -1366,46 +1377,384 @@ __global__ void extract_path_kernel(BfParams p, int v) {
     p.ctl->cycleLen = len;
 }
 
-// Finds, for each (source, target) pair of original ids, the first in-edge of
-// the target whose source matches (computeRatioForCycle's lookup,
-// cost_time_ratio_solver.cpp:103-122) and returns its edge id and the double
-// cost/time of that edge.  Target ids >= numNodes denote the closing layer.
-__global__ void lookup_pairs_kernel(LookupArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.count) return;
-    const long long S = a.pairSrc[i], T = a.pairTrgt[i];
-    a.edgeOut[i] = -2;
-    a.cOut[i] = 0;
-    a.tOut[i] = 0;
-    if (S < 0 || T < 0) return;
+// The first in-edge of target T whose source is S (original ids; T >=
+// numNodes denotes the closing layer), as computeRatioForCycle's lookup does
+// (cost_time_ratio_solver.cpp:103-122): its edge id and the double cost and
+// time of that edge.  Returns false when there is none.
+__device__ bool lookup_edge(const LookupArgs& a, long long S, long long T, long long* edge, double* c, double* t) {
+    if (S < 0 || T < 0) return false;
     const int lt = (int)(T / a.n), v = (int)(T % a.n);
     const int ls = (int)(S / a.n), s = (int)(S % a.n);
-    if (lt > a.nY) return;
+    if (lt > a.nY) return false;
     int part;
     const int* src;
     const int* sp;
     const int* ted;
     long long block;
     if (lt == a.nY) {
-        if (ls != a.nY - 1) return;
+        if (ls != a.nY - 1) return false;
         part = 0; src = a.srcDummy; sp = a.spInter; ted = a.tedgeInter; block = a.nY - 1;
     } else if (ls == lt) {
         part = 1; src = a.srcIntra; sp = a.spIntra; ted = a.tedgeIntra; block = lt;
     } else if (lt >= 1 && ls == lt - 1) {
         part = 0; src = a.srcInter; sp = a.spInter; ted = a.tedgeInter; block = lt - 1;
     } else {
-        return;
+        return false;
     }
     const int slice = v >> 5, lane = v & 31;
     for (int j = sp[slice]; j < sp[slice + 1]; ++j) {
         const long long e = (long long)j * 32 + lane;
         if (src[e] == s) {
             const long long off = (long long)lt * a.layerStride + (part ? a.interEntries : 0) + e;
-            a.edgeOut[i] = block * a.eBlock + ted[e];
-            a.cOut[i] = a.c32 ? (double)a.c32[off] : a.c64[off];
-            a.tOut[i] = a.t32 ? (double)a.t32[off] : a.t64 ? a.t64[off] : a.tconst;
+            *edge = block * a.eBlock + ted[e];
+            *c = a.c32 ? (double)a.c32[off] : a.c64[off];
+            *t = a.t32 ? (double)a.t32[off] : a.t64 ? a.t64[off] : a.tconst;
+            return true;
+        }
+    }
+    return false;
+}
+
+// lookup_edge for each (source, target) pair of a cycle; edge -2 when absent.
+__global__ void lookup_pairs_kernel(LookupArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.count) return;
+    long long e = -2;
+    double c = 0, t = 0;
+    if (!lookup_edge(a, a.pairSrc[i], a.pairTrgt[i], &e, &c, &t)) e = -2, c = 0, t = 0;
+    a.edgeOut[i] = e;
+    a.cOut[i] = c;
+    a.tOut[i] = t;
+}
+
+// ---------------------------------------------------------------------------
+// Batched ratio solves.  Each CTA takes graphs from a queue and runs the
+// host driver's ratio solve on the device for each: the initial upper bound
+// (cost_time_ratio_solver.cpp:652-707), the Lawler iterations (:558-635)
+// with their Bellman-Ford calls as one-CTA teams, and the cycle evaluations
+// (computeRatioForCycle, :88-133) in the same double operations and order as
+// the host.  The first branch's Lawler result is the solve's result unless
+// its cycle wraps (:840-850); then the host takes the graph over with branch
+// and bound, and the device's work on it only cost time.
+// ---------------------------------------------------------------------------
+namespace {
+
+// (int)std::round(x) as x86-64 computes it: out of range or NaN gives INT_MIN.
+__device__ __forceinline__ int round_to_int_x86(double x) {
+    const double r = round(x);  // half away from zero, as std::round
+    if (!(r >= -2147483648.0 && r <= 2147483647.0)) return (int)0x80000000;
+    return (int)r;
+}
+__device__ __forceinline__ double via_float(double x) { return (double)__double2float_rn(x); }
+
+struct CycleSums {
+    double ratio, wsum;
+};
+
+// computeRatioForCycle's sums over a stored cycle record, one thread, in the
+// cycle's order: C += c, T += t, W += c - lambda * t, each a rounded double
+// operation.
+__device__ CycleSums record_sums(const PairJob& J, int rec, int m, double lambda) {
+    const double* c = J.recC[rec];
+    const double* t = J.recT[rec];
+    double C = 0, T = 0, W = 0;
+    for (int i = 0; i < m; ++i) {
+        const double ci = __ldcg(c + i), ti = __ldcg(t + i);
+        C = __dadd_rn(C, ci);
+        T = __dadd_rn(T, ti);
+        W = __dadd_rn(W, __dsub_rn(ci, __dmul_rn(lambda, ti)));
+    }
+    return {__ddiv_rn(C, T), W};
+}
+
+// A cycle from the Bellman-Ford walk in the cycle buffer (p(v0), ..., v0,
+// or the upper-bound path) into record `rec`: the walk reversed, closed with
+// the copy of its first node when `close`, and every consecutive pair's edge,
+// cost and time (a closing-layer target is its copy: b + numNodes when
+// b < n < a, cost_time_ratio_solver.cpp:109-111).  All threads of the CTA;
+// returns the edge count, -1 when an edge is missing, -2 when the record is
+// too small.
+__device__ int record_cycle(const PairJob& J, const BfParams& P, int rec, int len, bool close) {
+    __shared__ int sMissing;
+    const int count = len + (close ? 1 : 0);
+    if (count > J.cap + 1 || len < 1) return -2;
+    int* nodes = J.recNodes[rec];
+    const long long nn = P.numNodes;
+    const int n = P.n;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) nodes[i] = __ldcg(P.cycleBuf + (len - 1 - i));
+    if (close && threadIdx.x == 0) nodes[len] = __ldcg(P.cycleBuf + (len - 1)) + (int)nn;
+    if (threadIdx.x == 0) sMissing = 0;
+    __syncthreads();
+    const int m = count - 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int a = nodes[i];
+        long long b = nodes[i + 1];
+        if (b < n && a > n) b += nn;
+        long long e;
+        double c, t;
+        if (!lookup_edge(J.lk, a, b, &e, &c, &t)) {
+            sMissing = 1;
+            e = -2, c = 0, t = 0;
+        }
+        J.recEdges[rec][i] = e;
+        J.recC[rec][i] = c;
+        J.recT[rec][i] = t;
+    }
+    __syncthreads();
+    return sMissing ? -1 : m;
+}
+
+// Lawler's outcome of one Bellman-Ford call (the host driver's bellman_ford).
+enum Outcome { OUT_FOUND = 0, OUT_NONE = 1, OUT_ZERO = 2 };
+
+template <class CT, int TK>
+__device__ __noinline__ void bf_call(const BfParams& P, const Team& t, char* smem) {
+    bf_body<CT, TK, false>(P, t, smem);
+}
+
+// The whole ratio solve of one graph by this CTA.  P is the job's
+// Bellman-Ford parameters in shared memory.
+template <class CT, int TK>
+__device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
+    __shared__ int sState[4];        // [0] verdict, [1] done, [2] record of the negative cycle, [3] its edges
+    __shared__ double sRatio;
+    const int n = P.n;
+    Control* ctl = P.ctl;
+    const double tolerance = (double)(float)1e-8;
+    const double ubInf = (double)__int_as_float(0x7f800000);
+
+    // ---- initial upper bound (cost_time_ratio_solver.cpp:652-707) ----
+    // the layer-1 node with the lowest float mean in-cost among those with
+    // more than three in-edges, first in index order (node 0 if none)
+    Key best{kInfD, 0x7fffffff};
+    {
+        const CT* c1 = reinterpret_cast<const CT*>(P.cost) + P.layerStride;
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const int s = v >> 5, lane = v & 31;
+            float mean = 0;
+            int num = 0;
+            for (int j = __ldg(P.spInter + s); j < __ldg(P.spInter + s + 1); ++j) {
+                const long long e = (long long)j * 32 + lane;
+                if (__ldg(P.srcInter + e) < 0) continue;
+                mean = (float)((double)mean + (double)c1[e]);
+                ++num;
+            }
+            for (int j = __ldg(P.spIntra + s); j < __ldg(P.spIntra + s + 1); ++j) {
+                const long long e = (long long)j * 32 + lane;
+                if (__ldg(P.srcIntra + e) < 0) continue;
+                mean = (float)((double)mean + (double)c1[P.interEntries + e]);
+                ++num;
+            }
+            mean = mean / (float)num;
+            const Key k{(double)mean, v};
+            if (num > 3 && mean < __int_as_float(0x7f800000) && key_less(k, best)) best = k;
+        }
+        best = block_min(best, 0);
+    }
+    const int startV = best.i == 0x7fffffff ? 0 : best.i;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) J.branchOf[v] = v == startV ? 0 : 1;
+    if (threadIdx.x == 0) {
+        P.mode = 1;
+        P.branchId = 0;
+        P.lambda = 10;
+        P.ub = ubInf;
+        ctl->status = BF_RUNNING;
+        ctl->error = 0;
+    }
+    __syncthreads();
+    bf_call<CT, TK>(P, t, smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        J.bfCalls++;
+        J.sweeps += ctl->sweeps;
+    }
+    if (*(volatile int*)&ctl->error) {
+        if (threadIdx.x == 0) J.status = PAIR_ERR_WAIT;
+        return;
+    }
+    {
+        const int st = *(volatile int*)&ctl->status;
+        if (st == BF_LAYER_UNREACHED) {  // the empty cycle's 0/0 bound: (true, NaN, no rows)
+            if (threadIdx.x == 0) J.status = PAIR_NAN;
             return;
         }
+        if (st != BF_UB_DONE) {
+            if (threadIdx.x == 0) {
+                J.status = st < 0 ? PAIR_ERR_BF : PAIR_ERR_UB;
+                J.bfStatus = st;
+            }
+            return;
+        }
+    }
+    int neg = 0;
+    {
+        const int m = record_cycle(J, P, neg, *(volatile int*)&ctl->cycleLen, false);
+        if (m < 0) {
+            if (threadIdx.x == 0) J.status = m == -2 ? PAIR_HOST : PAIR_ERR_EDGE;
+            return;
+        }
+        if (threadIdx.x == 0) {
+            sState[3] = m;
+            double lambda = 10;
+            CycleSums ev = record_sums(J, neg, m, lambda);
+            double cycleCost = via_float(ev.wsum);
+            int guard = 0, bad = 0;
+            while (cycleCost > 0 || isnan(cycleCost)) {
+                if (++guard > 4000) {
+                    bad = 1;
+                    break;
+                }
+                lambda += lambda;
+                ev = record_sums(J, neg, m, lambda);
+                cycleCost = via_float(ev.wsum);
+            }
+            sRatio = via_float(ev.ratio);
+            sState[1] = bad;
+        }
+        __syncthreads();
+        if (sState[1]) {
+            if (threadIdx.x == 0) J.status = PAIR_ERR_GUARD;
+            return;
+        }
+    }
+    // A NaN or infinite bound: the host's branch-and-bound path (the heap
+    // comparison that ends the first branch does not hold then).
+    if (!(sRatio < (double)__int_as_float(0x7f800000))) {
+        if (threadIdx.x == 0) J.status = PAIR_HOST;
+        return;
+    }
+
+    // ---- the first branch: every node starts (cost_time_ratio_solver.cpp:794-829) ----
+    for (int v = threadIdx.x; v < n; v += blockDim.x) J.branchOf[v] = 0;
+    double currentRatio = sRatio;  // every thread keeps the same copy
+    double oldRatio = currentRatio;
+    int negEdges = sState[3];
+    for (int i = 0;;) {
+        if (threadIdx.x == 0) {
+            P.mode = 0;
+            P.branchId = 0;
+            P.lambda = currentRatio;
+            P.ub = ubInf;
+            ctl->status = BF_RUNNING;
+        }
+        __syncthreads();
+        bf_call<CT, TK>(P, t, smem);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            J.bfCalls++;
+            J.sweeps += ctl->sweeps;
+            J.lawlerIters++;
+        }
+        if (*(volatile int*)&ctl->error) {
+            if (threadIdx.x == 0) J.status = PAIR_ERR_WAIT;
+            return;
+        }
+        const int st = *(volatile int*)&ctl->status;
+        int outcome;
+        if (st == BF_FOUND_CYCLE) {
+            const int cand = neg ^ 1;
+            const int m = record_cycle(J, P, cand, *(volatile int*)&ctl->cycleLen, true);
+            if (m < 0) {
+                if (threadIdx.x == 0) J.status = m == -2 ? PAIR_HOST : PAIR_ERR_EDGE;
+                return;
+            }
+            if (threadIdx.x == 0) {
+                const int integral = round_to_int_x86(record_sums(J, cand, m, currentRatio).wsum);
+                int o;
+                if (integral < 0) o = OUT_FOUND;
+                else if (integral == 0) o = OUT_NONE;
+                else o = round_to_int_x86(record_sums(J, neg, negEdges, currentRatio).wsum) == 0 ? OUT_ZERO : OUT_NONE;
+                sState[0] = o;
+                sState[3] = m;
+            }
+            __syncthreads();
+            outcome = sState[0];
+            if (outcome == OUT_FOUND) {
+                neg = cand;
+                negEdges = sState[3];
+            }
+        } else if (st == BF_LAYER_UNREACHED || st == BF_WRAP_NO_IMPROVE || st == BF_MAX_SWEEPS) {
+            if (threadIdx.x == 0)
+                sState[0] = st != BF_MAX_SWEEPS &&
+                                    round_to_int_x86(record_sums(J, neg, negEdges, currentRatio).wsum) == 0
+                                ? OUT_ZERO
+                                : OUT_NONE;
+            __syncthreads();
+            outcome = sState[0];
+        } else {
+            if (threadIdx.x == 0) {
+                J.status = PAIR_ERR_BF;
+                J.bfStatus = st;
+            }
+            return;
+        }
+        if (outcome != OUT_FOUND) break;
+        // lawlerSoubroutine's update and stopping rules (:584-597)
+        if (threadIdx.x == 0) sRatio = record_sums(J, neg, negEdges, currentRatio).ratio;
+        __syncthreads();
+        currentRatio = sRatio;
+        if (fabs(oldRatio - currentRatio) < tolerance) break;
+        if (currentRatio - tolerance > oldRatio) break;
+        oldRatio = currentRatio;
+        if (i > 1000) break;
+        ++i;
+    }
+    // passes of the cycle through layer 0 (:606-634): more than one, and the
+    // branch and bound splits the branch -- the host's part
+    if (threadIdx.x == 0) {
+        const int* nodes = J.recNodes[neg];
+        int wraps = 0;
+        bool left = false;
+        for (int i = 0; i <= negEdges; ++i) {
+            const int vtx = __ldcg(nodes + i);
+            if (left && vtx < n) left = false;
+            if (vtx >= n && !left) {
+                ++wraps;
+                left = true;
+            }
+        }
+        if (wraps > 1 && n > 1) {
+            J.status = PAIR_HOST;
+        } else {
+            const CycleSums fin = record_sums(J, neg, negEdges, currentRatio);
+            double T = 0;
+            for (int i = 0; i < negEdges; ++i) T += __ldcg(J.recT[neg] + i);
+            J.passes = 1;
+            J.objective = __double2float_rn(fin.ratio);
+            J.nEdges = negEdges;
+            J.rec = neg;
+            J.adjT = T;
+            J.ratio = fin.ratio;
+            J.status = PAIR_DONE;
+        }
+    }
+}
+
+}  // namespace
+
+template <class CT, int TK>
+__global__ void __launch_bounds__(kBatchThreads, kBatchBlocksPerSm) bf_batch_kernel(PairJob* jobs, int count,
+                                                                                   int* next) {
+    extern __shared__ double4 smemRaw[];
+    char* smem = reinterpret_cast<char*>(smemRaw);
+    __shared__ BfParams P;
+    __shared__ int sJob;
+    for (;;) {
+        if (threadIdx.x == 0) sJob = atomicAdd(next, 1);
+        __syncthreads();
+        const int j = sJob;
+        if (j >= count) return;
+        if (threadIdx.x == 0) P = jobs[j].bf;
+        __syncthreads();
+        const Team t{0, 1, &P.ctl->barCount, &P.ctl->barGen, &P.ctl->error, P.spinLimit};
+        const long long c0 = clock64();
+        pair_solve<CT, TK>(jobs[j], P, t, smem);
+        if (threadIdx.x == 0) {
+            jobs[j].candidates = P.ctl->candidates;
+            jobs[j].fallbackWalks = P.ctl->fallbackWalks;
+            jobs[j].cycles = clock64() - c0;
+        }
+        __syncthreads();
     }
 }
 
@@ -1467,6 +1816,30 @@ cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t 
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream) {
     extract_path_kernel<<<1, 32, 0, stream>>>(p, v);
     return cudaGetLastError();
+}
+
+static const void* bf_batch_fn(int costIsF32, int timeKind) {
+    if (costIsF32)
+        return timeKind == 0 ? (const void*)bf_batch_kernel<float, 0>
+                             : timeKind == 1 ? (const void*)bf_batch_kernel<float, 1> : (const void*)bf_batch_kernel<float, 2>;
+    return timeKind == 0 ? (const void*)bf_batch_kernel<double, 0>
+                         : timeKind == 1 ? (const void*)bf_batch_kernel<double, 1> : (const void*)bf_batch_kernel<double, 2>;
+}
+
+cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, int costIsF32, int timeKind, int blocks,
+                            int threads, size_t smemBytes, cudaStream_t stream) {
+    const void* fn = bf_batch_fn(costIsF32, timeKind);
+    const cudaError_t e = allow_max_dynamic_smem(fn);
+    if (e != cudaSuccess) return e;
+    void* args[] = {(void*)&jobs, (void*)&count, (void*)&next};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
+}
+
+cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm) {
+    const void* fn = bf_batch_fn(costIsF32, timeKind);
+    const cudaError_t e = allow_max_dynamic_smem(fn);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, smemBytes);
 }
 
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream) {

@@ -226,8 +226,14 @@ __global__ void plain_energy_backward_kernel(EnergyArgs a, const long long* edge
 // cost = fd[x2, y2] (higherOrderDeformationEnergy.cpp).  Scatters coef into
 // grad[x2, y2] of every listed product edge; an edge listed twice
 // contributes twice.
+// Every cycle edge e reads fd[x2, y2]: with slope coef in the cost column,
+// and, when coefT != 0 (a ratio whose time column is ("*", "feature"):
+// t = max(0, maxFd - fd), maxFd the matrix's maximum), with slope -1 in
+// the time -- the adjoint there is +coefT at fd[x2, y2] and -coefT at the
+// maximum's entry `argmax` (a subgradient: zero where the time is clamped at
+// 0, and the two cancel when e reads the maximum itself).
 __global__ void conj_energy_backward_kernel(EnergyArgs a, const long long* edges, int count, long long eBlock,
-                                            double coef, double* grad) {
+                                            double coef, double coefT, long long argmax, double* grad) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const long long e = edges[i];
@@ -243,7 +249,12 @@ __global__ void conj_energy_backward_kernel(EnergyArgs a, const long long* edges
         default: y2 = m2; break;
     }
     const int x2 = a.eX[3 * t + 2];
-    atomicAdd(grad + (long long)x2 * a.nvy + y2, coef);
+    const long long at = (long long)x2 * a.nvy + y2;
+    if (coef != 0.0) atomicAdd(grad + at, coef);
+    if (coefT != 0.0 && a.maxFd - __ldg(a.FD + at) > 0.0) {
+        atomicAdd(grad + at, coefT);
+        atomicAdd(grad + argmax, -coefT);
+    }
 }
 
 // Inverse of export_kernel: column c of a [rows x cols] edge-ordered matrix
@@ -708,6 +719,249 @@ __global__ void layer1_mean_kernel(const CT* cost, long long layerStride, long l
     (void)nslices;
 }
 
+// ---------------------------------------------------------------------------
+// Vertex normals on the device (utils::normals3d / normals2d,
+// helper/utils.cpp:86-157).  Every value is computed with the operations, in
+// the order, of the reference's host loops (this file is compiled without
+// fused multiply-adds), so the results are the same bit for bit.
+// ---------------------------------------------------------------------------
+
+// 3D, step 1: every face's edge cross product (its unit normal times twice
+// its area, libigl's area weighting) and each vertex's corner count.
+__global__ void face_normals_kernel(const double* V, long long nv, const int* F, long long nf, double* fn, int* deg,
+                                    int* bad) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+        const int a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
+        if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv) {
+            atomicExch(bad, 1);
+            continue;
+        }
+        double u[3], w[3];
+        for (int k = 0; k < 3; ++k) {
+            u[k] = V[3 * b + k] - V[3 * a + k];
+            w[k] = V[3 * c + k] - V[3 * a + k];
+        }
+        fn[3 * f] = u[1] * w[2] - u[2] * w[1];
+        fn[3 * f + 1] = u[2] * w[0] - u[0] * w[2];
+        fn[3 * f + 2] = u[0] * w[1] - u[1] * w[0];
+        atomicAdd(deg + a, 1);
+        atomicAdd(deg + b, 1);
+        atomicAdd(deg + c, 1);
+    }
+}
+
+// Exclusive prefix sum of n counts into off[0..n] by one CTA, tile by tile.
+__global__ void exclusive_scan_kernel(const int* in, long long n, int* off) {
+    __shared__ int warpSum[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < n; base += blockDim.x) {
+        const long long i = base + threadIdx.x;
+        const int x = i < n ? in[i] : 0;
+        int incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warpSum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            int ws = lane < nw ? warpSum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, ws, o);
+                if (lane >= o) ws += y;
+            }
+            if (lane < nw) warpSum[lane] = ws;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = (w > 0 ? warpSum[w - 1] : 0) + incl - x;
+        if (i < n) off[i] = carry + before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warpSum[nw - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) off[n] = carry;
+}
+
+// 3D, step 2: each vertex's incident faces (a face with a repeated vertex
+// is listed once per corner, as the reference adds it once per corner).
+// Faces with an index outside V were flagged by step 1 and are skipped, as
+// they were not counted.
+__global__ void face_lists_kernel(const int* F, long long nv, long long nf, const int* off, int* cursor, int* list) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+        const int a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
+        if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv) continue;
+        for (int k = 0; k < 3; ++k) {
+            const int v = F[3 * f + k];
+            list[off[v] + atomicAdd(cursor + v, 1)] = (int)f;
+        }
+    }
+}
+
+// 3D, step 3: per vertex, its faces in ascending order (the reference's
+// accumulation order), their normals summed from 0, then unit length.
+__global__ void vertex_normals_kernel(const double* fn, long long nv, const int* off, int* list, double* out) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv; v += (long long)gridDim.x * blockDim.x) {
+        const int lo = off[v], hi = off[v + 1];
+        for (int j = lo + 1; j < hi; ++j) {  // insertion sort: vertex degrees are small
+            const int f = list[j];
+            int q = j - 1;
+            while (q >= lo && list[q] > f) {
+                list[q + 1] = list[q];
+                --q;
+            }
+            list[q + 1] = f;
+        }
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int j = lo; j < hi; ++j) {
+            const long long f = list[j];
+            x = x + fn[3 * f];
+            y = y + fn[3 * f + 1];
+            z = z + fn[3 * f + 2];
+        }
+        const double len = sqrt(x * x + y * y + z * z);
+        if (len > 0) {
+            x = x / len;
+            y = y / len;
+            z = z / len;
+        }
+        out[3 * v] = x;
+        out[3 * v + 1] = y;
+        out[3 * v + 2] = z;
+    }
+}
+
+// 2D: the whole curve by one CTA.  `V` is scratch for the curve moved into
+// the xy-plane, `en` and `el` for the edge normals and lengths.  *bad: 1 no
+// coordinate plane, 2 an edge index outside V.
+__global__ void curve_normals_kernel(const double* Vin, int nv, const int* E, double* V, double* en, double* el,
+                                     double* out, int* bad) {
+    __shared__ double sums[3];
+    __shared__ int sZero, sBad;
+    __shared__ double red[4][32];
+    __shared__ double sMm;
+    __shared__ float sMult, sMaxX;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x < 3) {  // the column sums in row order, as the reference adds them
+        double s = 0;
+        for (int r = 0; r < nv; ++r) s += Vin[3 * r + threadIdx.x];
+        sums[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) sBad = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int zero = -1;
+        for (int i = 0; i < 3; ++i)
+            if (fabs(sums[i]) < 1e-4) {
+                zero = i;
+                break;
+            }
+        sZero = zero;
+        if (zero == -1) *bad = 1;
+    }
+    __syncthreads();
+    const int zero = sZero;
+    if (zero == -1) return;
+    const int order[3] = {zero == 2 ? 0 : zero == 1 ? 0 : 1, zero == 2 ? 1 : 2, zero == 2 ? 2 : zero == 1 ? 1 : 0};
+    for (int r = threadIdx.x; r < nv; r += blockDim.x)
+        for (int k = 0; k < 3; ++k) V[3 * r + k] = Vin[3 * r + order[k]];
+    __syncthreads();
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+        const int a = E[2 * i], b = E[2 * i + 1];
+        if (a < 0 || b < 0 || a >= nv || b >= nv) {
+            sBad = 2;
+            continue;
+        }
+        const double ev0 = V[3 * a] - V[3 * b], ev1 = V[3 * a + 1] - V[3 * b + 1], ev2 = V[3 * a + 2] - V[3 * b + 2];
+        el[i] = sqrt(ev0 * ev0 + ev1 * ev1 + ev2 * ev2);
+        const double n0 = ev1, n1 = -ev0, n2 = ev2;  // rotation about z
+        const double len = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+        en[3 * i] = len > 0 ? n0 / len : n0;
+        en[3 * i + 1] = len > 0 ? n1 / len : n1;
+        en[3 * i + 2] = len > 0 ? n2 / len : n2;
+    }
+    __syncthreads();
+    if (sBad) {
+        if (threadIdx.x == 0) *bad = sBad;
+        return;
+    }
+    // extremes of x and y (exact in any order)
+    double mx = -INFINITY, mn = INFINITY, my = -INFINITY, mny = INFINITY;
+    for (int r = threadIdx.x; r < nv; r += blockDim.x) {
+        mx = fmax(mx, V[3 * r]);
+        mn = fmin(mn, V[3 * r]);
+        my = fmax(my, V[3 * r + 1]);
+        mny = fmin(mny, V[3 * r + 1]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        my = fmax(my, __shfl_xor_sync(0xffffffffu, my, o));
+        mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    }
+    if (lane == 0) {
+        red[0][w] = mx;
+        red[1][w] = mn;
+        red[2][w] = my;
+        red[3][w] = mny;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < nw; ++q) {
+            mx = fmax(mx, red[0][q]);
+            mn = fmin(mn, red[1][q]);
+            my = fmax(my, red[2][q]);
+            mny = fmin(mny, red[3][q]);
+        }
+        const float maxX = (float)mx, minX = (float)mn, maxY = (float)my, minY = (float)mny;
+        sMaxX = maxX;
+        sMult = (float)(0.1 * (double)fminf(fabsf(maxX - minX), fabsf(maxY - minY)));
+    }
+    __syncthreads();
+    // does the offset curve reach past maxX?  (utils.cpp:120-133, with the
+    // reference's pairing of vertex r with edge r's normal)
+    double mm = -INFINITY;
+    const double mult = (double)sMult;
+    for (int r = threadIdx.x; r < nv; r += blockDim.x) mm = fmax(mm, V[3 * r] + mult * en[3 * r]);
+    for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+    if (lane == 0) red[0][w] = mm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < nw; ++q) mm = fmax(mm, red[0][q]);
+        sMm = mm;
+    }
+    __syncthreads();
+    // flipping every edge normal negates every sum below exactly
+    const double sign = (float)sMm < sMaxX ? -1.0 : 1.0;
+    for (int j = threadIdx.x; j < nv; j += blockDim.x) {
+        const int ip = j == 0 ? nv - 1 : j - 1;
+        double v[3];
+        for (int k = 0; k < 3; ++k) v[k] = el[ip] * (sign * en[3 * ip + k]) + el[j] * (sign * en[3 * j + k]);
+        const double len = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int k = 0; k < 3; ++k) out[3 * j + k] = len > 0 ? v[k] / len : v[k];
+    }
+}
+
+cudaError_t launch_normals_3d(const double* V, long long nv, const int* F, long long nf, double* fn, int* deg,
+                              int* off, int* cursor, int* list, double* out, int* bad, cudaStream_t s) {
+    const int threads = 256;
+    const int fb = (int)std::min<long long>(std::max<long long>(1, (nf + threads - 1) / threads), 4096);
+    const int vb = (int)std::min<long long>(std::max<long long>(1, (nv + threads - 1) / threads), 4096);
+    face_normals_kernel<<<fb, threads, 0, s>>>(V, nv, F, nf, fn, deg, bad);
+    exclusive_scan_kernel<<<1, 1024, 0, s>>>(deg, nv, off);
+    face_lists_kernel<<<fb, threads, 0, s>>>(F, nv, nf, off, cursor, list);
+    vertex_normals_kernel<<<vb, threads, 0, s>>>(fn, nv, off, list, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normals_2d(const double* Vin, int nv, const int* E, double* V, double* en, double* el, double* out,
+                              int* bad, cudaStream_t s) {
+    curve_normals_kernel<<<1, 256, 0, s>>>(Vin, nv, E, V, en, el, out, bad);
+    return cudaGetLastError();
+}
+
 // Host wrappers -------------------------------------------------------------
 // Persistent grid of a stream pass: as many CTAs as can be resident at once
 // (one full wave; a partial second wave would double the pass).
@@ -829,9 +1083,10 @@ cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* e
     return cudaGetLastError();
 }
 cudaError_t launch_conj_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
-                                       double coef, double* grad, cudaStream_t s) {
+                                       double coef, double coefT, long long argmax, double* grad, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
-    conj_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, grad);
+    conj_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, coefT, argmax,
+                                                                      grad);
     return cudaGetLastError();
 }
 cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,

@@ -419,6 +419,9 @@ class Graph {
     double colScale[2] = {1.0, 1.0};
     int adjKind = 0;
     double adjT = 0;
+    double adjLambda = 0;     // the ratio result's C / T in double
+    double fdMax = 0;         // maxFd of the ("*", "feature") time column, as the energy used it
+    long long fdArgmax = 0;   // the first feat_diff entry holding the maximum
     DBuf<long long> wAdjEdges;
     DBuf<double> wImport;
     void backward_feat_diff(double grad, double* gradFd, bool accumulate);
@@ -428,6 +431,18 @@ class Graph {
     // -------------------------------------------------------------------
     void solve_ratio(int K);
     void solve_min_cost(int K);
+    // Batched ratio solves (pgc_solve_batch): the costs generated and
+    // rescaled and a one-CTA Bellman-Ford team prepared for the device's
+    // solve in `job`; then the result taken from the finished job, or the
+    // solve finished on the host when the device handed it back.
+    void batch_begin(int K, PairJob& job, int threads, size_t smemCap, bool regenerate);
+    void batch_end(const PairJob& job);
+    int batchK = 0;
+    size_t batchSmem = 0;  // dynamic shared memory the prepared batch team needs
+    size_t batch_smem_bytes() const { return batchSmem; }
+    DBuf<int> bRecNodes[2];
+    DBuf<long long> bRecEdges[2];
+    DBuf<double> bRecC[2], bRecT[2];
     void export_csv();
 
     // cost export / product space
@@ -453,6 +468,11 @@ class Graph {
         size_t smemBytes;   // dynamic shared memory per CTA
     };
     Run prepare_run(int K, bool ratio);
+    // batch mode of prepare_run: one CTA of batchThreads threads, DP records
+    // in global memory, staging only within batchSmemCap bytes
+    int batchThreads = 0;
+    size_t batchSmemCap = 0;
+    void solve_ratio_rescaled(int K);
     void ensure_workspace(int K, int blocks);
     std::vector<int> cta_cuts(int blocks, int K, int warps) const;
     void upload_cta_slices(const std::vector<int>& cut, int K, int warps);
@@ -585,8 +605,15 @@ void Graph::generate() {
         a.maxSO3 = (double)(float)robust_loss_host(2 * M_PI, rlAlpha, rlC, rlPwr);
         if (tm == FEATURE) {
             double m = -std::numeric_limits<double>::infinity();
-            for (double x : FD) m = std::max(m, x);
+            long long at = 0;
+            for (size_t i = 0; i < FD.size(); ++i)
+                if (FD[i] > m) {
+                    m = FD[i];
+                    at = (long long)i;
+                }
             a.maxFd = (double)(float)m;
+            fdMax = a.maxFd;
+            fdArgmax = at;
         }
         if (reg) {
             dNX.upload(NX.data(), NX.size(), s);
@@ -855,6 +882,35 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
         return bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(rowCap, costBytes, timeBytes);
     };
     const size_t tables = bf_shared_table_bytes(T.n, r.Kp);
+    if (batchThreads > 0) {
+        // one CTA of the batched launch: no shared DP tables; the two step
+        // buffers only when they fit the launch's shared-memory budget
+        r.threads = batchThreads;
+        r.blocks = 1;
+        r.coop = false;
+        r.sharedTables = false;
+        r.flagSync = 0;
+        int maxSl = 0, rowCap = 0;
+        size_t need = stage_need(1, maxSl, rowCap);
+        r.rowCap = rowCap;
+        r.stageSrcOnly = 0;
+        if (!stageOn || need > batchSmemCap) {
+            const size_t srcOnly = bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(rowCap, 0, 0);
+            if (stageOn && srcOnly <= batchSmemCap) {
+                r.stageSrcOnly = 1;
+                need = srcOnly;
+            } else {
+                r.rowCap = 0;
+                need = bf_stage_offset(maxSl);
+            }
+        }
+        if (need > batchSmemCap) throw Failure(PGC_ERR_ARG, "the graph's slice lists exceed the batch's shared memory");
+        r.maxCtaSlices = maxSl;
+        r.smemBytes = need;
+        ensure_workspace(K, 1);
+        upload_cta_slices(cut, K, r.threads / 32);
+        return r;
+    }
     int envBlocks = env_int("PGC_BF_BLOCKS", 0), envThreads = env_int("PGC_BF_THREADS", 0);
     if (!envBlocks) envBlocks = shapeBlocks;
     if (!envThreads) envThreads = shapeThreads;
@@ -1211,7 +1267,14 @@ void Graph::solve_ratio(int K) {
     // In-place rescale of the generator's costs (cost_time_ratio_solver.cpp:875-882).
     rescale_column(0, scaling);
     if (ncols > 1) rescale_column(1, scaling);
+    solve_ratio_rescaled(K);
+    (void)wall0;
+}
 
+// The ratio solve after the rescale: the initial upper bound, then branch
+// and bound with Lawler in each branch (cost_time_ratio_solver.cpp:741-864).
+void Graph::solve_ratio_rescaled(int K) {
+    const double scaling = 100000.0;
     Run r = prepare_run(K, true);
     reset_predecessors();
     const int n = T.n;
@@ -1414,7 +1477,144 @@ void Graph::solve_ratio(int K) {
     adjKind = 1;
     adjT = 0;
     for (double t : negativeCycle.t) adjT += t;
-    (void)wall0;
+    adjLambda = fin.ratio;
+}
+
+void Graph::batch_begin(int K, PairJob& J, int threads, size_t smemCap, bool regenerate) {
+    if (regenerate) generate();
+    else ensure_generated();
+    stats = Stats();
+    batchK = K;
+    const double scaling = 100000.0;
+    rescale_column(0, scaling);
+    if (ncols > 1) rescale_column(1, scaling);
+    batchThreads = threads;
+    batchSmemCap = smemCap;
+    Run r;
+    try {
+        r = prepare_run(K, true);
+    } catch (...) {
+        batchThreads = 0;
+        throw;
+    }
+    batchThreads = 0;
+    batchSmem = r.smemBytes;
+    reset_predecessors();
+    // PGC_BATCH_CYCLE_CAP (tests): a smaller record, so that graphs are
+    // handed back to the host
+    const long long capMax = std::min<long long>(kBatchCycleCap, std::max(1, env_int("PGC_BATCH_CYCLE_CAP", (int)kBatchCycleCap)));
+    const int cap = (int)std::min<long long>(numNodes() + 4, capMax);
+    for (int k = 0; k < 2; ++k) {
+        bRecNodes[k].alloc((size_t)cap + 1);
+        bRecEdges[k].alloc((size_t)cap);
+        bRecC[k].alloc((size_t)cap);
+        bRecT[k].alloc((size_t)cap);
+    }
+    J = PairJob{};
+    J.bf = params(r, 0, 0, 0.0, std::numeric_limits<float>::infinity());
+    J.bf.ctaSlice = wCtaSlice.p;
+    LookupArgs& a = J.lk;
+    a.n = T.n;
+    a.nY = T.nY;
+    a.numNodes = numNodes();
+    a.eBlock = T.eBlock;
+    a.spInter = dSp[INTER].p;
+    a.spIntra = dSp[INTRA].p;
+    a.srcInter = dSrc[INTER].p;
+    a.srcDummy = dSrcDummy.p ? dSrcDummy.p : dSrc[INTER].p;
+    a.srcIntra = dSrc[INTRA].p;
+    a.tedgeInter = dTedge[INTER].p;
+    a.tedgeIntra = dTedge[INTRA].p;
+    a.interEntries = T.entries[INTER];
+    a.layerStride = T.layerStride();
+    a.c64 = e64[0].p;
+    a.t64 = ncols > 1 ? e64[1].p : nullptr;
+    a.c32 = e64Stale[0] ? e32[0].p : nullptr;
+    a.t32 = ncols > 1 && e64Stale[1] ? e32[1].p : nullptr;
+    a.tconst = ncols > 1 ? 0.0 : scaling / 2;
+    J.branchOf = wBranch.p;
+    J.tconst = a.tconst;
+    for (int k = 0; k < 2; ++k) {
+        J.recNodes[k] = bRecNodes[k].p;
+        J.recEdges[k] = bRecEdges[k].p;
+        J.recC[k] = bRecC[k].p;
+        J.recT[k] = bRecT[k].p;
+    }
+    J.cap = cap;
+    J.status = PAIR_PENDING;
+    Control c{};
+    c.epoch = ctlEpoch;
+    PGC_CUDA(cudaMemcpyAsync(wCtl.p, &c, sizeof(Control), cudaMemcpyHostToDevice, stream));
+    PGC_CUDA(sync_stream());
+}
+
+void Graph::batch_end(const PairJob& J) {
+    Control c{};
+    d2h(&c, wCtl.p, sizeof(Control));
+    PGC_CUDA(sync_stream());
+    ctlEpoch = c.epoch;
+    stats.bfCalls = J.bfCalls;
+    stats.sweeps = J.sweeps;
+    stats.lawlerIters = J.lawlerIters;
+    stats.candidates = J.candidates;
+    stats.fallbackWalks = J.fallbackWalks;
+    stats.branches = 1;
+    stats.launches += 1;
+    {
+        int khz = 0;
+        if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) == cudaSuccess && khz > 0)
+            stats.deviceMs = (double)J.cycles / khz;  // the CTA's time on this graph at the top SM clock
+    }
+    stats.ctas = 1;
+    stats.threads = J.bf.maxCtaSlices >= 0 ? kBatchThreads : 0;
+    switch (J.status) {
+        case PAIR_DONE: {
+            std::vector<long long> edges((size_t)std::max(0, J.nEdges));
+            if (J.nEdges > 0) d2h(edges.data(), bRecEdges[J.rec].p, sizeof(long long) * edges.size());
+            PGC_CUDA(sync_stream());
+            resPasses = J.passes != 0;
+            resObjective = J.objective;
+            rows_for_edges(edges);
+            adjKind = 1;
+            adjT = J.adjT;
+            adjLambda = J.ratio;
+            return;
+        }
+        case PAIR_NAN:
+            stats.lawlerIters = 0;
+            resPasses = true;
+            resObjective = std::numeric_limits<float>::quiet_NaN();
+            rows_for_edges({});
+            adjKind = 0;
+            adjT = 0;
+            return;
+        case PAIR_HOST:
+            // branch and bound (or a cycle longer than the device record):
+            // the host's solve from the rescaled costs
+            stats = Stats();
+            solve_ratio_rescaled(batchK);
+            return;
+        case PAIR_ERR_WAIT:
+            wLayerFlag.zero(stream);
+            ctlEpoch = 0;
+            PGC_CUDA(sync_stream());
+            throw Failure(PGC_ERR_TIMEOUT, "a wait of the batched Bellman-Ford solve ran out");
+        case PAIR_ERR_UB:
+            throw Failure(PGC_ERR_INTERNAL, "no closed path through the upper-bound start node");
+        case PAIR_ERR_EDGE:
+            throw Failure(PGC_ERR_INTERNAL, "cycle edge not found in the product graph");
+        case PAIR_ERR_GUARD:
+            throw Failure(PGC_ERR_INTERNAL, "upper-bound ratio search does not terminate");
+        case PAIR_ERR_BF:
+            if (J.bfStatus == BF_ERR_EMPTY_BRANCH) throw Failure(PGC_ERR_INTERNAL, "no nodes in branch");
+            if (J.bfStatus == BF_ERR_CYCLE_CAP) throw Failure(PGC_ERR_INTERNAL, "cycle longer than its buffer");
+            if (J.bfStatus == BF_ERR_WALK) throw Failure(PGC_ERR_INTERNAL, "predecessor walk left the node range");
+            if (J.bfStatus == BF_ERR_CHUNK) throw Failure(PGC_ERR_INTERNAL, "a slice exceeds the shared-memory scratch");
+            if (J.bfStatus == BF_RUNNING) throw Failure(PGC_ERR_INTERNAL, "Bellman-Ford launch ended without a verdict");
+            throw Failure(PGC_ERR_INTERNAL, "unexpected Bellman-Ford status " + std::to_string(J.bfStatus));
+        default:
+            throw Failure(PGC_ERR_INTERNAL, "the batched solve ended without a verdict");
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1705,12 +1905,11 @@ void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
         // The conjugate energies read feat_diff once per edge, fd[x2, y2]:
         // in the cost column with slope 1 for ("vanilla", *) and
         // ("feature", *), not at all for the other cost modes.  Their time
-        // column reads it only in ("*", "feature") as max(fd) - fd, a
-        // maximum over the whole matrix, which is not differentiated here.
+        // column reads it only in ("*", "feature"), as max(0, maxFd - fd)
+        // (higherOrderDeformationEnergy.cpp:323-327); a ratio's adjoint
+        // takes its subgradient (conj_energy_backward_kernel).
         cm = string_to_mode(costName);
         tm = string_to_mode(timeName);
-        if (adjKind == 1 && tm == FEATURE)
-            throw Failure(PGC_ERR_MODE, "the ratio adjoint does not cover a time column that reads feat_diff (\"feature\")");
     }
     if (adjKind == 0 || !generated) throw Failure(PGC_ERR_STATE, "no ratio or minimum-cost result to differentiate");
     double coef = grad * colScale[0];
@@ -1722,8 +1921,15 @@ void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
     wAdjEdges.upload(resEdges.data(), resEdges.size(), stream);
     if (!conj) {
         PGC_CUDA(launch_plain_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coef, gradFd, stream));
-    } else if (cm == VANILLA || cm == FEATURE) {
-        PGC_CUDA(launch_conj_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coef, gradFd, stream));
+    } else {
+        // time part of a ratio: d lambda* / d t_e = -lambda* / T, scaled by
+        // the time column's rescale factor, times d t_e / d fd = -1
+        const double coefT = (adjKind == 1 && tm == FEATURE && ncols > 1) ? grad * adjLambda * colScale[1] / adjT : 0.0;
+        const double coefC = (cm == VANILLA || cm == FEATURE) ? coef : 0.0;
+        a.maxFd = fdMax;
+        if (coefC != 0.0 || coefT != 0.0)
+            PGC_CUDA(launch_conj_energy_backward(a, wAdjEdges.p, (int)resEdges.size(), T.eBlock, coefC, coefT, fdArgmax,
+                                                 gradFd, stream));
     }
     stats.launches++;
     PGC_CUDA(sync_stream());
@@ -1814,6 +2020,7 @@ void Graph::export_csv() {
 // ===========================================================================
 using pgc::Failure;
 using pgc::Graph;
+using pgc::PairJob;
 
 struct pgc_graph {
     Graph g;
@@ -2073,52 +2280,182 @@ int pgc_set_team_shape(pgc_graph* h, int ctas, int threads_per_cta) {
     });
 }
 
+namespace {
+// Phases of the calling thread's last pgc_solve_batch (pgc_batch_profile).
+thread_local double g_batchProfile[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+}  // namespace
+
+int pgc_batch_profile(double* out8) {
+    return guarded([&] {
+        if (!out8) throw Failure(PGC_ERR_ARG, "null output");
+        for (int i = 0; i < 8; ++i) out8[i] = g_batchProfile[i];
+    });
+}
+
 int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver, int max_depth, int ctas_per_graph,
                     int workers, int regenerate, int* status) {
     return guarded([&] {
+        for (double& x : g_batchProfile) x = 0;
+        const auto tStart = std::chrono::steady_clock::now();
         if (count < 0 || (count > 0 && (!graphs || !status))) throw Failure(PGC_ERR_ARG, "null argument");
         const std::string name = solver ? solver : "";
         const bool ratio = name == "lawlercpu" || name == "lawlergpu";
         if (workers <= 0) workers = 64;
-        if (ctas_per_graph <= 0) {
-            // the device runs at most 32 kernels side by side (host work
-            // queues): teams that together cover the SMs keep them all busy
-            int dev = 0, sms = 0;
-            PGC_CUDA(cudaGetDevice(&dev));
-            PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            ctas_per_graph = std::max(1, sms / (int)std::max<int64_t>(1, std::min<int64_t>(count, 32)));
-        }
-        workers = (int)std::min<int64_t>(workers, count);
-        std::atomic<int64_t> next{0};
+        workers = (int)std::max<int64_t>(1, std::min<int64_t>(workers, count));
         std::vector<std::string> errors((size_t)count);
-        auto work = [&] {
-            for (;;) {
-                const int64_t i = next.fetch_add(1);
-                if (i >= count) return;
-                pgc_graph* h = graphs[i];
-                if (!h) {
-                    status[i] = PGC_ERR_ARG;
-                    continue;
+        // Runs f(i) for every graph on the worker threads; a graph whose
+        // status is already a failure is skipped.
+        auto for_each_graph = [&](auto&& f) {
+            std::atomic<int64_t> next{0};
+            auto work = [&] {
+                for (;;) {
+                    const int64_t i = next.fetch_add(1);
+                    if (i >= count) return;
+                    if (status[i] != PGC_OK) continue;
+                    status[i] = f(i);
+                    if (status[i] != PGC_OK) errors[(size_t)i] = pgc_last_error();
                 }
+            };
+            std::vector<std::thread> pool;
+            for (int w = 1; w < workers; ++w) pool.emplace_back(work);
+            work();
+            for (auto& t : pool) t.join();
+        };
+        for (int64_t i = 0; i < count; ++i) status[i] = graphs[i] ? PGC_OK : PGC_ERR_ARG;
+        int dev = 0, sms = 0;
+        PGC_CUDA(cudaGetDevice(&dev));
+        PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (ratio && pgc::env_int("PGC_BATCH_STREAMS", 0) == 0) {
+            // One launch solves every graph: its CTAs take the graphs from a
+            // queue, largest first, and run each whole ratio solve on the
+            // device.  The costs are generated and rescaled per graph by the
+            // workers first; graphs whose first branch's cycle wraps are
+            // finished on the host afterwards, with branch and bound.
+            const int threads = pgc::kBatchThreads;
+            int smemOptin = 0;
+            PGC_CUDA(cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            const size_t smemCap = (size_t)std::max(0, smemOptin / pgc::kBatchBlocksPerSm - 2048);
+            std::vector<PairJob> jobs((size_t)count);
+            std::vector<int> costF32((size_t)count, 0), timeKind((size_t)count, 0);
+            std::vector<size_t> smemNeed((size_t)count, 0);
+            std::vector<double> work((size_t)count, 0);
+            for_each_graph([&](int64_t i) {
+                pgc_graph* h = graphs[i];
+                return guarded([&] {
+                    Graph& g = h->g;
+                    if (g.device != dev) throw Failure(PGC_ERR_ARG, "a batch's graphs must live on the current device");
+                    const int K = max_depth >= 1 ? max_depth : g.maxDepth;
+                    g.blockingSync = true;
+                    try {
+                        g.batch_begin(K, jobs[(size_t)i], threads, smemCap, regenerate != 0);
+                    } catch (...) {
+                        g.blockingSync = false;
+                        throw;
+                    }
+                    g.blockingSync = false;
+                    costF32[(size_t)i] = jobs[(size_t)i].bf.cost == (const void*)g.e32[0].p ? 1 : 0;
+                    timeKind[(size_t)i] = jobs[(size_t)i].bf.time == nullptr ? 0
+                                          : jobs[(size_t)i].bf.time == (const void*)g.e32[1].p ? 1 : 2;
+                    smemNeed[(size_t)i] = jobs[(size_t)i].bf.maxCtaSlices >= 0 ? g.batch_smem_bytes() : 0;
+                    work[(size_t)i] = (double)g.T.layerStride() * g.T.nY * K;
+                });
+            });
+            g_batchProfile[0] = ms_since(tStart);
+            const auto tKernel = std::chrono::steady_clock::now();
+            // one launch per (cost type, time kind) group, largest graphs first
+            pgc::DBuf<PairJob> dJobs;
+            pgc::DBuf<int> dNext;
+            cudaStream_t bs = nullptr;
+            PGC_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+            struct StreamGuard {
+                cudaStream_t s;
+                ~StreamGuard() { if (s) cudaStreamDestroy(s); }
+            } guard{bs};
+            std::vector<int64_t> order;
+            for (int64_t i = 0; i < count; ++i)
+                if (status[i] == PGC_OK) order.push_back(i);
+            std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+                const int gx = costF32[(size_t)x] * 3 + timeKind[(size_t)x], gy = costF32[(size_t)y] * 3 + timeKind[(size_t)y];
+                if (gx != gy) return gx < gy;
+                return work[(size_t)x] > work[(size_t)y];
+            });
+            std::vector<PairJob> packed(order.size());
+            for (size_t k = 0; k < order.size(); ++k) packed[k] = jobs[(size_t)order[k]];
+            if (!packed.empty()) {
+                dJobs.alloc(packed.size());
+                dNext.alloc(8);
+                PGC_CUDA(cudaMemcpyAsync(dJobs.p, packed.data(), sizeof(PairJob) * packed.size(),
+                                         cudaMemcpyHostToDevice, bs));
+                PGC_CUDA(cudaMemsetAsync(dNext.p, 0, 8 * sizeof(int), bs));
+                for (size_t k0 = 0, grp = 0; k0 < order.size(); ++grp) {
+                    size_t k1 = k0;
+                    size_t smem = 0;
+                    const int cf = costF32[(size_t)order[k0]], tk = timeKind[(size_t)order[k0]];
+                    while (k1 < order.size() && costF32[(size_t)order[k1]] == cf && timeKind[(size_t)order[k1]] == tk)
+                        smem = std::max(smem, smemNeed[(size_t)order[k1++]]);
+                    int perSm = 0;
+                    PGC_CUDA(pgc::bf_batch_max_blocks(cf, tk, threads, smem, &perSm));
+                    if (perSm < 1) throw Failure(PGC_ERR_CUDA, "the batched solve kernel cannot be resident");
+                    const int blocks = (int)std::min<size_t>(k1 - k0, (size_t)sms * (size_t)perSm);
+                    g_batchProfile[5] += blocks;
+                    g_batchProfile[6] = threads;
+                    g_batchProfile[7] = std::max(g_batchProfile[7], (double)smem);
+                    PGC_CUDA(pgc::launch_bf_batch(dJobs.p + k0, (int)(k1 - k0), dNext.p + grp % 8, cf, tk, blocks, threads,
+                                             smem, bs));
+                    k0 = k1;
+                }
+                PGC_CUDA(cudaMemcpyAsync(packed.data(), dJobs.p, sizeof(PairJob) * packed.size(),
+                                         cudaMemcpyDeviceToHost, bs));
+                PGC_CUDA(cudaStreamSynchronize(bs));
+                for (size_t k = 0; k < order.size(); ++k) jobs[(size_t)order[k]] = packed[k];
+            }
+            g_batchProfile[1] = ms_since(tKernel);
+            const auto tEnd = std::chrono::steady_clock::now();
+            for (const PairJob& J : jobs) {
+                if (J.status == pgc::PAIR_HOST) g_batchProfile[3] += 1;
+                if (J.status == pgc::PAIR_DONE || J.status == pgc::PAIR_NAN) g_batchProfile[4] += 1;
+            }
+            for_each_graph([&](int64_t i) {
+                return guarded([&] {
+                    Graph& g = graphs[i]->g;
+                    g.blockingSync = true;
+                    try {
+                        g.batch_end(jobs[(size_t)i]);
+                    } catch (...) {
+                        g.blockingSync = false;
+                        throw;
+                    }
+                    g.blockingSync = false;
+                });
+            });
+            g_batchProfile[2] = ms_since(tEnd);
+        } else {
+            // each graph on its own stream with a small team: the device runs
+            // at most 32 kernels side by side (host work queues), so teams
+            // that together cover the SMs keep them all busy
+            if (ctas_per_graph <= 0)
+                ctas_per_graph = std::max(1, sms / (int)std::max<int64_t>(1, std::min<int64_t>(count, 32)));
+            for_each_graph([&](int64_t i) {
+                pgc_graph* h = graphs[i];
                 const int saved = h->g.teamCap;
                 h->g.teamCap = ctas_per_graph;
                 h->g.blockingSync = true;
-                status[i] = regenerate ? pgc_generate(h) : PGC_OK;
-                if (status[i] == PGC_OK)
-                    status[i] = ratio ? pgc_solve_with_cost_time_ratio(h, solver, max_depth)
-                                      : pgc_solve_with_minimum_cost(h, solver, max_depth);
-                if (status[i] != PGC_OK) errors[(size_t)i] = pgc_last_error();
+                int rc = regenerate ? pgc_generate(h) : PGC_OK;
+                if (rc == PGC_OK)
+                    rc = ratio ? pgc_solve_with_cost_time_ratio(h, solver, max_depth)
+                               : pgc_solve_with_minimum_cost(h, solver, max_depth);
                 h->g.teamCap = saved;
                 h->g.blockingSync = false;
-            }
-        };
-        std::vector<std::thread> pool;
-        for (int w = 1; w < workers; ++w) pool.emplace_back(work);
-        work();
-        for (auto& t : pool) t.join();
+                return rc;
+            });
+        }
         for (int64_t i = 0; i < count; ++i)
             if (status[i] != PGC_OK)
-                throw Failure(status[i], "graph " + std::to_string(i) + " of the batch failed: " + errors[(size_t)i]);
+                throw Failure(status[i], "graph " + std::to_string(i) + " of the batch failed: " +
+                                             (graphs[i] ? errors[(size_t)i] : std::string("null handle")));
     });
 }
 
@@ -2221,90 +2558,68 @@ int pgc_product_graph_sizes(const int32_t* EX, int64_t nex, int64_t nvx, int64_t
     });
 }
 
+// utils::normals2d (helper/utils.cpp:93-157) on the device: the curve is
+// copied in, curve_normals_kernel computes the normals with the reference's
+// operations in its order, and they are copied back.
 int pgc_compute_normals_2d(const double* Vin, int64_t nv, const int32_t* E, int64_t ne, double* out) {
     return guarded([&] {
         if (nv < 0 || (nv > 0 && (!Vin || !E || !out))) throw Failure(PGC_ERR_ARG, "null argument");
         if (nv != ne) throw Failure(PGC_ERR_ARG, "V.rows() != E.rows()");
-        std::vector<double> V(Vin, Vin + 3 * nv);
-        int zero = -1;
-        for (int i = 0; i < 3; ++i) {
-            double s = 0;
-            for (int64_t r = 0; r < nv; ++r) s += V[(size_t)(3 * r + i)];
-            if (std::fabs(s) < 1e-4) { zero = i; break; }
-        }
-        if (zero == -1) throw Failure(PGC_ERR_ARG, "points dont lie on xy, xz or yz plane");
-        if (zero != 2) {
-            const int order[3] = {zero == 1 ? 0 : 1, 2, zero == 1 ? 1 : 0};
-            std::vector<double> W(V.size());
-            for (int64_t r = 0; r < nv; ++r)
-                for (int k = 0; k < 3; ++k) W[(size_t)(3 * r + k)] = V[(size_t)(3 * r + order[k])];
-            V.swap(W);
-        }
-        std::vector<double> en((size_t)(3 * ne)), el((size_t)ne);
-        for (int64_t i = 0; i < ne; ++i) {
-            const int a = E[2 * i], b = E[2 * i + 1];
-            const double ev[3] = {V[(size_t)(3 * a)] - V[(size_t)(3 * b)], V[(size_t)(3 * a + 1)] - V[(size_t)(3 * b + 1)],
-                                  V[(size_t)(3 * a + 2)] - V[(size_t)(3 * b + 2)]};
-            el[(size_t)i] = std::sqrt(ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2]);
-            // rotation about z: (x, y, z) -> (y, -x, z)
-            double nrm[3] = {ev[1], -ev[0], ev[2]};
-            const double len = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-            for (int k = 0; k < 3; ++k) en[(size_t)(3 * i + k)] = len > 0 ? nrm[k] / len : nrm[k];
-        }
-        float maxX = -INFINITY, minX = INFINITY, maxY = -INFINITY, minY = INFINITY;
-        {
-            double mx = -INFINITY, mn = INFINITY, my = -INFINITY, mny = INFINITY;
-            for (int64_t r = 0; r < nv; ++r) {
-                mx = std::max(mx, V[(size_t)(3 * r)]); mn = std::min(mn, V[(size_t)(3 * r)]);
-                my = std::max(my, V[(size_t)(3 * r + 1)]); mny = std::min(mny, V[(size_t)(3 * r + 1)]);
-            }
-            maxX = (float)mx; minX = (float)mn; maxY = (float)my; minY = (float)mny;
-        }
-        const float mult = (float)(0.1 * std::min(std::fabs(maxX - minX), std::fabs(maxY - minY)));
-        double mm = -INFINITY;
-        for (int64_t r = 0; r < nv; ++r) mm = std::max(mm, V[(size_t)(3 * r)] + (double)mult * en[(size_t)(3 * r)]);
-        if ((float)mm < maxX)
-            for (auto& x : en) x = -x;
-        for (int64_t i = 1; i < nv + 1; ++i) {
-            const int64_t j = i % nv;
-            double v[3];
-            for (int k = 0; k < 3; ++k)
-                v[k] = el[(size_t)(i - 1)] * en[(size_t)(3 * (i - 1) + k)] + el[(size_t)j] * en[(size_t)(3 * j + k)];
-            const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-            for (int k = 0; k < 3; ++k) out[3 * j + k] = len > 0 ? v[k] / len : v[k];
-        }
+        if (nv > INT_MAX / 3) throw Failure(PGC_ERR_ARG, "curve too long");
+        if (nv == 0) return;
+        cudaStream_t s = cudaStreamPerThread;
+        pgc::DBuf<double> dV, dW, dEn, dEl, dOut;
+        pgc::DBuf<int> dE, dBad;
+        dV.upload(Vin, (size_t)(3 * nv), s);
+        dE.upload(E, (size_t)(2 * ne), s);
+        dW.alloc((size_t)(3 * nv));
+        dEn.alloc((size_t)(3 * nv));
+        dEl.alloc((size_t)nv);
+        dOut.alloc((size_t)(3 * nv));
+        dBad.alloc(1);
+        dBad.zero(s);
+        PGC_CUDA(pgc::launch_normals_2d(dV.p, (int)nv, dE.p, dW.p, dEn.p, dEl.p, dOut.p, dBad.p, s));
+        int bad = 0;
+        PGC_CUDA(cudaMemcpyAsync(&bad, dBad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PGC_CUDA(cudaMemcpyAsync(out, dOut.p, sizeof(double) * (size_t)(3 * nv), cudaMemcpyDeviceToHost, s));
+        PGC_CUDA(cudaStreamSynchronize(s));
+        if (bad == 1) throw Failure(PGC_ERR_ARG, "points dont lie on xy, xz or yz plane");
+        if (bad == 2) throw Failure(PGC_ERR_ARG, "E refers to a vertex outside V");
     });
 }
 
 // utils::normals3d (helper/utils.cpp:86-90): libigl's per_vertex_normals
-// with its default (area) weighting -- the sum of the incident faces' unit
-// normals weighted by twice their area, i.e. of their edge cross products.
+// with its default (area) weighting -- per vertex the sum, in face order, of
+// its faces' edge cross products (unit normal times twice the area), scaled
+// to unit length; on the device (face_normals_kernel .. vertex_normals_kernel).
 int pgc_compute_normals_3d(const double* V, int64_t nv, const int32_t* F, int64_t nf, double* out) {
     return guarded([&] {
         if (nv < 0 || nf < 0 || (nv > 0 && (!V || !out)) || (nf > 0 && !F)) throw Failure(PGC_ERR_ARG, "null argument");
-        for (int64_t i = 0; i < 3 * nv; ++i) out[i] = 0.0;
-        for (int64_t f = 0; f < nf; ++f) {
-            const int a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
-            if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv)
-                throw Failure(PGC_ERR_ARG, "F refers to a vertex outside V");
-            double u[3], w[3];
-            for (int k = 0; k < 3; ++k) {
-                u[k] = V[3 * b + k] - V[3 * a + k];
-                w[k] = V[3 * c + k] - V[3 * a + k];
-            }
-            const double nrm[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
-            for (int k = 0; k < 3; ++k) {
-                out[3 * a + k] += nrm[k];
-                out[3 * b + k] += nrm[k];
-                out[3 * c + k] += nrm[k];
-            }
-        }
-        for (int64_t i = 0; i < nv; ++i) {
-            const double len = std::sqrt(out[3 * i] * out[3 * i] + out[3 * i + 1] * out[3 * i + 1] +
-                                         out[3 * i + 2] * out[3 * i + 2]);
-            if (len > 0)
-                for (int k = 0; k < 3; ++k) out[3 * i + k] /= len;
-        }
+        if (nv > INT_MAX / 3 || nf > INT_MAX / 3) throw Failure(PGC_ERR_ARG, "mesh too large");
+        if (nv == 0) return;
+        cudaStream_t s = cudaStreamPerThread;
+        pgc::DBuf<double> dV, dFn, dOut;
+        pgc::DBuf<int> dF, dDeg, dOff, dCur, dList, dBad;
+        dV.upload(V, (size_t)(3 * nv), s);
+        dF.alloc((size_t)std::max<int64_t>(1, 3 * nf));
+        if (nf > 0) PGC_CUDA(cudaMemcpyAsync(dF.p, F, sizeof(int) * (size_t)(3 * nf), cudaMemcpyHostToDevice, s));
+        dFn.alloc((size_t)std::max<int64_t>(1, 3 * nf));
+        dDeg.alloc((size_t)nv);
+        dDeg.zero(s);
+        dCur.alloc((size_t)nv);
+        dCur.zero(s);
+        dOff.alloc((size_t)nv + 1);
+        dList.alloc((size_t)std::max<int64_t>(1, 3 * nf));
+        dOut.alloc((size_t)(3 * nv));
+        dBad.alloc(1);
+        dBad.zero(s);
+        // faces with an index outside V are flagged and left out of every list
+        PGC_CUDA(pgc::launch_normals_3d(dV.p, nv, dF.p, nf, dFn.p, dDeg.p, dOff.p, dCur.p, dList.p, dOut.p, dBad.p, s));
+        int bad = 0;
+        PGC_CUDA(cudaMemcpyAsync(&bad, dBad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PGC_CUDA(cudaMemcpyAsync(out, dOut.p, sizeof(double) * (size_t)(3 * nv), cudaMemcpyDeviceToHost, s));
+        PGC_CUDA(cudaStreamSynchronize(s));
+        if (bad) throw Failure(PGC_ERR_ARG, "F refers to a vertex outside V");
     });
 }
 

@@ -78,6 +78,7 @@ def _declare(L):
     L.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.pgc_device_name.argtypes = [_h, ctypes.c_char_p, _i64]
+    L.pgc_batch_profile.argtypes = [_dp]
     L.pgc_last_error.restype = ctypes.c_char_p
     L.pgc_version.restype = ctypes.c_char_p
 
@@ -454,6 +455,18 @@ def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas
     _check(_lib.pgc_solve_batch(arr, len(gens), str(solver_name).encode(), -1 if max_depth is None else int(max_depth),
                                 int(ctas_per_graph), int(workers), int(bool(regenerate)), status))
     return [g._result() for g in gens]
+
+
+def last_batch_profile() -> dict:
+    """Where this thread's last solve_batch spent its time (no counterpart in
+    the reference): host wall-clock ms of preparing the graphs, of the
+    launch that solved them, and of taking the results over (or finishing
+    handed-back graphs on the host); graph counts; the launch's shape."""
+    buf = (ctypes.c_double * 8)()
+    _check(_lib.pgc_batch_profile(buf))
+    keys = ["prepare_ms", "launch_ms", "finish_ms", "handed_back", "solved_on_device", "ctas", "threads_per_cta",
+            "smem_bytes"]
+    return dict(zip(keys, list(buf)))
 
 
 def vertex_correspondences(matching, conjugate: bool | None = None) -> np.ndarray:

@@ -1,6 +1,8 @@
 """C ABI of libpgc.so without a GPU: the library loads, exports every entry
 point that include/pgc.h declares, and its host-only helpers and argument
-checks behave like the reference."""
+checks behave like the reference.  (The normals helpers run on the device:
+tests/test_gpu_normals.py; their restatement in the oracle is checked on the
+CPU in tests/test_oracle_normals.py.)"""
 import ctypes
 import os
 import re
@@ -28,41 +30,6 @@ def test_library_exports_every_declared_symbol(cpg):
 
 def test_library_is_sm100a_build(cpg):
     assert "sm_100a" in cpg.version()
-
-
-def test_normals_2d_matches_reference_rule(cpg):
-    from cyclic_product_graphs import synthetic
-
-    m = 37
-    t = np.linspace(0, 2 * np.pi, m, endpoint=False)
-    # off the origin: the reference picks the plane by the first coordinate
-    # column whose SUM is ~0 (utils.cpp:102-108), so a centred curve would be
-    # taken to lie in the yz-plane
-    V = np.stack([3 + 2 * np.cos(t), 1 + np.sin(t), np.zeros(m)], axis=1)
-    E = np.stack([np.arange(m), (np.arange(m) + 1) % m], axis=1).astype(np.int32)
-    got = cpg.compute_normals_2d(V, E)
-    want = synthetic.normals_2d(V, E)
-    np.testing.assert_allclose(got, want, atol=1e-12)
-    # outward: the normal at the rightmost point points to +x
-    assert got[0, 0] > 0.99
-
-
-def test_normals_2d_rejects_non_planar(cpg):
-    V = np.random.default_rng(0).normal(size=(5, 3)) + 1.0
-    E = np.stack([np.arange(5), (np.arange(5) + 1) % 5], axis=1)
-    with pytest.raises(cpg.PGCError, match="plane"):
-        cpg.compute_normals_2d(V, E)
-
-
-def test_normals_3d_area_weighted(cpg):
-    from cyclic_product_graphs import synthetic
-
-    V, F = synthetic.icosphere(2)
-    got = cpg.compute_normals_3d(V, F)
-    np.testing.assert_allclose(got, synthetic.vertex_normals(V, F), atol=1e-12)
-    np.testing.assert_allclose(np.linalg.norm(got, axis=1), 1.0, atol=1e-12)
-    # on the unit sphere the normals are the positions
-    np.testing.assert_allclose(got, V / np.linalg.norm(V, axis=1, keepdims=True), atol=0.05)
 
 
 def test_create_rejects_bad_shapes(cpg):

@@ -5,13 +5,21 @@
   (1e5 / (2 max(median, 0.001))) and T = sum of the cycle's rescaled times.
 * The minimum-cost adjoint agrees with central finite differences
   (h = 1e-3) at points where the cycle does not change within +-h.
+* The ratio adjoint agrees with central finite differences of
+  lambda = s_c C(fd) / (s_t T(fd)) over the solved cycle, the rescale factors
+  s held fixed (rounding passed straight through), where the cycle does not
+  change within +-h: plain graphs (also at the differentiation
+  configuration's size, 2,000 x 100, K = 2) and the conjugate mode whose time
+  column reads feat_diff, max(0, maxFd - fd).
 * torch carries the gradient on to learnable features; the batched forward
   gives the single-pair results and gradients.
 * Blackbox interpolation reproduces its definition -(y(w) - y(w + tau g)) / tau,
   with both solves recomputed independently by the oracle.
 * Conjugate graph: the adjoint scatters into fd[x2, y2] of every cycle edge
-  (ratio: the rescale factor over T; minimum cost: 1), and a ratio whose time
-  column reads feat_diff ("feature") is refused.
+  (ratio: the rescale factor over T; minimum cost: 1); a ratio whose time
+  column reads feat_diff ("feature": max(0, maxFd - fd)) adds lambda* s_t / T
+  at fd[x2, y2] of every cycle edge with a positive time and subtracts it at
+  the matrix maximum's entry (a subgradient).
 """
 import numpy as np
 import pytest
@@ -211,8 +219,102 @@ def test_conjugate_min_cost_adjoint_and_unsupported_time_mode(cpg, oracle):
     for e in o.last_cycle_edges():
         want[ps[e][5], ps[e][2]] += 1.0
     np.testing.assert_allclose(_device_grad(g, want.shape, 3.0), 3.0 * want, rtol=1e-12, atol=1e-18)
-    # a time column that reads feat_diff through its maximum is not differentiated
-    g2, _ = _conj_gens(cpg, oracle, p, True, "robustso3", "feature")
-    g2.solve_with_cost_time_ratio("lawlergpu", 2)
-    with pytest.raises(cpg.PGCError, match="feature"):
-        _device_grad(g2, p["feat_diff"].shape)
+
+
+@pytest.mark.parametrize("cost,time", [("robustso3", "feature"), ("plainso3", "feature")])
+def test_conjugate_feature_time_adjoint_matches_gradient_from_oracle_cycle(cpg, oracle, cost, time):
+    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=13)
+    g, o = _conj_gens(cpg, oracle, p, True, cost, time)
+    raw = o.get_cost_vector()
+    K = 2
+    try:
+        ro = o.solve_with_cost_time_ratio("lawlercpu", K)
+    except RuntimeError:
+        pytest.skip("the reference stops with no nodes in branch on this pair")
+    rg = g.solve_with_cost_time_ratio("lawlergpu", K)
+    assert rg[1] == ro[1] and np.array_equal(rg[2], ro[2])
+    edges = o.last_cycle_edges()
+    scaled = o.get_cost_vector()
+    C, T = scaled[edges, 0].sum(), scaled[edges, 1].sum()  # integers: exact in any order
+    lam = C / T
+    s_t = 1e5 / (2 * max(np.median(raw[:, 1]), 0.001))
+    fd = p["feat_diff"]
+    max_fd = float(np.float32(fd.max()))
+    argmax = np.unravel_index(int(np.argmax(fd)), fd.shape)
+    ps = o.get_product_space()
+    want = np.zeros(fd.shape)
+    for e in edges:  # the cost column (SO(3) terms) does not read feat_diff
+        y2, x2 = ps[e][2], ps[e][5]
+        if max_fd - fd[x2, y2] > 0:
+            want[x2, y2] += lam * s_t / T
+            want[argmax] -= lam * s_t / T
+    got = _device_grad(g, want.shape)
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-16)
+
+
+def _ratio_fd_check(cpg, g, make, fd0, K, h, directions, seed, tol):
+    """Central differences of lambda = s_c C / (s_t T) over the solved cycle
+    with the solve's rescale factors held fixed, along random directions
+    where the cycle (and the matrix maximum's entry) stays the same within
+    +-h, against the adjoint.  Returns how many directions were checked."""
+    raw = g.get_cost_vector()
+    g.solve_with_cost_time_ratio("lawlergpu", K)
+    scaled = g.get_cost_vector()
+    s = scaled.sum(axis=0) / raw.sum(axis=0)  # the factors (rounding averages out over every edge)
+    edges = g.last_cycle_edges()
+    edges_sorted = np.sort(edges)
+    grad = _device_grad(g, fd0.shape)
+    probe = make()
+
+    def lam_fixed(fd):
+        probe.set_feat_diff(fd)
+        c = probe.get_cost_vector()
+        C = s[0] * c[edges, 0].sum()
+        T = s[1] * c[edges, 1].sum() if c.shape[1] > 1 else 5e4 * len(edges)
+        return C / T
+
+    def same_cycle(fd):
+        probe.set_feat_diff(fd)
+        probe.solve_with_cost_time_ratio("lawlergpu", K)
+        return np.array_equal(np.sort(probe.last_cycle_edges()), edges_sorted)
+
+    rng = np.random.default_rng(seed)
+    checked = 0
+    for _ in range(directions):
+        d = rng.standard_normal(fd0.shape)
+        plus, minus = fd0 + h * d, fd0 - h * d
+        if np.argmax(plus) != np.argmax(fd0) or np.argmax(minus) != np.argmax(fd0):
+            continue
+        if not (same_cycle(plus) and same_cycle(minus)):
+            continue
+        fdiff = (lam_fixed(plus) - lam_fixed(minus)) / (2 * h)
+        analytic = float((grad * d).sum())
+        assert abs(fdiff - analytic) <= tol * abs(analytic) + 1e-9, (fdiff, analytic)
+        checked += 1
+    return checked
+
+
+@pytest.mark.parametrize("nv,m,K,seed", [(150, 10, 2, 3), (2000, 100, 2, 100000)])
+def test_ratio_adjoint_matches_central_differences(cpg, oracle, nv, m, K, seed):
+    p = synthetic.make_pair(n_vertices=nv, n_curve=m, feat_dim=64 if nv >= 2000 else 16, seed=seed)
+
+    def make():
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], False, False, False)
+        g.set_cost_time_ratio_mode("vanilla", "nomode")
+        return g
+
+    assert _ratio_fd_check(cpg, make(), make, p["feat_diff"].copy(), K, 1e-3, 6, seed, 1e-3) >= 3
+
+
+@pytest.mark.parametrize("cost", ["robustso3", "plainso3"])
+def test_conjugate_feature_time_adjoint_matches_central_differences(cpg, oracle, cost):
+    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=13)
+
+    def make():
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], True, True, False)
+        g.set_normals(p["NX"], p["NY"])
+        g.set_cost_time_ratio_mode(cost, "feature")
+        return g
+
+    # h = 1e-2: maxFd passes through float, whose spacing near the maximum is ~1e-6
+    assert _ratio_fd_check(cpg, make(), make, p["feat_diff"].copy(), 2, 1e-2, 8, 4, 2e-3) >= 3

@@ -1,7 +1,12 @@
 """Batched solves (solve_batch / pgc_solve_batch): many graphs of uneven size
 solved concurrently with one-CTA teams must return exactly what the oracle
 returns for each of them, for the ratio and the minimum-cost solver, and a
-failing member must be reported without affecting the others."""
+failing member must be reported without affecting the others.
+
+Ratio solves run in one launch whose CTAs each solve whole graphs on the
+device; a graph whose cycle needs branch and bound, or outgrows the device's
+cycle record, is handed back to the host.  Both routes, and the route with
+one stream and launch sequence per graph (PGC_BATCH_STREAMS=1), must agree."""
 import numpy as np
 import pytest
 
@@ -71,3 +76,46 @@ def test_batch_rejects_repeated_generators(cpg, oracle):
     g, _ = _build(cpg, oracle, _specs()[0])
     with pytest.raises(ValueError):
         cpg.solve_batch([g, g], "lawlergpu", 2)
+
+
+def test_batch_device_solves_equal_the_stream_route(cpg, oracle, monkeypatch):
+    pairs = [_build(cpg, oracle, s) for s in _specs()]
+    gens = [g for g, _ in pairs]
+    device = cpg.solve_batch(gens, "lawlergpu", None, regenerate=True)
+    monkeypatch.setenv("PGC_BATCH_STREAMS", "1")
+    streams = cpg.solve_batch(gens, "lawlergpu", None, regenerate=True)
+    for a, b in zip(device, streams):
+        _same(a, b)
+
+
+def test_batch_hands_long_cycles_back_to_the_host(cpg, oracle, monkeypatch):
+    """With a cycle record of 8 edges every graph is handed back to the host,
+    which finishes it from the rescaled costs: the answers do not change."""
+    monkeypatch.setenv("PGC_BATCH_CYCLE_CAP", "8")
+    pairs = [_build(cpg, oracle, s) for s in _specs()[:5]]
+    got = cpg.solve_batch([g for g, _ in pairs], "lawlergpu", None, regenerate=True)
+    for (g, o), res in zip(pairs, got):
+        _same(res, o.solve_with_cost_time_ratio("lawlercpu"))
+
+
+def test_batch_adjoint_after_device_solves(cpg, oracle):
+    """The adjoint of a batched ratio solve equals the adjoint after a single
+    solve of the same graph (the device solve records the cycle and its time
+    sum the same way)."""
+    import torch
+
+    pairs = [_build(cpg, oracle, s) for s in _specs()[:3]]
+    gens = [g for g, _ in pairs]
+    cpg.solve_batch(gens, "lawlergpu", None, regenerate=True)
+    grads = []
+    for g, spec in zip(gens, _specs()[:3]):
+        p = synthetic.make_pair(n_vertices=spec[0], n_curve=spec[1], feat_dim=16, seed=spec[4])
+        buf = torch.zeros(p["feat_diff"].shape, dtype=torch.float64, device="cuda")
+        g.backward_feat_diff(1.0, buf.data_ptr())
+        grads.append(buf.cpu().numpy())
+    for g, gb in zip(gens, grads):
+        g.generate()
+        g.solve_with_cost_time_ratio("lawlergpu")
+        buf = torch.zeros(gb.shape, dtype=torch.float64, device="cuda")
+        g.backward_feat_diff(1.0, buf.data_ptr())
+        assert np.array_equal(buf.cpu().numpy(), gb)

@@ -11,7 +11,7 @@ their stated sizes, through the public API.
   thread, since the reference's cycle choice races between OpenMP threads --
   come from tests/golden/scale_cases.json (tests/golden/make_scale_golden.py)
   when the regenerated inputs have the fixture's digest, else from an oracle
-  run on the spot.
+  run on the spot.  The plain pairs are also solved together as one batch.
 * The large pruned conjugate configuration's layer (20,000-vertex mesh,
   K = 4, SO(3) robust cost against feature time, regulariser on) at 20 curve
   points instead of 500: the device's energies agree with the oracle's within
@@ -63,6 +63,22 @@ def test_stated_size_matches_oracle(cpg, oracle, case, solver):
     want = _expected(oracle, case, pair)[solver]
     g = si.generator(cpg.product_graph_generator, case, pair)
     _check(g, _solve(g, solver, case["k"]), want)
+
+
+def test_stated_size_pairs_solved_as_one_batch(cpg, oracle):
+    """The eight batched-serving pairs and the four differentiation pairs
+    solved together by one batched launch (each CTA runs whole ratio solves
+    on the device): every pair's answer is the oracle's."""
+    cases = si.CFG2 + si.CFG3
+    pairs = [si.make_inputs(c) for c in cases]
+    gens = []
+    for c, p in zip(cases, pairs):
+        g = si.generator(cpg.product_graph_generator, c, p)
+        g.set_max_depth_cost_time_ratio(c["k"])
+        gens.append(g)
+    got = cpg.solve_batch(gens, "lawlergpu", None, regenerate=True)
+    for c, p, g, res in zip(cases, pairs, gens, got):
+        _check(g, res, _expected(oracle, c, p)["ratio"])
 
 
 def test_fixture_inputs_are_reproduced():
