@@ -153,18 +153,21 @@ int pgc_set_team_cap(pgc_graph* g, int max_ctas);
  * results do not depend on it. */
 int pgc_set_team_shape(pgc_graph* g, int ctas, int threads_per_cta);
 
-/* No reference counterpart.  Solves `count` graphs concurrently: each one as
- * pgc_solve_with_cost_time_ratio (solver "lawlercpu"/"lawlergpu") or
- * pgc_solve_with_minimum_cost (any other name) would, on its own stream with
- * a team of at most `ctas_per_graph` CTAs (0: SMs / min(count, 32), so the
- * teams the device runs side by side cover its SMs), driven by `workers`
- * host threads (0: 64; waiting threads sleep).  Graphs run side by side only as
- * far as the device has host work queues: start the process with
- * CUDA_DEVICE_MAX_CONNECTIONS=32 (the Python package sets it as a default
- * before CUDA starts); with the CUDA default of 8, streams share queues and
- * the batch runs about 3x slower.  With
- * `regenerate` != 0 each graph first recomputes its
- * edge costs (pgc_generate).  Each graph's result is read afterwards with
+/* No reference counterpart.  Solves `count` graphs concurrently, each with
+ * the result pgc_solve_with_cost_time_ratio (solver "lawlercpu"/"lawlergpu")
+ * or pgc_solve_with_minimum_cost (any other name) would give it.
+ * Ratio solvers: `workers` host threads (0: 64) generate and rescale every
+ * graph's costs; then one persistent launch runs each graph's whole ratio
+ * solve on the device, teams of `ctas_per_graph` CTAs (0: the environment's
+ * PGC_BATCH_TEAM, else 8) taking the graphs largest first; a graph whose
+ * first-branch cycle wraps is finished on the host with branch and bound.
+ * PGC_BATCH_STREAMS=1 selects the route of the other solvers instead.
+ * Other solvers: each graph on its own stream with a team of at most
+ * `ctas_per_graph` CTAs (0: SMs / min(count, 32)); graphs run side by side
+ * only as far as the device has host work queues, so start the process with
+ * CUDA_DEVICE_MAX_CONNECTIONS=32 (CUDA's default of 8 runs such a batch about
+ * 3x slower).  With `regenerate` != 0 each graph first recomputes its edge
+ * costs (pgc_generate).  Each graph's result is read afterwards with
  * pgc_result*; status[i] receives its return code.  Returns PGC_OK when all
  * succeeded, else the first failure's code (with its message).  The handles
  * must be distinct. */

@@ -242,6 +242,7 @@ struct PairJob {
     double* recC[2];
     double* recT[2];
     int cap;
+    int ctas;              // CTAs of the Bellman-Ford team bf was prepared for
     // outputs
     int status;            // PairStatus
     int bfStatus;          // the failing call's status for PAIR_ERR_BF
@@ -256,6 +257,7 @@ struct PairJob {
 };
 
 constexpr int kStepDoneStride = 8;  // one 32-byte sector per CTA step counter
+constexpr int kTeamWordStride = 8;  // words of a batched-solve team (one sector)
 // Polls of a device wait before it gives up (~2 s with its back-off).
 constexpr unsigned kDefaultSpinLimit = 1u << 24;
 // Predecessor loads a literal walk advances per round between team barriers.
@@ -291,14 +293,24 @@ __host__ __device__ inline size_t bf_stage_offset(int maxCtaSlices) {
 __host__ __device__ inline size_t bf_stage_buffer_bytes(int rowCap, int costBytes, int timeBytes) {
     return (size_t)rowCap * 32 * (4 + costBytes + timeBytes);
 }
+// Attributes of a device that stay fixed while the process runs, queried
+// once per device (attribute queries can go to the driver and serialise
+// between host threads).
+struct DeviceInfo {
+    int sms, smemOptin, clockKhz;
+};
+cudaError_t device_info(int device, DeviceInfo* out);
 cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
                       bool sharedTables, size_t smemBytes, cudaStream_t stream);
 cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream);
 // Batched ratio solves: `count` jobs taken from a queue (*next, zeroed by the
-// caller) by `blocks` CTAs of `threads` threads.
-cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, int costIsF32, int timeKind, int blocks,
-                            int threads, size_t smemBytes, cudaStream_t stream);
+// caller) by teams of `teamCtas` CTAs (blocks / teamCtas teams) of `threads`
+// threads.  teamWords: kTeamWordStride zeroed words per team; spin: polls of
+// a team barrier before it gives up.
+cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamWords, int teamCtas, unsigned spin,
+                            int costIsF32, int timeKind, int blocks, int threads, size_t smemBytes,
+                            cudaStream_t stream);
 cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);

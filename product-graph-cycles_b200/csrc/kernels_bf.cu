@@ -40,6 +40,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <set>
+#include <tuple>
 
 #include "device_common.cuh"
 
@@ -937,19 +941,19 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
     // (each record is written once, by one thread)
     for (long long r = tid; r < 2LL * n * Kp; r += nth) {
         const long long node = (r / Kp) % n;
-        const bool start = r < (long long)n * Kp && r % Kp == 0 && p.branchOf[node] == p.branchId;
+        const bool start = r < (long long)n * Kp && r % Kp == 0 && __ldcg(p.branchOf + node) == p.branchId;
         p.dv[r] = start ? 0.0 : kInfD;
         p.doh[r] = make_int2(kLapUnknown, 0);  // every (origin, hops) word, in either layout
     }
     for (long long i = tid; i < n; i += nth) {
         p.bak[i] = kInfD;
-        if (p.branchOf[i] == p.branchId) p.pred[i] = -1;
+        if (__ldcg(p.branchOf + i) == p.branchId) p.pred[i] = -1;
     }
     {
         // branch size and the last branch node (the reference's indexNodeInLayer)
         int last = -1, cnt = 0;
         for (long long i = tid; i < n; i += nth)
-            if (p.branchOf[i] == p.branchId) { ++cnt; last = (int)i; }
+            if (__ldcg(p.branchOf + i) == p.branchId) { ++cnt; last = (int)i; }
         Key km{-(double)last, last < 0 ? 0x7fffffff : last};
         if (last < 0) km.v = 1.0;
         km = block_min(km, 0);
@@ -1067,7 +1071,7 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
             int anyFinite = 0;
             const size_t dRow = (size_t)(p.nY & 1) * n * Kp;
             for (long long i = tid; i < n; i += nth) {
-                if (p.branchOf[i] != p.branchId) { p.lbOut[i] = kInfD; p.originOut[i] = -1; continue; }
+                if (__ldcg(p.branchOf + i) != p.branchId) { p.lbOut[i] = kInfD; p.originOut[i] = -1; continue; }
                 const double lb = ldV<S>(p, lastRowBase + (size_t)i * Kp);
                 int o = ldOH<S>(p, dRow, (int)i, 0).x;
                 if (o < 0 && !isinf((float)lb)) o = dij_walk_end(p, (int)i);
@@ -1118,7 +1122,7 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
             const size_t wRow = (size_t)((p.nY - 1) & 1) * n * Kp;
             const long long layerSpan = (long long)n * K;
             for (long long i = tid; i < n; i += nth) {
-                if (p.branchOf[i] == p.branchId) {
+                if (__ldcg(p.branchOf + i) == p.branchId) {
                     const double cand = ldV<S>(p, lastRowBase + (size_t)i * Kp);
                     const double b = p.bak[i];
                     double* d0 = p.dv + (size_t)i * Kp;
@@ -1164,7 +1168,7 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
             long long decided = 0;
             for (long long i = tid; i < n; i += nth) {
                 int st = 0;
-                if (p.branchOf[i] == p.branchId) {
+                if (__ldcg(p.branchOf + i) == p.branchId) {
                     const double d0 = ldV<S>(p, (size_t)i * Kp);
                     if (d0 < 0) {
                         int v0 = -1;
@@ -1467,41 +1471,53 @@ __device__ CycleSums record_sums(const PairJob& J, int rec, int m, double lambda
     return {__ddiv_rn(C, T), W};
 }
 
+// The CTAs that solve one graph together: `all` is the whole team, with
+// its own barrier words; `bf` is its first bf.ncta CTAs, the Bellman-Ford
+// team the graph was prepared for (a graph with fewer 32-node slices than
+// the team has CTAs uses fewer), with the graph's Control barrier words.
+// The other CTAs skip the Bellman-Ford calls and wait at the next barrier.
+struct SolveTeam {
+    Team all, bf;
+    __device__ bool lead() const { return all.cta == 0 && threadIdx.x == 0; }
+    __device__ bool in_bf() const { return all.cta < bf.ncta; }
+};
+
 // A cycle from the Bellman-Ford walk in the cycle buffer (p(v0), ..., v0,
 // or the upper-bound path) into record `rec`: the walk reversed, closed with
 // the copy of its first node when `close`, and every consecutive pair's edge,
 // cost and time (a closing-layer target is its copy: b + numNodes when
-// b < n < a, cost_time_ratio_solver.cpp:109-111).  All threads of the CTA;
+// b < n < a, cost_time_ratio_solver.cpp:109-111).  All threads of the team;
 // returns the edge count, -1 when an edge is missing, -2 when the record is
-// too small.
-__device__ int record_cycle(const PairJob& J, const BfParams& P, int rec, int len, bool close) {
-    __shared__ int sMissing;
+// too small, -3 when a team barrier ran out.
+__device__ int record_cycle(const PairJob& J, const BfParams& P, const Team& t, int rec, int len, bool close) {
     const int count = len + (close ? 1 : 0);
     if (count > J.cap + 1 || len < 1) return -2;
     int* nodes = J.recNodes[rec];
     const long long nn = P.numNodes;
     const int n = P.n;
-    for (int i = threadIdx.x; i < len; i += blockDim.x) nodes[i] = __ldcg(P.cycleBuf + (len - 1 - i));
-    if (close && threadIdx.x == 0) nodes[len] = __ldcg(P.cycleBuf + (len - 1)) + (int)nn;
-    if (threadIdx.x == 0) sMissing = 0;
-    __syncthreads();
+    for (long long i = t.thread(); i < len; i += t.nthreads()) nodes[i] = __ldcg(P.cycleBuf + (len - 1 - i));
+    if (close && t.cta == 0 && threadIdx.x == 0) nodes[len] = __ldcg(P.cycleBuf + (len - 1)) + (int)nn;
+    if (!team_sync(t)) return -3;
     const int m = count - 1;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        const int a = nodes[i];
-        long long b = nodes[i + 1];
+    int missing = 0;
+    for (long long i = t.thread(); i < m; i += t.nthreads()) {
+        const int a = __ldcg(nodes + i);
+        long long b = __ldcg(nodes + i + 1);
         if (b < n && a > n) b += nn;
         long long e;
-        double c, t;
-        if (!lookup_edge(J.lk, a, b, &e, &c, &t)) {
-            sMissing = 1;
-            e = -2, c = 0, t = 0;
+        double c, tm;
+        if (!lookup_edge(J.lk, a, b, &e, &c, &tm)) {
+            missing = 1;
+            e = -2, c = 0, tm = 0;
         }
         J.recEdges[rec][i] = e;
         J.recC[rec][i] = c;
-        J.recT[rec][i] = t;
+        J.recT[rec][i] = tm;
     }
-    __syncthreads();
-    return sMissing ? -1 : m;
+    bool ok;
+    const int anyMissing = team_sync_or(t, missing, ok);
+    if (!ok) return -3;
+    return anyMissing ? -1 : m;
 }
 
 // Lawler's outcome of one Bellman-Ford call (the host driver's bellman_ford).
@@ -1512,16 +1528,45 @@ __device__ __noinline__ void bf_call(const BfParams& P, const Team& t, char* sme
     bf_body<CT, TK, false>(P, t, smem);
 }
 
-// The whole ratio solve of one graph by this CTA.  P is the job's
-// Bellman-Ford parameters in shared memory.
+// One Bellman-Ford call of the team: the lead publishes the call's state,
+// the Bellman-Ford CTAs run it, and every CTA reads its verdict after the
+// closing barrier.  False when a team barrier ran out.
 template <class CT, int TK>
-__device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
-    __shared__ int sState[4];        // [0] verdict, [1] done, [2] record of the negative cycle, [3] its edges
+__device__ bool team_bf_call(PairJob& J, const BfParams& P, const SolveTeam& S, char* smem, bool resetError) {
+    if (S.lead()) {
+        P.ctl->status = BF_RUNNING;
+        if (resetError) P.ctl->error = 0;
+    }
+    if (!team_sync(S.all)) return false;
+    if (S.in_bf()) bf_call<CT, TK>(P, S.bf, smem);
+    if (!team_sync(S.all)) return false;
+    if (S.lead()) {
+        J.bfCalls++;
+        J.sweeps += *(volatile int*)&P.ctl->sweeps;
+    }
+    return true;
+}
+
+// The whole ratio solve of one graph by the team.  P is the job's
+// Bellman-Ford parameters in each CTA's shared memory.  Work over nodes and
+// cycle edges is spread over the team's threads; the sums over a cycle run on
+// one thread of every CTA, in the same order, so every CTA takes the same
+// branches; only the lead writes the job's outputs.
+template <class CT, int TK>
+__device__ void pair_solve(PairJob& J, BfParams& P, const SolveTeam& S, char* smem) {
+    __shared__ int sState[4];        // [1] the bound search gave up, [3] edges of the last record
     __shared__ double sRatio;
+    const Team& t = S.all;
+    const bool lead = S.lead();
     const int n = P.n;
     Control* ctl = P.ctl;
     const double tolerance = (double)(float)1e-8;
     const double ubInf = (double)__int_as_float(0x7f800000);
+#define PGC_TEAM_FAIL()                                \
+    do {                                               \
+        if (lead) J.status = PAIR_ERR_WAIT;            \
+        return;                                        \
+    } while (0)
 
     // ---- initial upper bound (cost_time_ratio_solver.cpp:652-707) ----
     // the layer-1 node with the lowest float mean in-cost among those with
@@ -1529,7 +1574,8 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
     Key best{kInfD, 0x7fffffff};
     {
         const CT* c1 = reinterpret_cast<const CT*>(P.cost) + P.layerStride;
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        for (long long vv = t.thread(); vv < n; vv += t.nthreads()) {
+            const int v = (int)vv;
             const int s = v >> 5, lane = v & 31;
             float mean = 0;
             int num = 0;
@@ -1550,36 +1596,39 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
             if (num > 3 && mean < __int_as_float(0x7f800000) && key_less(k, best)) best = k;
         }
         best = block_min(best, 0);
+        if (t.ncta > 1) {
+            // (value, index) keys are totally ordered: the team's minimum is
+            // the one-CTA scan's, however the nodes were split
+            if (threadIdx.x == 0) {
+                P.redVal[t.cta] = best.v;
+                P.redIdx[t.cta] = best.i;
+            }
+            if (!team_sync(t)) PGC_TEAM_FAIL();
+            best = Key{kInfD, 0x7fffffff};
+            for (int c = 0; c < t.ncta; ++c) {
+                const Key k{__ldcg(P.redVal + c), __ldcg(P.redIdx + c)};
+                if (key_less(k, best)) best = k;
+            }
+        }
     }
     const int startV = best.i == 0x7fffffff ? 0 : best.i;
-    for (int v = threadIdx.x; v < n; v += blockDim.x) J.branchOf[v] = v == startV ? 0 : 1;
+    for (long long v = t.thread(); v < n; v += t.nthreads()) J.branchOf[v] = v == startV ? 0 : 1;
     if (threadIdx.x == 0) {
         P.mode = 1;
         P.branchId = 0;
         P.lambda = 10;
         P.ub = ubInf;
-        ctl->status = BF_RUNNING;
-        ctl->error = 0;
     }
-    __syncthreads();
-    bf_call<CT, TK>(P, t, smem);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        J.bfCalls++;
-        J.sweeps += ctl->sweeps;
-    }
-    if (*(volatile int*)&ctl->error) {
-        if (threadIdx.x == 0) J.status = PAIR_ERR_WAIT;
-        return;
-    }
+    if (!team_bf_call<CT, TK>(J, P, S, smem, true)) PGC_TEAM_FAIL();
+    if (*(volatile int*)&ctl->error) PGC_TEAM_FAIL();
     {
         const int st = *(volatile int*)&ctl->status;
         if (st == BF_LAYER_UNREACHED) {  // the empty cycle's 0/0 bound: (true, NaN, no rows)
-            if (threadIdx.x == 0) J.status = PAIR_NAN;
+            if (lead) J.status = PAIR_NAN;
             return;
         }
         if (st != BF_UB_DONE) {
-            if (threadIdx.x == 0) {
+            if (lead) {
                 J.status = st < 0 ? PAIR_ERR_BF : PAIR_ERR_UB;
                 J.bfStatus = st;
             }
@@ -1588,9 +1637,10 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
     }
     int neg = 0;
     {
-        const int m = record_cycle(J, P, neg, *(volatile int*)&ctl->cycleLen, false);
+        const int m = record_cycle(J, P, t, neg, *(volatile int*)&ctl->cycleLen, false);
+        if (m == -3) PGC_TEAM_FAIL();
         if (m < 0) {
-            if (threadIdx.x == 0) J.status = m == -2 ? PAIR_HOST : PAIR_ERR_EDGE;
+            if (lead) J.status = m == -2 ? PAIR_HOST : PAIR_ERR_EDGE;
             return;
         }
         if (threadIdx.x == 0) {
@@ -1613,19 +1663,19 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
         }
         __syncthreads();
         if (sState[1]) {
-            if (threadIdx.x == 0) J.status = PAIR_ERR_GUARD;
+            if (lead) J.status = PAIR_ERR_GUARD;
             return;
         }
     }
     // A NaN or infinite bound: the host's branch-and-bound path (the heap
     // comparison that ends the first branch does not hold then).
     if (!(sRatio < (double)__int_as_float(0x7f800000))) {
-        if (threadIdx.x == 0) J.status = PAIR_HOST;
+        if (lead) J.status = PAIR_HOST;
         return;
     }
 
     // ---- the first branch: every node starts (cost_time_ratio_solver.cpp:794-829) ----
-    for (int v = threadIdx.x; v < n; v += blockDim.x) J.branchOf[v] = 0;
+    for (long long v = t.thread(); v < n; v += t.nthreads()) J.branchOf[v] = 0;
     double currentRatio = sRatio;  // every thread keeps the same copy
     double oldRatio = currentRatio;
     int negEdges = sState[3];
@@ -1635,27 +1685,18 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
             P.branchId = 0;
             P.lambda = currentRatio;
             P.ub = ubInf;
-            ctl->status = BF_RUNNING;
         }
-        __syncthreads();
-        bf_call<CT, TK>(P, t, smem);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            J.bfCalls++;
-            J.sweeps += ctl->sweeps;
-            J.lawlerIters++;
-        }
-        if (*(volatile int*)&ctl->error) {
-            if (threadIdx.x == 0) J.status = PAIR_ERR_WAIT;
-            return;
-        }
+        if (!team_bf_call<CT, TK>(J, P, S, smem, false)) PGC_TEAM_FAIL();
+        if (lead) J.lawlerIters++;
+        if (*(volatile int*)&ctl->error) PGC_TEAM_FAIL();
         const int st = *(volatile int*)&ctl->status;
         int outcome;
         if (st == BF_FOUND_CYCLE) {
             const int cand = neg ^ 1;
-            const int m = record_cycle(J, P, cand, *(volatile int*)&ctl->cycleLen, true);
+            const int m = record_cycle(J, P, t, cand, *(volatile int*)&ctl->cycleLen, true);
+            if (m == -3) PGC_TEAM_FAIL();
             if (m < 0) {
-                if (threadIdx.x == 0) J.status = m == -2 ? PAIR_HOST : PAIR_ERR_EDGE;
+                if (lead) J.status = m == -2 ? PAIR_HOST : PAIR_ERR_EDGE;
                 return;
             }
             if (threadIdx.x == 0) {
@@ -1682,7 +1723,7 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
             __syncthreads();
             outcome = sState[0];
         } else {
-            if (threadIdx.x == 0) {
+            if (lead) {
                 J.status = PAIR_ERR_BF;
                 J.bfStatus = st;
             }
@@ -1701,7 +1742,7 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
     }
     // passes of the cycle through layer 0 (:606-634): more than one, and the
     // branch and bound splits the branch -- the host's part
-    if (threadIdx.x == 0) {
+    if (lead) {
         const int* nodes = J.recNodes[neg];
         int wraps = 0;
         bool left = false;
@@ -1728,33 +1769,49 @@ __device__ void pair_solve(PairJob& J, BfParams& P, const Team& t, char* smem) {
             J.status = PAIR_DONE;
         }
     }
+#undef PGC_TEAM_FAIL
 }
 
 }  // namespace
 
+// Teams of teamCtas consecutive CTAs take graphs from the queue, largest
+// first.  A team's words (teamWords + kTeamWordStride * team, zeroed by the
+// caller): barrier counter, generation, error, and the job its lead drew.
+// With more than one CTA per team the launch is cooperative, so that every
+// CTA of a team is resident.
 template <class CT, int TK>
-__global__ void __launch_bounds__(kBatchThreads, kBatchBlocksPerSm) bf_batch_kernel(PairJob* jobs, int count,
-                                                                                   int* next) {
+__global__ void __launch_bounds__(kBatchThreads, kBatchBlocksPerSm)
+    bf_batch_kernel(PairJob* jobs, int count, int* next, unsigned* teamWords, int teamCtas, unsigned spin) {
     extern __shared__ double4 smemRaw[];
     char* smem = reinterpret_cast<char*>(smemRaw);
     __shared__ BfParams P;
-    __shared__ int sJob;
+    __shared__ int sJob, sCtas;
+    const int cta = (int)(blockIdx.x % (unsigned)teamCtas);
+    unsigned* w = teamWords + (size_t)(blockIdx.x / (unsigned)teamCtas) * kTeamWordStride;
+    const Team all{cta, teamCtas, w, w + 1, reinterpret_cast<int*>(w + 2), spin};
+    const bool lead = cta == 0 && threadIdx.x == 0;
     for (;;) {
-        if (threadIdx.x == 0) sJob = atomicAdd(next, 1);
+        if (lead) w[3] = (unsigned)atomicAdd(next, 1);
+        if (!team_sync(all)) return;
+        if (threadIdx.x == 0) sJob = (int)__ldcg(w + 3);
         __syncthreads();
         const int j = sJob;
         if (j >= count) return;
-        if (threadIdx.x == 0) P = jobs[j].bf;
-        __syncthreads();
-        const Team t{0, 1, &P.ctl->barCount, &P.ctl->barGen, &P.ctl->error, P.spinLimit};
-        const long long c0 = clock64();
-        pair_solve<CT, TK>(jobs[j], P, t, smem);
         if (threadIdx.x == 0) {
+            P = jobs[j].bf;
+            sCtas = jobs[j].ctas < 1 ? 1 : jobs[j].ctas > teamCtas ? teamCtas : jobs[j].ctas;
+        }
+        __syncthreads();
+        const SolveTeam S{all, Team{cta, sCtas, &P.ctl->barCount, &P.ctl->barGen, &P.ctl->error, P.spinLimit}};
+        const long long c0 = clock64();
+        pair_solve<CT, TK>(jobs[j], P, S, smem);
+        if (lead) {
             jobs[j].candidates = P.ctl->candidates;
             jobs[j].fallbackWalks = P.ctl->fallbackWalks;
             jobs[j].cycles = clock64() - c0;
         }
-        __syncthreads();
+        // nobody draws the next job before every CTA has read this one
+        if (!team_sync(all)) return;
     }
 }
 
@@ -1784,14 +1841,52 @@ static const void* bf_fn(int costIsF32, int timeKind, bool sharedTables) {
 // lower it under each other's launches); each launch then requests its own
 // size.
 static cudaError_t allow_max_dynamic_smem(const void* fn) {
-    int dev = 0, optin = 0;
+    int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    // set once per (function, device): every later launch finds it set
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (done.count({fn, dev})) return cudaSuccess;
+    }
+    DeviceInfo info{};
+    e = device_info(dev, &info);
     if (e == cudaSuccess) {
         cudaFuncAttributes a{};
         e = cudaFuncGetAttributes(&a, fn);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     info.smemOptin - (int)a.sharedSizeBytes);
+    }
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(mu);
+        done.insert({fn, dev});
+    }
+    return e;
+}
+
+// Resident CTAs per SM of `fn` with this block and shared memory, cached.
+static cudaError_t max_blocks_per_sm(const void* fn, int threads, size_t smemBytes, int* blocksPerSm) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+    const auto key = std::make_tuple(fn, dev, threads, smemBytes);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const auto it = cache.find(key);
+        if (it != cache.end()) {
+            *blocksPerSm = it->second;
+            return cudaSuccess;
+        }
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, smemBytes);
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = *blocksPerSm;
     }
     return e;
 }
@@ -1810,7 +1905,7 @@ cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t 
     const void* fn = bf_fn(costIsF32, timeKind, false);
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, smemBytes);
+    return max_blocks_per_sm(fn, threads, smemBytes, blocksPerSm);
 }
 
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream) {
@@ -1826,12 +1921,15 @@ static const void* bf_batch_fn(int costIsF32, int timeKind) {
                          : timeKind == 1 ? (const void*)bf_batch_kernel<double, 1> : (const void*)bf_batch_kernel<double, 2>;
 }
 
-cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, int costIsF32, int timeKind, int blocks,
-                            int threads, size_t smemBytes, cudaStream_t stream) {
+cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamWords, int teamCtas, unsigned spin,
+                            int costIsF32, int timeKind, int blocks, int threads, size_t smemBytes,
+                            cudaStream_t stream) {
+    if (teamCtas < 1 || blocks < teamCtas || blocks % teamCtas != 0) return cudaErrorInvalidValue;
     const void* fn = bf_batch_fn(costIsF32, timeKind);
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
-    void* args[] = {(void*)&jobs, (void*)&count, (void*)&next};
+    void* args[] = {(void*)&jobs, (void*)&count, (void*)&next, (void*)&teamWords, (void*)&teamCtas, (void*)&spin};
+    if (teamCtas > 1) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
 }
 
@@ -1839,7 +1937,29 @@ cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t
     const void* fn = bf_batch_fn(costIsF32, timeKind);
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, fn, threads, smemBytes);
+    return max_blocks_per_sm(fn, threads, smemBytes, blocksPerSm);
+}
+
+cudaError_t device_info(int device, DeviceInfo* out) {
+    static std::mutex mu;
+    static std::map<int, DeviceInfo> cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const auto it = cache.find(device);
+        if (it != cache.end()) {
+            *out = it->second;
+            return cudaSuccess;
+        }
+    }
+    DeviceInfo d{};
+    cudaError_t e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d.smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d.clockKhz, cudaDevAttrClockRate, device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[device] = d;
+    *out = d;
+    return cudaSuccess;
 }
 
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream) {

@@ -15,6 +15,8 @@
 #include <cstdint>
 #include <map>
 #include <mutex>
+#include <set>
+#include <tuple>
 
 #include "device_common.cuh"
 
@@ -965,15 +967,33 @@ cudaError_t launch_normals_2d(const double* Vin, int nv, const int* E, double* V
 // Host wrappers -------------------------------------------------------------
 // Persistent grid of a stream pass: as many CTAs as can be resident at once
 // (one full wave; a partial second wave would double the pass).
+// The grid is cached per (kernel, device, block, shared memory): the
+// occupancy query is not free and every pass of every solve asks it.
 template <class K>
 static int stream_grid(K kernel, int threads, size_t smem) {
-    int dev = 0, sms = 0, per = 0;
-    int grid = 148;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1)
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
-    else
-        grid = sms * per;
+        return 148;
+    }
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+    const auto key = std::make_tuple((const void*)kernel, dev, threads, smem);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    int grid = 148, per = 0;
+    DeviceInfo info{};
+    if (device_info(dev, &info) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) {
+        cudaGetLastError();
+        return grid;
+    }
+    grid = info.sms * per;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = grid;
     return grid;
 }
 
@@ -1001,11 +1021,20 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
 cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
     const size_t smem = (size_t)(1 << a.bits) * sizeof(unsigned);
     if (smem > 48 * 1024) {
-        // digits wider than 13 bits need the opt-in shared memory; every
-        // caller sets the same value, so concurrent solves do not race
-        const cudaError_t e = cudaFuncSetAttribute(select_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)(sizeof(unsigned) << 14));
+        // digits wider than 13 bits need the opt-in shared memory, set once
+        // per device
+        static std::mutex mu;
+        static std::set<int> done;
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lk(mu);
+        if (!done.count(dev)) {
+            e = cudaFuncSetAttribute(select_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(sizeof(unsigned) << 14));
+            if (e != cudaSuccess) return e;
+            done.insert(dev);
+        }
     }
     select_hist_kernel<<<stream_grid(select_hist_kernel, 512, smem), 512, smem, s>>>(a);
     return cudaGetLastError();

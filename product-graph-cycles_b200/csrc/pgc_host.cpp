@@ -432,10 +432,10 @@ class Graph {
     void solve_ratio(int K);
     void solve_min_cost(int K);
     // Batched ratio solves (pgc_solve_batch): the costs generated and
-    // rescaled and a one-CTA Bellman-Ford team prepared for the device's
-    // solve in `job`; then the result taken from the finished job, or the
+    // rescaled and a Bellman-Ford team of up to `ctas` CTAs prepared for the
+    // device's solve in `job`; then the result taken from the finished job, or the
     // solve finished on the host when the device handed it back.
-    void batch_begin(int K, PairJob& job, int threads, size_t smemCap, bool regenerate);
+    void batch_begin(int K, PairJob& job, int threads, int ctas, size_t smemCap, bool regenerate);
     void batch_end(const PairJob& job);
     int batchK = 0;
     size_t batchSmem = 0;  // dynamic shared memory the prepared batch team needs
@@ -468,9 +468,11 @@ class Graph {
         size_t smemBytes;   // dynamic shared memory per CTA
     };
     Run prepare_run(int K, bool ratio);
-    // batch mode of prepare_run: one CTA of batchThreads threads, DP records
-    // in global memory, staging only within batchSmemCap bytes
+    // batch mode of prepare_run: a team of up to batchCtas CTAs of
+    // batchThreads threads, DP records in global memory, staging only within
+    // batchSmemCap bytes
     int batchThreads = 0;
+    int batchCtas = 1;
     size_t batchSmemCap = 0;
     void solve_ratio_rescaled(int K);
     void ensure_workspace(int K, int blocks);
@@ -862,9 +864,9 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     // (threads / 32) slices, up to the number that can be co-resident.  Each
     // CTA stages its next step's streams in two shared-memory buffers; when
     // they cannot fit, it reads the streams in place.
-    int sms = 0, smemOptin = 0;
-    PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    PGC_CUDA(cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    DeviceInfo info{};
+    PGC_CUDA(device_info(device, &info));
+    const int sms = info.sms, smemOptin = info.smemOptin;
     const size_t smemCap = (size_t)std::max(0, smemOptin - 1024);  // static shared memory of the kernel
     const int costBytes = r.costF32 ? 4 : 8, timeBytes = r.timeKind == 1 ? 4 : r.timeKind == 2 ? 8 : 0;
     const bool stageOn = env_int("PGC_BF_STAGE", 1) != 0;
@@ -883,15 +885,16 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
     };
     const size_t tables = bf_shared_table_bytes(T.n, r.Kp);
     if (batchThreads > 0) {
-        // one CTA of the batched launch: no shared DP tables; the two step
-        // buffers only when they fit the launch's shared-memory budget
+        // a team of the batched launch: up to batchCtas CTAs, none with
+        // fewer than one slice; no shared DP tables; the two step buffers
+        // only when they fit the launch's shared-memory budget
         r.threads = batchThreads;
-        r.blocks = 1;
+        r.blocks = std::max(1, std::min(batchCtas, T.nslices));
         r.coop = false;
         r.sharedTables = false;
-        r.flagSync = 0;
+        r.flagSync = r.blocks > 1 && env_int("PGC_BF_FLAGS", 1) ? 1 : 0;
         int maxSl = 0, rowCap = 0;
-        size_t need = stage_need(1, maxSl, rowCap);
+        size_t need = stage_need(r.blocks, maxSl, rowCap);
         r.rowCap = rowCap;
         r.stageSrcOnly = 0;
         if (!stageOn || need > batchSmemCap) {
@@ -907,7 +910,8 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
         if (need > batchSmemCap) throw Failure(PGC_ERR_ARG, "the graph's slice lists exceed the batch's shared memory");
         r.maxCtaSlices = maxSl;
         r.smemBytes = need;
-        ensure_workspace(K, 1);
+        // the team's reductions outside the Bellman-Ford calls use every CTA
+        ensure_workspace(K, std::max(r.blocks, batchCtas));
         upload_cta_slices(cut, K, r.threads / 32);
         return r;
     }
@@ -1480,7 +1484,7 @@ void Graph::solve_ratio_rescaled(int K) {
     adjLambda = fin.ratio;
 }
 
-void Graph::batch_begin(int K, PairJob& J, int threads, size_t smemCap, bool regenerate) {
+void Graph::batch_begin(int K, PairJob& J, int threads, int ctas, size_t smemCap, bool regenerate) {
     if (regenerate) generate();
     else ensure_generated();
     stats = Stats();
@@ -1489,6 +1493,7 @@ void Graph::batch_begin(int K, PairJob& J, int threads, size_t smemCap, bool reg
     rescale_column(0, scaling);
     if (ncols > 1) rescale_column(1, scaling);
     batchThreads = threads;
+    batchCtas = std::max(1, ctas);
     batchSmemCap = smemCap;
     Run r;
     try {
@@ -1513,6 +1518,7 @@ void Graph::batch_begin(int K, PairJob& J, int threads, size_t smemCap, bool reg
     J = PairJob{};
     J.bf = params(r, 0, 0, 0.0, std::numeric_limits<float>::infinity());
     J.bf.ctaSlice = wCtaSlice.p;
+    J.ctas = r.blocks;
     LookupArgs& a = J.lk;
     a.n = T.n;
     a.nY = T.nY;
@@ -1561,11 +1567,11 @@ void Graph::batch_end(const PairJob& J) {
     stats.branches = 1;
     stats.launches += 1;
     {
-        int khz = 0;
-        if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) == cudaSuccess && khz > 0)
-            stats.deviceMs = (double)J.cycles / khz;  // the CTA's time on this graph at the top SM clock
+        DeviceInfo info{};
+        if (device_info(device, &info) == cudaSuccess && info.clockKhz > 0)
+            stats.deviceMs = (double)J.cycles / info.clockKhz;  // the CTA's time on this graph at the top SM clock
     }
-    stats.ctas = 1;
+    stats.ctas = J.ctas;
     stats.threads = J.bf.maxCtaSlices >= 0 ? kBatchThreads : 0;
     switch (J.status) {
         case PAIR_DONE: {
@@ -2325,9 +2331,11 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
             for (auto& t : pool) t.join();
         };
         for (int64_t i = 0; i < count; ++i) status[i] = graphs[i] ? PGC_OK : PGC_ERR_ARG;
-        int dev = 0, sms = 0;
+        int dev = 0;
         PGC_CUDA(cudaGetDevice(&dev));
-        PGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        pgc::DeviceInfo info{};
+        PGC_CUDA(pgc::device_info(dev, &info));
+        const int sms = info.sms;
         if (ratio && pgc::env_int("PGC_BATCH_STREAMS", 0) == 0) {
             // One launch solves every graph: its CTAs take the graphs from a
             // queue, largest first, and run each whole ratio solve on the
@@ -2335,9 +2343,13 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
             // workers first; graphs whose first branch's cycle wraps are
             // finished on the host afterwards, with branch and bound.
             const int threads = pgc::kBatchThreads;
-            int smemOptin = 0;
-            PGC_CUDA(cudaDeviceGetAttribute(&smemOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            const size_t smemCap = (size_t)std::max(0, smemOptin / pgc::kBatchBlocksPerSm - 2048);
+            const size_t smemCap = (size_t)std::max(0, info.smemOptin / pgc::kBatchBlocksPerSm - 2048);
+            // CTAs per team (PGC_BATCH_TEAM, default 8): a team relaxes a
+            // graph's steps side by side, so more CTAs per graph shorten each
+            // solve; fewer overlap more graphs' latencies
+            int team = ctas_per_graph > 0 ? ctas_per_graph : pgc::env_int("PGC_BATCH_TEAM", 8);
+            team = std::max(1, std::min(team, sms * pgc::kBatchBlocksPerSm));
+            const unsigned spin = (unsigned)std::max(1, pgc::env_int("PGC_BF_SPIN_LIMIT", (int)pgc::kDefaultSpinLimit));
             std::vector<PairJob> jobs((size_t)count);
             std::vector<int> costF32((size_t)count, 0), timeKind((size_t)count, 0);
             std::vector<size_t> smemNeed((size_t)count, 0);
@@ -2350,7 +2362,7 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
                     const int K = max_depth >= 1 ? max_depth : g.maxDepth;
                     g.blockingSync = true;
                     try {
-                        g.batch_begin(K, jobs[(size_t)i], threads, smemCap, regenerate != 0);
+                        g.batch_begin(K, jobs[(size_t)i], threads, team, smemCap, regenerate != 0);
                     } catch (...) {
                         g.blockingSync = false;
                         throw;
@@ -2368,6 +2380,7 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
             // one launch per (cost type, time kind) group, largest graphs first
             pgc::DBuf<PairJob> dJobs;
             pgc::DBuf<int> dNext;
+            pgc::DBuf<unsigned> dTeamWords;
             cudaStream_t bs = nullptr;
             PGC_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
             struct StreamGuard {
@@ -2387,6 +2400,11 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
             if (!packed.empty()) {
                 dJobs.alloc(packed.size());
                 dNext.alloc(8);
+                // words of at most 32 teams per SM, allocated once: a group's
+                // launch may still run when the next group's words are zeroed
+                // behind it on the stream
+                const size_t maxTeams = (size_t)sms * 32;
+                dTeamWords.alloc(maxTeams * pgc::kTeamWordStride);
                 PGC_CUDA(cudaMemcpyAsync(dJobs.p, packed.data(), sizeof(PairJob) * packed.size(),
                                          cudaMemcpyHostToDevice, bs));
                 PGC_CUDA(cudaMemsetAsync(dNext.p, 0, 8 * sizeof(int), bs));
@@ -2399,12 +2417,17 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
                     int perSm = 0;
                     PGC_CUDA(pgc::bf_batch_max_blocks(cf, tk, threads, smem, &perSm));
                     if (perSm < 1) throw Failure(PGC_ERR_CUDA, "the batched solve kernel cannot be resident");
-                    const int blocks = (int)std::min<size_t>(k1 - k0, (size_t)sms * (size_t)perSm);
+                    // whole teams, all resident (the launch is cooperative
+                    // when a team has more than one CTA)
+                    const int g = std::min(team, sms * perSm);
+                    const int teams = (int)std::min<size_t>({k1 - k0, (size_t)(sms * perSm / g), maxTeams});
+                    const int blocks = teams * g;
+                    PGC_CUDA(cudaMemsetAsync(dTeamWords.p, 0, (size_t)teams * pgc::kTeamWordStride * sizeof(unsigned), bs));
                     g_batchProfile[5] += blocks;
                     g_batchProfile[6] = threads;
                     g_batchProfile[7] = std::max(g_batchProfile[7], (double)smem);
-                    PGC_CUDA(pgc::launch_bf_batch(dJobs.p + k0, (int)(k1 - k0), dNext.p + grp % 8, cf, tk, blocks, threads,
-                                             smem, bs));
+                    PGC_CUDA(pgc::launch_bf_batch(dJobs.p + k0, (int)(k1 - k0), dNext.p + grp % 8, dTeamWords.p, g,
+                                                  spin, cf, tk, blocks, threads, smem, bs));
                     k0 = k1;
                 }
                 PGC_CUDA(cudaMemcpyAsync(packed.data(), dJobs.p, sizeof(PairJob) * packed.size(),

@@ -432,20 +432,24 @@ def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas
                 workers: int = 0, regenerate: bool = False):
     """Solve many generators concurrently (no counterpart in the reference).
 
-    Each generator is solved as ``solve_with_cost_time_ratio`` (solver
+    Each generator gets the result ``solve_with_cost_time_ratio`` (solver
     ``"lawlercpu"``/``"lawlergpu"``) or ``solve_with_minimum_cost`` (any other
-    name) would, on its own CUDA stream with a Bellman-Ford team of at most
-    ``ctas_per_graph`` CTAs (0: SMs / min(graphs, 32)), by ``workers`` native
-    threads (0: 64); with
-    ``regenerate`` each first recomputes its edge costs.  Returns the list of
-    ``(passes_layers_just_once, final_objective, matching)`` triples.
+    name) would give it; with ``regenerate`` each first recomputes its edge
+    costs.  Returns the list of ``(passes_layers_just_once, final_objective,
+    matching)`` triples.
 
-    The device runs the graphs' streams side by side only as far as it has
-    host work queues: CUDA's default is 8, and a process started with
-    ``CUDA_DEVICE_MAX_CONNECTIONS=32`` (read when CUDA initialises) runs a
-    batch about 3x faster.  The package does not set it: that is the
-    application's choice, since it changes how all of the process's streams
-    share the device.
+    Ratio solvers: ``workers`` native threads (0: 64) generate and rescale the
+    costs, then one persistent launch runs every graph's whole ratio solve on
+    the device, teams of ``ctas_per_graph`` CTAs (0: ``PGC_BATCH_TEAM``, else
+    8) taking the graphs largest first; a graph whose first-branch cycle wraps
+    is finished on the host with branch and bound.  Other solvers run each
+    graph on its own CUDA stream with a team of at most ``ctas_per_graph``
+    CTAs (0: SMs / min(graphs, 32)); the device runs those streams side by
+    side only as far as it has host work queues: CUDA's default is 8, and a
+    process started with ``CUDA_DEVICE_MAX_CONNECTIONS=32`` (read when CUDA
+    initialises) runs such a batch about 3x faster.  The package does not set
+    it: that is the application's choice, since it changes how all of the
+    process's streams share the device.
     """
     gens = list(generators)
     if len(set(id(g) for g in gens)) != len(gens):
