@@ -249,9 +249,12 @@ def _time_pair_steps(g, stream, solver, k, steps, warmup, info, world):
     result = st = prof = None
     edges = info["layers"] * info["edges_per_block"]
     flush = torch.empty(1 << 25, dtype=torch.float64, device="cuda") if 8 * edges < L2_BYTES else None
+    import cyclic_product_graphs as cpg
+
     with ClockSampler(torch.cuda.current_device()) as clocks:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        n0 = cpg.kernel_launches()
         for i in range(steps):
             if flush is not None:
                 with torch.cuda.stream(stream):
@@ -263,9 +266,9 @@ def _time_pair_steps(g, stream, solver, k, steps, warmup, info, world):
             prof = g.last_profile()
             sweeps += st["sweeps"]
             bf_us += st["device_us"]
-            launches += st["kernel_launches"] + 1  # + the energy kernel of generate()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        launches = cpg.kernel_launches() - n0  # the library's kernels in the timed steps
     step_ms = [a.elapsed_time(b) for a, b in ev]
     return dict(total_ms=max_over_ranks(sum(step_ms), world, "cuda"), sweeps=sweeps, bf_us=bf_us,
                 launches=launches, result=result, stats=st, profile=prof, clocks=clocks.summary(), wall=wall)
@@ -526,7 +529,7 @@ def _batch_config(workload, pairs, world):
     return {"workload": workload, "pairs": len(pairs), "vx_range": BATCHES[workload][1],
             "vy_range": BATCHES[workload][2], "k": BATCHES[workload][3],
             "edges_total": int(sum(len(p["EY"]) * (2 * len(p["EX"]) + len(p["VX"])) for p in pairs)),
-            "parallelism": f"one stream + a small CTA team per pair, replicas x{world}",
+            "parallelism": f"one persistent launch, a team of CTAs per pair, replicas x{world}",
             "l2": "inputs larger than L2 (all pairs' cost streams together)"}
 
 
@@ -534,7 +537,7 @@ def _fwdbwd_config(workload, pairs, k, world):
     """The `config` of a fwd/bwd line, the same in both arms."""
     return {"workload": workload, "pairs": int(pairs), "vx": FWDBWD[workload][1], "vy": FWDBWD[workload][2],
             "k": int(k), "feature_dim": FWDBWD[workload][4],
-            "parallelism": f"one stream + a small CTA team per pair, replicas x{world}",
+            "parallelism": f"one persistent launch, a team of CTAs per pair, replicas x{world}",
             "l2": "per-pair streams of all pairs exceed L2"}
 
 
@@ -550,10 +553,10 @@ def _batch_pairs(name, seed):
 
 def run_batch(args, world, rank):
     """Batched serving: every step solves all pairs of the batch concurrently
-    (solve_batch: one stream and a small Bellman-Ford team per pair, the teams
-    the device runs side by side covering its SMs; costs regenerated on the
-    device first).  Also timed: the same pairs solved one
-    after the other with full-GPU teams (the plain per-pair GPU Lawler)."""
+    (solve_batch: costs regenerated and rescaled on the device, then one
+    persistent launch in which teams of CTAs run each pair's whole ratio
+    solve, largest pairs first).  Also timed: the same pairs solved one after
+    the other with full-GPU teams (the plain per-pair GPU Lawler)."""
     specs, pairs = _batch_pairs(args.workload, args.seed + rank)
     import numpy as np
     import torch
@@ -586,15 +589,23 @@ def run_batch(args, world, rank):
     stream = torch.cuda.current_stream()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     bytes_moved = 0
+    launches = 0
+    profiles = []
     with ClockSampler(dev) as clocks:
         for i in range(args.steps):
             torch.cuda.synchronize()
+            n0 = cpg.kernel_launches()
             ev[i][0].record(stream)
             step()
             ev[i][1].record(stream)
             torch.cuda.synchronize()
+            launches += cpg.kernel_launches() - n0
+            profiles.append(cpg.last_batch_profile())
             for g, info, sp in zip(gens, infos, specs):
                 bytes_moved += algorithmic_bytes_per_sweep(info, sp["k"], True) * g.last_stats()["sweeps"]
+    pair_device_ms = sum(g.last_stats()["device_us"] for g in gens) / 1000.0
+    # Bellman-Ford steps of the last step's solves (one per (layer, depth), and the closing layer's depth 0)
+    bf_steps = sum(g.last_stats()["sweeps"] * (info["layers"] * sp["k"] + 1) for g, info, sp in zip(gens, infos, specs))
     total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
     solves = len(gens) * args.steps
     value = replica_throughput(solves, world, total_ms)
@@ -619,7 +630,6 @@ def run_batch(args, world, rank):
     # end to end from host arrays: handles built, batch solved, matchings back
     # (the timed handles are released first: their memory returns to the
     # library's caching allocator, as in a serving process)
-    launches = sum(g.last_stats()["kernel_launches"] + 1 for g in gens)
     del gens
     import gc
 
@@ -642,16 +652,26 @@ def run_batch(args, world, rank):
                                 "sample": f"all {seq_n} pairs solved one after the other, full-GPU teams"},
         "e2e": {"value": world * len(pairs) / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": 1},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_kernel (all pairs)",
+                     "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_batch_kernel (all pairs)",
                      "note": "algorithmic bytes of every sweep of every pair / batch step time"},
+        "batch_profile": dict(_median_profile(profiles, pair_device_ms), bf_steps=bf_steps,
+                              team_us_per_step=1000.0 * pair_device_ms / max(1, bf_steps)),
         "clocks": clocks.summary(),
     }
-    line["gpu_launches"] = launches * args.steps
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = _batch_cpu_sample(specs, pairs)
     return line
+
+
+def _median_profile(profiles, pair_device_ms):
+    """The timed steps' batch phases (host wall clock, ms; medians over the
+    steps) and the last step's summed per-pair device time: the team clock
+    of each pair's whole ratio solve inside the persistent launch."""
+    out = {k: statistics.median(p[k] for p in profiles) for k in profiles[0]} if profiles else {}
+    out["pair_device_ms_sum"] = pair_device_ms
+    return out
 
 
 def _batch_cpu_sample(specs, pairs, count=2):
@@ -755,17 +775,21 @@ def run_fwdbwd(args, world, rank):
         torch.distributed.barrier()
     stream = torch.cuda.current_stream()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    profiles = []
     with ClockSampler(dev) as clocks:
         for i in range(args.steps):
             torch.cuda.synchronize()
+            n0 = cpg.kernel_launches()
             ev[i][0].record(stream)
             lam = step()
             ev[i][1].record(stream)
             torch.cuda.synchronize()
+            launches += cpg.kernel_launches() - n0  # the library's kernels; torch's cdist/sum are not counted
+            profiles.append(cpg.last_batch_profile())
+    pair_device_ms = sum(g.last_stats()["device_us"] for g in gens) / 1000.0
     total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
     value = replica_throughput(len(gens) * args.steps, world, total_ms)
-    # per pair and step: the solve's launches, the energy kernel and the adjoint kernel
-    launches = args.steps * sum(g.last_stats()["kernel_launches"] + 2 for g in gens)
     grads_ok = all(t.grad is not None and bool(torch.isfinite(t.grad).all()) for t in fX)
 
     step_plain()
@@ -808,6 +832,7 @@ def run_fwdbwd(args, world, rank):
         "gradients_finite": grads_ok,
         "mean_objective": mean_objective,
         "gpu_launches": launches,
+        "batch_profile": _median_profile(profiles, pair_device_ms),
         "clocks": clocks.summary(),
     }
 

@@ -174,6 +174,10 @@ int pgc_set_team_shape(pgc_graph* g, int ctas, int threads_per_cta);
 int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver_name, int max_depth,
                     int ctas_per_graph, int workers, int regenerate, int* status);
 
+/* No reference counterpart.  Kernel launches the library has issued in this
+ * process so far, on every device and thread (a counter that only grows). */
+int pgc_kernel_launches(int64_t* out);
+
 /* No reference counterpart.  Where the calling thread's last
  * pgc_solve_batch spent its time (host wall clock, ms) when it solved ratio
  * cycles in one launch: out8 = {costs generated and rescaled, teams

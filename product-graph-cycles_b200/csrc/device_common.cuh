@@ -300,6 +300,10 @@ struct DeviceInfo {
     int sms, smemOptin, clockKhz;
 };
 cudaError_t device_info(int device, DeviceInfo* out);
+// Kernel launches the library has issued in this process: every launch
+// helper counts its launches.
+void note_launch();
+long long launch_count();
 cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks, int threads, bool cooperative,
                       bool sharedTables, size_t smemBytes, cudaStream_t stream);
 cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);

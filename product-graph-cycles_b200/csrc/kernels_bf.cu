@@ -39,6 +39,7 @@
 // barriers.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -1897,6 +1898,7 @@ cudaError_t launch_bf(const BfParams& p, int costIsF32, int timeKind, int blocks
     const void* fn = bf_fn(costIsF32, timeKind, sharedTables);
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
+    note_launch();
     if (cooperative) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
 }
@@ -1909,6 +1911,7 @@ cudaError_t bf_max_coop_blocks(int costIsF32, int timeKind, int threads, size_t 
 }
 
 cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream) {
+    note_launch();
     extract_path_kernel<<<1, 32, 0, stream>>>(p, v);
     return cudaGetLastError();
 }
@@ -1929,6 +1932,7 @@ cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamW
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&jobs, (void*)&count, (void*)&next, (void*)&teamWords, (void*)&teamCtas, (void*)&spin};
+    note_launch();
     if (teamCtas > 1) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
 }
@@ -1939,6 +1943,10 @@ cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t
     if (e != cudaSuccess) return e;
     return max_blocks_per_sm(fn, threads, smemBytes, blocksPerSm);
 }
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 cudaError_t device_info(int device, DeviceInfo* out) {
     static std::mutex mu;
@@ -1964,6 +1972,7 @@ cudaError_t device_info(int device, DeviceInfo* out) {
 
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream) {
     if (a.count <= 0) return cudaSuccess;
+    note_launch();
     lookup_pairs_kernel<<<(a.count + 127) / 128, 128, 0, stream>>>(a);
     return cudaGetLastError();
 }

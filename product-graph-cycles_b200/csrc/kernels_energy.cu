@@ -951,15 +951,20 @@ cudaError_t launch_normals_3d(const double* V, long long nv, const int* F, long 
     const int threads = 256;
     const int fb = (int)std::min<long long>(std::max<long long>(1, (nf + threads - 1) / threads), 4096);
     const int vb = (int)std::min<long long>(std::max<long long>(1, (nv + threads - 1) / threads), 4096);
+    note_launch();
     face_normals_kernel<<<fb, threads, 0, s>>>(V, nv, F, nf, fn, deg, bad);
+    note_launch();
     exclusive_scan_kernel<<<1, 1024, 0, s>>>(deg, nv, off);
+    note_launch();
     face_lists_kernel<<<fb, threads, 0, s>>>(F, nv, nf, off, cursor, list);
+    note_launch();
     vertex_normals_kernel<<<vb, threads, 0, s>>>(fn, nv, off, list, out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_normals_2d(const double* Vin, int nv, const int* E, double* V, double* en, double* el, double* out,
                               int* bad, cudaStream_t s) {
+    note_launch();
     curve_normals_kernel<<<1, 256, 0, s>>>(Vin, nv, E, V, en, el, out, bad);
     return cudaGetLastError();
 }
@@ -1006,15 +1011,18 @@ static int grid_for(long long total, int threads) {
 
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s) {
     const size_t smem = a.hist0 ? 2 * kTopBins * sizeof(unsigned) : 0;
+    note_launch();
     plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, smem), 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
     const size_t smem = a.hist0 ? 2 * kTopBins * sizeof(unsigned) : 0;
+    note_launch();
     ho_energy_kernel<<<stream_grid(ho_energy_kernel, 256, smem), 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
+    note_launch();
     quaternion_kernel<<<grid_for((long long)a.nY * a.nEX, 128), 128, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -1036,33 +1044,39 @@ cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
             done.insert(dev);
         }
     }
+    note_launch();
     select_hist_kernel<<<stream_grid(select_hist_kernel, 512, smem), 512, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,
                                   cudaStream_t s) {
+    note_launch();
     select_compact_kernel<<<stream_grid(select_compact_kernel, 256, 0), 256, 0, s>>>(a, out, count, cap);
     return cudaGetLastError();
 }
 cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long above, unsigned long long* out,
                                     cudaStream_t s) {
+    note_launch();
     select_min_above_kernel<<<stream_grid(select_min_above_kernel, 256, 0), 256, 0, s>>>(a, above, out);
     return cudaGetLastError();
 }
 cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
                            int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
                            int writeF64, cudaStream_t s) {
+    note_launch();
     rescale_kernel<<<stream_grid(rescale_kernel, 256, 0), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
                                                         factor, clip, exact, writeF64);
     return cudaGetLastError();
 }
 cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
                           const int* ti, const int* tr, cudaStream_t s) {
+    note_launch();
     to_f64_kernel<<<stream_grid(to_f64_kernel, 256, 0), 256, 0, s>>>(col32, col, layerStride, interEntries, nY, ti, tr);
     return cudaGetLastError();
 }
 cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,
                           long long interEntries, int nY, const int* ti, const int* tr, int* exact, cudaStream_t s) {
+    note_launch();
     to_f32_kernel<<<stream_grid(to_f32_kernel, 256, 0), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
                                                        exact);
     return cudaGetLastError();
@@ -1070,6 +1084,7 @@ cudaError_t launch_to_f32(const double* col, float* col32, long long total, long
 cudaError_t launch_export(const double* col, double* out, int cols, int c, long long total, long long layerStride,
                           long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
                           cudaStream_t s) {
+    note_launch();
     export_kernel<<<grid_for(total, 256), 256, 0, s>>>(col, out, cols, c, total, layerStride, interEntries, nY,
                                                        eBlock, ti, tr);
     return cudaGetLastError();
@@ -1108,12 +1123,14 @@ cudaError_t noalloc_export_scratch(int device, double** ptr) {
 cudaError_t launch_plain_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
                                         double coef, double* grad, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
+    note_launch();
     plain_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, grad);
     return cudaGetLastError();
 }
 cudaError_t launch_conj_energy_backward(const EnergyArgs& a, const long long* edges, int count, long long eBlock,
                                        double coef, double coefT, long long argmax, double* grad, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
+    note_launch();
     conj_energy_backward_kernel<<<(count + 127) / 128, 128, 0, s>>>(a, edges, count, eBlock, coef, coefT, argmax,
                                                                       grad);
     return cudaGetLastError();
@@ -1121,6 +1138,7 @@ cudaError_t launch_conj_energy_backward(const EnergyArgs& a, const long long* ed
 cudaError_t launch_import(const double* in, double* col, int cols, int c, long long total, long long layerStride,
                           long long interEntries, int nY, long long eBlock, const int* ti, const int* tr,
                           cudaStream_t s) {
+    note_launch();
     import_kernel<<<grid_for(total, 256), 256, 0, s>>>(in, col, cols, c, total, layerStride, interEntries, nY, eBlock,
                                                        ti, tr);
     return cudaGetLastError();
@@ -1128,6 +1146,7 @@ cudaError_t launch_import(const double* in, double* col, int cols, int c, long l
 cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s) {
+    note_launch();
     layer1_mean_kernel<double><<<(n + 255) / 256, 256, 0, s>>>(cost, layerStride, interEntries, n, nslices, spI, spA,
                                                                srcI, srcA, meanOut, countOut);
     return cudaGetLastError();
@@ -1135,6 +1154,7 @@ cudaError_t launch_layer1_mean(const double* cost, long long layerStride, long l
 cudaError_t launch_layer1_mean(const float* cost, long long layerStride, long long interEntries, int n, int nslices,
                                const int* spI, const int* spA, const int* srcI, const int* srcA, float* meanOut,
                                int* countOut, cudaStream_t s) {
+    note_launch();
     layer1_mean_kernel<float><<<(n + 255) / 256, 256, 0, s>>>(cost, layerStride, interEntries, n, nslices, spI, spA,
                                                               srcI, srcA, meanOut, countOut);
     return cudaGetLastError();

@@ -2294,6 +2294,13 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }
 }  // namespace
 
+int pgc_kernel_launches(int64_t* out) {
+    return guarded([&] {
+        if (!out) throw Failure(PGC_ERR_ARG, "null output");
+        *out = pgc::launch_count();
+    });
+}
+
 int pgc_batch_profile(double* out8) {
     return guarded([&] {
         if (!out8) throw Failure(PGC_ERR_ARG, "null output");

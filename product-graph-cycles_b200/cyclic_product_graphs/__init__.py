@@ -79,6 +79,7 @@ def _declare(L):
                                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.pgc_device_name.argtypes = [_h, ctypes.c_char_p, _i64]
     L.pgc_batch_profile.argtypes = [_dp]
+    L.pgc_kernel_launches.argtypes = [_lp]
     L.pgc_last_error.restype = ctypes.c_char_p
     L.pgc_version.restype = ctypes.c_char_p
 
@@ -471,6 +472,15 @@ def last_batch_profile() -> dict:
     keys = ["prepare_ms", "launch_ms", "finish_ms", "handed_back", "solved_on_device", "ctas", "threads_per_cta",
             "smem_bytes"]
     return dict(zip(keys, list(buf)))
+
+
+def kernel_launches() -> int:
+    """Kernel launches the library has issued in this process so far (no
+    counterpart in the reference): the difference across a region is the
+    number of the library's kernels that ran in it."""
+    out = ctypes.c_int64()
+    _check(_lib.pgc_kernel_launches(ctypes.byref(out)))
+    return int(out.value)
 
 
 def vertex_correspondences(matching, conjugate: bool | None = None) -> np.ndarray:

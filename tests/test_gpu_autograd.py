@@ -275,7 +275,10 @@ def _ratio_fd_check(cpg, g, make, fd0, K, h, directions, seed, tol):
 
     def same_cycle(fd):
         probe.set_feat_diff(fd)
-        probe.solve_with_cost_time_ratio("lawlergpu", K)
+        try:
+            probe.solve_with_cost_time_ratio("lawlergpu", K)
+        except cpg.PGCError:  # the reference's "no nodes in branch" end: no cycle to compare
+            return False
         return np.array_equal(np.sort(probe.last_cycle_edges()), edges_sorted)
 
     rng = np.random.default_rng(seed)
@@ -306,15 +309,23 @@ def test_ratio_adjoint_matches_central_differences(cpg, oracle, nv, m, K, seed):
     assert _ratio_fd_check(cpg, make(), make, p["feat_diff"].copy(), K, 1e-3, 6, seed, 1e-3) >= 3
 
 
-@pytest.mark.parametrize("cost", ["robustso3", "plainso3"])
-def test_conjugate_feature_time_adjoint_matches_central_differences(cpg, oracle, cost):
-    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=13)
+@pytest.mark.parametrize("cost,seed", [("robustso3", 24), ("plainso3", 14)])
+def test_conjugate_feature_time_adjoint_matches_central_differences(cpg, oracle, cost, seed):
+    """The ("*", "feature") time column divides by maxFd, the matrix maximum:
+    the adjoint's subgradient puts that term on the maximum's entry.  The
+    maximum is raised by 0.5 so that +-h moves keep it on the same entry; the
+    pairs are ones where the oracle keeps the solved cycle along at least
+    three of the ten directions (elsewhere the branch and bound changes the
+    cycle or ends with "no nodes in branch")."""
+    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=seed)
+    fd0 = p["feat_diff"].copy()
+    fd0.flat[np.argmax(fd0)] += 0.5
 
     def make():
-        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], True, True, False)
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], fd0, True, True, False)
         g.set_normals(p["NX"], p["NY"])
         g.set_cost_time_ratio_mode(cost, "feature")
         return g
 
-    # h = 1e-2: maxFd passes through float, whose spacing near the maximum is ~1e-6
-    assert _ratio_fd_check(cpg, make(), make, p["feat_diff"].copy(), 2, 1e-2, 8, 4, 2e-3) >= 3
+    # h = 2e-3: maxFd (about 1.5) passes through float, whose spacing there is ~1.2e-7
+    assert _ratio_fd_check(cpg, make(), make, fd0.copy(), 2, 2e-3, 10, 4, 2e-3) >= 3
