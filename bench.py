@@ -310,7 +310,7 @@ def _traffic(workload):
     try:
         with open(tpath) as f:
             d = json.load(f)
-        return d.get("dram_bytes_per_launch"), d.get("kind", "measured") + ": " + d.get("source", "")
+        return d.get("dram_bytes_per_launch"), {"kind": d.get("kind", "unstated"), "source": d.get("source", "")}
     except Exception:
         return None, None
 
@@ -347,7 +347,9 @@ def measure_pair(args, world, rank, workload, steps, warmup, e2e_steps, with_min
              "algorithmic_bytes_per_sweep": b_sweep, "sweeps_per_solve": t["sweeps"] / steps_done,
              "bf_ms_per_solve": t["bf_us"] / 1000.0 / steps_done}
         if ratio_mode:
-            r["traffic"], r["traffic_source"] = _traffic(workload)
+            r["traffic"], src = _traffic(workload)
+            if src:
+                r["traffic_kind"], r["traffic_source"] = src["kind"], src["source"]
         return r
 
     t = _time_pair_steps(g, stream, "ratio", k, steps, warmup, info, world)
@@ -604,8 +606,11 @@ def run_batch(args, world, rank):
             for g, info, sp in zip(gens, infos, specs):
                 bytes_moved += algorithmic_bytes_per_sweep(info, sp["k"], True) * g.last_stats()["sweeps"]
     pair_device_ms = sum(g.last_stats()["device_us"] for g in gens) / 1000.0
-    # Bellman-Ford steps of the last step's solves (one per (layer, depth), and the closing layer's depth 0)
-    bf_steps = sum(g.last_stats()["sweeps"] * (info["layers"] * sp["k"] + 1) for g, info, sp in zip(gens, infos, specs))
+    # Bellman-Ford steps of the last step's solves, and where the lead thread's cycles went
+    profs = [g.last_profile() for g in gens]
+    bf_steps = sum(pr["steps"] for pr in profs)
+    cycle_split = {k: sum(pr[k] for pr in profs) for k in ("cycles_relax", "cycles_handoff", "cycles_bookkeeping",
+                                                           "cycles_sweep_tail", "cycles_stage_wait")}
     total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
     solves = len(gens) * args.steps
     value = replica_throughput(solves, world, total_ms)
@@ -657,7 +662,8 @@ def run_batch(args, world, rank):
                      "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "bf_batch_kernel (all pairs)",
                      "note": "algorithmic bytes of every sweep of every pair / batch step time"},
         "batch_profile": dict(_median_profile(profiles, pair_device_ms), bf_steps=bf_steps,
-                              team_us_per_step=1000.0 * pair_device_ms / max(1, bf_steps)),
+                              team_us_per_step=1000.0 * pair_device_ms / max(1, bf_steps),
+                              lead_cycles_per_step={k: v / max(1, bf_steps) for k, v in cycle_split.items()}),
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -956,9 +962,10 @@ def main():
             print(json.dumps(line), flush=True)
         return
 
-    # 32 host work queues let batched solves (one stream per pair) run side
-    # by side; CUDA's default of 8 serialises them.  Read when CUDA starts,
-    # so it is set before anything touches the device.
+    # 32 host work queues let the stream route of batched solves (one stream
+    # per pair: minimum-cost batches, the plain per-pair comparison's teams)
+    # run side by side; CUDA's default of 8 serialises them.  Read when CUDA
+    # starts, so it is set before anything touches the device.
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if world > 1:
         import datetime

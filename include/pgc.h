@@ -129,8 +129,10 @@ int pgc_solve_with_minimum_cost(pgc_graph* g, const char* solver_name, int max_d
  * straight through; the energy's adjoint scatters every cycle edge into the
  * feat_diff entries its cost reads (plain graph: two; conjugate graph:
  * fd[x2, y2] in the ("vanilla", *) and ("feature", *) modes, none in the
- * others).  PGC_ERR_STATE without a result; PGC_ERR_MODE for a ratio on a
- * conjugate graph whose time column reads feat_diff ("*", "feature"). */
+ * others; a ratio whose time column reads feat_diff, ("*", "feature") with
+ * t = max(0, maxFd - fd), adds its time part and puts the subgradient of
+ * maxFd on the matrix maximum's first entry).  PGC_ERR_STATE without a
+ * result. */
 int pgc_backward_feat_diff(pgc_graph* g, double grad_objective, double* grad_feat_diff, int accumulate);
 
 /* No reference counterpart (the oracle's setCostVector).  Sets the edge costs
@@ -141,6 +143,13 @@ int pgc_set_cost_vector(pgc_graph* g, const double* costs, int64_t rows, int64_t
 /* No reference counterpart.  Replaces feat_diff [|VX| x |VY|]; the next solve
  * regenerates the costs.  Lets one handle serve many training steps. */
 int pgc_set_feat_diff(pgc_graph* g, const double* feat_diff, int64_t rows, int64_t cols);
+
+/* No reference counterpart.  pgc_set_feat_diff from DEVICE memory (row-major
+ * float64 on the handle's GPU): one device-to-device copy on the handle's
+ * stream, complete when the call returns, so the buffer may be freed then.
+ * The caller orders the buffer's producer before the call (synchronize the
+ * producing stream, or give the handle that stream with pgc_set_stream). */
+int pgc_set_feat_diff_device(pgc_graph* g, const double* feat_diff, int64_t rows, int64_t cols);
 
 /* No reference counterpart.  Most CTAs one Bellman-Ford launch of this graph
  * may use (0, the default: as many as shorten a step).  A small team is

@@ -427,6 +427,12 @@ class Graph {
     void backward_feat_diff(double grad, double* gradFd, bool accumulate);
     void set_cost_vector(const double* in, int64_t rows, int64_t cols);
     void set_feat_diff(const double* fd, int64_t rows, int64_t cols);
+    void set_feat_diff_device(const double* fd, int64_t rows, int64_t cols);
+    // After set_feat_diff_device the matrix lives only in dFD; the host copy
+    // is read back when a host reader needs it (the feature-time maximum, the
+    // CSV export).
+    bool fdHostStale = false;
+    void ensure_fd_host();
 
     // -------------------------------------------------------------------
     void solve_ratio(int K);
@@ -529,7 +535,7 @@ void Graph::upload_template() {
     dEX.upload(EX.data(), EX.size(), s);
     dVX.upload(VX.data(), VX.size(), s);
     dVY.upload(VY.data(), VY.size(), s);
-    dFD.upload(FD.data(), FD.size(), s);
+    if (!fdHostStale) dFD.upload(FD.data(), FD.size(), s);  // else dFD already holds it
     templateReady = true;
 }
 
@@ -606,6 +612,7 @@ void Graph::generate() {
         a.rlPwr = rlPwr;
         a.maxSO3 = (double)(float)robust_loss_host(2 * M_PI, rlAlpha, rlC, rlPwr);
         if (tm == FEATURE) {
+            ensure_fd_host();
             double m = -std::numeric_limits<double>::infinity();
             long long at = 0;
             for (size_t i = 0; i < FD.size(); ++i)
@@ -1566,6 +1573,16 @@ void Graph::batch_end(const PairJob& J) {
     stats.fallbackWalks = J.fallbackWalks;
     stats.branches = 1;
     stats.launches += 1;
+    // the lead thread's cycle counters, summed over the solve's calls
+    stats.cycA = c.cycPhaseA;
+    stats.cycB = c.cycPhaseB;
+    stats.cycSync = c.cycSync;
+    stats.cycTail = c.cycTail;
+    stats.cycWrap = c.cycWrap;
+    stats.cycCand = c.cycCand;
+    stats.cycLead = c.cycLead;
+    stats.cycStage = c.cycStage;
+    stats.steps = J.sweeps * ((long long)(T.nY + 1) * (T.entries[INTRA] == 0 ? 1 : batchK) - 1);
     {
         DeviceInfo info{};
         if (device_info(device, &info) == cudaSuccess && info.clockKhz > 0)
@@ -1969,9 +1986,31 @@ void Graph::set_cost_vector(const double* in, int64_t rows, int64_t cols) {
 void Graph::set_feat_diff(const double* fd, int64_t rows, int64_t cols) {
     if (rows != nvx || cols != nvy) throw Failure(PGC_ERR_ARG, "feat_diff must be |VX| x |VY|");
     copy_in(FD, fd, (size_t)(rows * cols));
+    fdHostStale = false;
     if (templateReady) dFD.upload(FD.data(), FD.size(), stream);
     generated = false;
     adjKind = 0;
+}
+
+// feat_diff from device memory: one device-to-device copy on the handle's
+// stream, finished before returning (the caller may free its buffer then).
+void Graph::set_feat_diff_device(const double* fd, int64_t rows, int64_t cols) {
+    if (rows != nvx || cols != nvy) throw Failure(PGC_ERR_ARG, "feat_diff must be |VX| x |VY|");
+    const size_t n = (size_t)(rows * cols);
+    dFD.alloc(n);
+    PGC_CUDA(cudaMemcpyAsync(dFD.p, fd, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    PGC_CUDA(sync_stream());
+    FD.resize(n);
+    fdHostStale = true;
+    generated = false;
+    adjKind = 0;
+}
+
+void Graph::ensure_fd_host() {
+    if (!fdHostStale) return;
+    d2h(FD.data(), dFD.p, FD.size() * sizeof(double));
+    PGC_CUDA(sync_stream());
+    fdHostStale = false;
 }
 
 void Graph::product_space(int32_t* out) {
@@ -2012,6 +2051,7 @@ void Graph::export_csv() {
     writeD(VY, nvy, 3, "VY");
     writeI(EX, nex, 2, "EX");
     writeI(EY, ney, 2, "EY");
+    ensure_fd_host();
     writeD(FD, nvx, nvy, "FeatDiffMatrix");
     if (conj) {
         writeD(NX, nvx, 3, "NX");
@@ -2264,6 +2304,14 @@ int pgc_set_feat_diff(pgc_graph* h, const double* feat_diff, int64_t rows, int64
         if (!h || !feat_diff) throw Failure(PGC_ERR_ARG, "null argument");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.set_feat_diff(feat_diff, rows, cols);
+    });
+}
+
+int pgc_set_feat_diff_device(pgc_graph* h, const double* feat_diff, int64_t rows, int64_t cols) {
+    return guarded([&] {
+        if (!h || !feat_diff) throw Failure(PGC_ERR_ARG, "null argument");
+        PGC_CUDA(cudaSetDevice(h->g.device));
+        h->g.set_feat_diff_device(feat_diff, rows, cols);
     });
 }
 

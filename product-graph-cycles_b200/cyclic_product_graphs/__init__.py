@@ -75,6 +75,7 @@ def _declare(L):
     L.pgc_backward_feat_diff.argtypes = [_h, ctypes.c_double, ctypes.c_void_p, ctypes.c_int]
     L.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
     L.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
+    L.pgc_set_feat_diff_device.argtypes = [_h, ctypes.c_void_p, _i64, _i64]
     L.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.pgc_device_name.argtypes = [_h, ctypes.c_char_p, _i64]
@@ -266,6 +267,12 @@ class product_graph_generator:
         if FD.ndim != 2:
             raise ValueError("feat_diff must be a 2-d matrix")
         _check(_lib.pgc_set_feat_diff(self._h, FD.ctypes.data_as(_dp), FD.shape[0], FD.shape[1]))
+
+    def set_feat_diff_device(self, ptr: int, rows: int, cols: int):
+        """Replace feat_diff from device memory: ``ptr`` addresses rows x cols
+        row-major float64 on this handle's GPU, already written (synchronise
+        its producer first).  Copied before the call returns."""
+        _check(_lib.pgc_set_feat_diff_device(self._h, ctypes.c_void_p(int(ptr)), int(rows), int(cols)))
 
     def backward_feat_diff(self, grad_objective: float, grad_feat_diff_ptr: int, accumulate: bool = False):
         """grad_objective * d(last objective)/d(feat_diff) into a device buffer (|VX| x |VY| float64)."""

@@ -10,8 +10,11 @@ library's hand-written adjoint kernel (``pgc_backward_feat_diff``):
 
 and the energy's adjoint scatters every cycle edge into the feat_diff
 entries its cost reads (plain graph: two; conjugate graph: one, in the
-("vanilla", *) and ("feature", *) modes).  torch carries the gradient on from feat_diff
-(e.g. to learnable features).  ``BlackboxMinCostCycle`` implements blackbox
+("vanilla", *) and ("feature", *) modes; a ratio whose time column reads
+feat_diff, ("*", "feature"), adds its time part with the subgradient of the
+matrix maximum on that maximum's entry).  torch carries the gradient on from
+feat_diff (e.g. to learnable features).  CUDA feat_diff tensors reach the
+library by a device-to-device copy.  ``BlackboxMinCostCycle`` implements blackbox
 interpolation (Vlastelica et al., ICLR 2020) over the edge costs: its
 backward solves again at w + tau * dL/dy and returns -(y(w) - y(w')) / tau.
 """
@@ -25,6 +28,19 @@ from . import solve_batch
 
 def _as_host(fd: torch.Tensor) -> np.ndarray:
     return fd.detach().to(device="cpu", dtype=torch.float64).contiguous().numpy()
+
+
+def _set_feat_diff(gen, fd: torch.Tensor, synced: bool = False):
+    """feat_diff into the handle: a device-to-device copy when it is a CUDA
+    tensor (its producer synchronised first, unless the caller did), else
+    through host memory."""
+    if fd.is_cuda:
+        src = fd.detach().to(dtype=torch.float64).contiguous()
+        if not synced:
+            torch.cuda.current_stream(src.device).synchronize()
+        gen.set_feat_diff_device(src.data_ptr(), src.shape[0], src.shape[1])
+    else:
+        gen.set_feat_diff(_as_host(fd))
 
 
 def _adjoint(gen, grad_out: torch.Tensor, like: torch.Tensor, synced: bool = False) -> torch.Tensor:
@@ -42,12 +58,11 @@ def _adjoint(gen, grad_out: torch.Tensor, like: torch.Tensor, synced: bool = Fal
 
 class RatioCycleObjective(torch.autograd.Function):
     """lambda*(feat_diff) of ``gen`` (a product_graph_generator whose geometry
-    and modes are set: plain, or conjugate with a time mode other than
-    "feature") by ``solve_with_cost_time_ratio``."""
+    and modes are set) by ``solve_with_cost_time_ratio``."""
 
     @staticmethod
     def forward(ctx, feat_diff, gen, max_depth=None):
-        gen.set_feat_diff(_as_host(feat_diff))
+        _set_feat_diff(gen, feat_diff)
         _, objective, _ = gen.solve_with_cost_time_ratio("lawlergpu", max_depth)
         ctx.gen = gen
         ctx.save_for_backward(feat_diff)
@@ -64,7 +79,7 @@ class MinCostCycleObjective(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, feat_diff, gen, max_depth=None):
-        gen.set_feat_diff(_as_host(feat_diff))
+        _set_feat_diff(gen, feat_diff)
         _, objective, _ = gen.solve_with_minimum_cost("dijkstragpu", max_depth)
         ctx.gen = gen
         ctx.save_for_backward(feat_diff)
@@ -79,8 +94,10 @@ class MinCostCycleObjective(torch.autograd.Function):
 class _BatchedRatio(torch.autograd.Function):
     @staticmethod
     def forward(ctx, gens, max_depth, *feat_diffs):
+        if any(fd.is_cuda for fd in feat_diffs):
+            torch.cuda.synchronize()  # every producer, once
         for g, fd in zip(gens, feat_diffs):
-            g.set_feat_diff(_as_host(fd))
+            _set_feat_diff(g, fd, synced=True)
         results = solve_batch(gens, "lawlergpu", max_depth)
         ctx.gens = gens
         ctx.save_for_backward(*feat_diffs)

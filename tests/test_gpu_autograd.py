@@ -329,3 +329,31 @@ def test_conjugate_feature_time_adjoint_matches_central_differences(cpg, oracle,
 
     # h = 2e-3: maxFd (about 1.5) passes through float, whose spacing there is ~1.2e-7
     assert _ratio_fd_check(cpg, make(), make, fd0.copy(), 2, 2e-3, 10, 4, 2e-3) >= 3
+
+
+@pytest.mark.parametrize("conj", [False, True])
+def test_device_feat_diff_equals_host_feat_diff(cpg, oracle, conj):
+    """set_feat_diff_device (a device-to-device copy, the host copy read back
+    only when a host reader needs it) gives the costs, solve and adjoint that
+    set_feat_diff gives; the conjugate case's time column reads feat_diff
+    through its maximum, computed from that host copy."""
+    p = synthetic.make_pair(icosphere_level=1, n_curve=8, feat_dim=8, seed=14)
+    fd = p["feat_diff"] * 1.25 + 0.01
+    gens = []
+    for _ in range(2):
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], conj, conj, False)
+        if conj:
+            g.set_normals(p["NX"], p["NY"])
+            g.set_cost_time_ratio_mode("plainso3", "feature")
+        gens.append(g)
+    host, dev = gens
+    host.set_feat_diff(fd)
+    t = torch.tensor(fd, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    dev.set_feat_diff_device(t.data_ptr(), *fd.shape)
+    del t
+    assert np.array_equal(host.get_cost_vector(), dev.get_cost_vector())
+    rh = host.solve_with_cost_time_ratio("lawlergpu", 2)
+    rd = dev.solve_with_cost_time_ratio("lawlergpu", 2)
+    assert rh[0] == rd[0] and rh[1] == rd[1] and np.array_equal(rh[2], rd[2])
+    np.testing.assert_array_equal(_device_grad(host, fd.shape), _device_grad(dev, fd.shape))
