@@ -117,6 +117,12 @@ struct BfParams {
     unsigned spinLimit;            // polls of any wait before it gives up and raises the error word
     int stallCta;                  // test hook (-1: none): this CTA's hand-off also waits on ctl->neverSet
     int literalAll;                // test hook: decide every candidate by the literal walk
+    // cluster-resident values of a batched team: each CTA keeps [2][dsCap][Kp]
+    // doubles of the nodes it owns at byte dsOffset of its dynamic shared
+    // memory, followed by the owner CTA of every slice (nslices bytes)
+    int ds;
+    int dsCap;
+    int dsOffset;
     Control* ctl;
     int* cycleBuf;                 // original node ids, walk order (reversed on the host)
     long long cycleCap;
@@ -183,10 +189,26 @@ struct SelectArgs {
     int nY;
     const int* tedgeInter;
     const int* tedgeIntra;
-    unsigned long long prefix, prefixMask;
-    int shift, bits;
-    unsigned long long* hist;  // 1 << bits counters
+    unsigned long long* hist;  // 1 << kMedianWideBits counters
 };
+
+// State of one column's median selection on the device: the key bits fixed
+// so far (prefix under mask), the wanted rank inside the bucket they select
+// and its size, the width of the next digit; then the order statistics, the
+// median, the rescale factor and whether the float copy is inexact.
+struct MedianState {
+    unsigned long long prefix, mask;
+    long long rank, bucket;
+    int shift, bits, done, even;
+    int err;                     // 1-3: the selection lost its rank
+    int needAbove;               // even count, rank the bucket's largest: xk1 is the smallest key above it
+    unsigned long long bucketTop, minAbove;
+    double xk, xk1, median, factor;
+    int inexact;                 // the rescaled column has a value that is not a float
+    int pad;
+};
+constexpr int kMedianWideBits = 14;          // the second digit's width
+constexpr long long kMedianCompact = 1 << 16;  // a bucket this small is selected in one block
 
 struct LookupArgs {
     int n, nY;
@@ -243,6 +265,7 @@ struct PairJob {
     double* recT[2];
     int cap;
     int ctas;              // CTAs of the Bellman-Ford team bf was prepared for
+    int threads;           // threads of each of those CTAs
     // outputs
     int status;            // PairStatus
     int bfStatus;          // the failing call's status for PAIR_ERR_BF
@@ -316,18 +339,19 @@ cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamW
                             int costIsF32, int timeKind, int blocks, int threads, size_t smemBytes,
                             cudaStream_t stream);
 cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
+// Clusters of clusterCtas CTAs of the batched kernel that fit the device at once.
+cudaError_t bf_batch_max_clusters(int costIsF32, int timeKind, int threads, size_t smemBytes, int clusterCtas,
+                                  int* clusters);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s);
-cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s);
-cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,
-                                  cudaStream_t s);
-cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long above, unsigned long long* out,
-                                    cudaStream_t s);
-cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
-                           int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
-                           int writeF64, cudaStream_t s);
+// Median of a column and its rescale (cost_time_ratio_solver.cpp:709-721),
+// enqueued whole on stream s (kernels_energy.cu).
+cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHist, MedianState* st,
+                                  unsigned long long* hist, double* band, unsigned long long* count, long long nValues,
+                                  double scaling, float* col32, double clip, cudaStream_t s);
+cudaError_t launch_rescale_f64(const SelectArgs& a, MedianState* st, double clip, cudaStream_t s);
 cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
                           const int* ti, const int* tr, cudaStream_t s);
 cudaError_t launch_to_f32(const double* col, float* col32, long long total, long long layerStride,

@@ -554,18 +554,48 @@ __global__ void ho_energy_kernel(EnergyArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Median by radix selection over the valid entries of one column.  Keys are
+// Median by radix selection over the valid entries of one column, decided on
+// the device: the selection's state (MedianState) lives in device memory, so
+// the host enqueues the whole chain -- digit passes, compaction of the last
+// bucket, the in-bucket selection, the rescale -- and waits once.  Keys are
 // the order-preserving 64-bit images of the doubles; digits from the most
-// significant one (the host picks their width and stops when the bucket is
-// small enough to finish on the host).
+// significant one: 12 bits (counted by the energy kernel while it wrote the
+// column), 14, then 12 at a time, until the bucket holding the wanted rank
+// has at most kMedianCompact members (or every bit is fixed).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double key_to_double(unsigned long long key) {
+    const unsigned long long u = (key >> 63) ? (key & 0x7fffffffffffffffULL) : ~key;
+    return __longlong_as_double((long long)u);
+}
 
-// Histogram of the next digit of the keys that match the current prefix.
+// Width of the digit counted after `shift` bits remain below the prefix.
+__device__ __forceinline__ int median_digit_bits(int shift) {
+    const int b = shift == 64 ? kTopDigitBits : shift == 64 - kTopDigitBits ? kMedianWideBits : kTopDigitBits;
+    return b < shift ? b : shift;
+}
+
+__global__ void median_init_kernel(MedianState* st, long long count) {
+    MedianState m{};
+    m.even = count % 2 == 0;
+    m.rank = m.even ? (count - 2) / 2 : count / 2;
+    m.bucket = count;
+    m.shift = 64;
+    m.bits = median_digit_bits(64);
+    m.minAbove = ~0ull;
+    *st = m;
+}
+
+// Histogram of the next digit of the keys that match the state's prefix.
 // A grid of one wave (occupancy-sized) keeps the final flush of the block
-// histograms short.
-__global__ void select_hist_kernel(SelectArgs a) {
+// histograms short.  Nothing to do once the selection is done.
+__global__ void median_hist_kernel(SelectArgs a, const MedianState* st) {
     extern __shared__ unsigned int sh[];
-    const int nb = 1 << a.bits;
+    __shared__ MedianState m;
+    if (threadIdx.x == 0) m = *st;
+    __syncthreads();
+    if (m.done || m.bits < 1 || m.bits > kMedianWideBits || m.bits > m.shift) return;
+    const int nb = 1 << m.bits;
+    const int shift = m.shift - m.bits;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     // Each thread counts a run of equal digits in a register and adds the run
@@ -573,12 +603,13 @@ __global__ void select_hist_kernel(SelectArgs a) {
     // digits of one column fall into a few bins, where per-entry atomics (or
     // warp matching) would serialise.
     unsigned runBin = 0xffffffffu, runCnt = 0;
+    const unsigned long long prefix = m.prefix, mask = m.mask;
     for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
                          [&](long long, double x, bool valid, bool) {
                              if (!valid) return;
                              const unsigned long long k = order_key(x);
-                             if ((k & a.prefixMask) != a.prefix) return;
-                             const unsigned bin = (unsigned)((k >> a.shift) & (unsigned long long)(nb - 1));
+                             if ((k & mask) != prefix) return;
+                             const unsigned bin = (unsigned)((k >> shift) & (unsigned long long)(nb - 1));
                              if (bin == runBin) {
                                  ++runCnt;
                              } else {
@@ -593,18 +624,204 @@ __global__ void select_hist_kernel(SelectArgs a) {
         if (sh[i]) atomicAdd(a.hist + i, (unsigned long long)sh[i]);
 }
 
-// Copies the values whose key matches (prefix, prefixMask) to out[0..cap).
-__global__ void select_compact_kernel(SelectArgs a, double* out, unsigned long long* count, long long cap) {
+// Block-wide search of a histogram of nb bins (1024 threads): the digit whose
+// cumulative count first exceeds `rank`, and the count below it.  Returns
+// false when the counts do not reach past the rank.
+__device__ bool find_digit(const unsigned long long* hist, int nb, long long rank, int* digit, long long* below) {
+    __shared__ long long part[1024];
+    __shared__ int sDigit;
+    __shared__ long long sBelow;
+    const int per = (nb + 1023) / 1024;
+    const int b0 = threadIdx.x * per, b1 = min(b0 + per, nb);
+    long long mine = 0;
+    for (int i = b0; i < b1; ++i) mine += (long long)hist[i];
+    part[threadIdx.x] = mine;
+    if (threadIdx.x == 0) sDigit = -1;
+    __syncthreads();
+    // inclusive scan of the parts (Hillis-Steele over 1024 entries)
+    for (int o = 1; o < 1024; o <<= 1) {
+        const long long x = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += x;
+        __syncthreads();
+    }
+    const long long before = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    if (before <= rank && rank < part[threadIdx.x]) {
+        long long acc = before;
+        for (int i = b0; i < b1; ++i) {
+            const long long c = (long long)hist[i];
+            if (acc + c > rank) {
+                sDigit = i;
+                sBelow = acc;
+                break;
+            }
+            acc += c;
+        }
+    }
+    __syncthreads();
+    *digit = sDigit;
+    *below = sBelow;
+    return sDigit >= 0;
+}
+
+// The digit holding the wanted rank from the last pass's histogram: the
+// prefix grows by it, the rank becomes the rank inside its bucket.  The
+// histogram is cleared for the next pass.  One block of 1024 threads.
+__global__ void median_scan_kernel(unsigned long long* hist, MedianState* st) {
+    __shared__ MedianState m;
+    if (threadIdx.x == 0) m = *st;
+    __syncthreads();
+    if (m.done) return;
+    if (m.bits < 1 || m.bits > kMedianWideBits || m.bits > m.shift) {
+        if (threadIdx.x == 0) {
+            st->err = 4;
+            st->done = 1;
+        }
+        return;
+    }
+    const int nb = 1 << m.bits;
+    int digit;
+    long long below;
+    const bool ok = find_digit(hist, nb, m.rank, &digit, &below);
+    if (threadIdx.x == 0) {
+        if (!ok) {
+            m.err = 1;
+            m.done = 1;
+        } else {
+            m.shift -= m.bits;
+            m.rank -= below;
+            m.bucket = (long long)hist[digit];
+            m.prefix |= (unsigned long long)digit << m.shift;
+            m.mask |= ((1ull << m.bits) - 1) << m.shift;
+            if (m.shift == 0 || m.bucket <= kMedianCompact) m.done = 1;
+            else m.bits = median_digit_bits(m.shift);
+        }
+        *st = m;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
+}
+
+// Copies the last bucket's values (keys matching the prefix) to out[0..cap);
+// nothing when every bit is fixed (the bucket's values are all equal).
+__global__ void median_compact_kernel(SelectArgs a, const MedianState* st, double* out, unsigned long long* count,
+                                      long long cap) {
+    __shared__ MedianState m;
+    if (threadIdx.x == 0) m = *st;
+    __syncthreads();
+    if (m.shift == 0 || m.err) return;
+    const unsigned long long prefix = m.prefix, mask = m.mask;
     for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
                          [&](long long, double x, bool valid, bool) {
-                           if (!valid || (order_key(x) & a.prefixMask) != a.prefix) return;
+                           if (!valid || (order_key(x) & mask) != prefix) return;
                            const unsigned long long at = atomicAdd(count, 1ull);
                            if ((long long)at < cap) out[at] = x;
                        });
 }
 
-// Smallest key strictly greater than `above` (all bits); *out starts at ~0.
-__global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, unsigned long long* out) {
+// The order statistics inside the last bucket (one block of 1024 threads):
+// xk of the rank, and for an even count the next one, either inside the
+// bucket or -- when the rank is the bucket's largest -- the smallest key
+// above it over the whole column (median_min_above_kernel, flagged here).
+// Radix selection over the bucket's remaining bits, 11 at a time.
+__global__ void median_select_kernel(MedianState* st, const double* band, const unsigned long long* count) {
+    __shared__ MedianState m;
+    __shared__ unsigned long long hist[1 << 11];
+    __shared__ unsigned long long sMin;
+    __shared__ long long sLess, sEq;
+    if (threadIdx.x == 0) m = *st;
+    __syncthreads();
+    if (m.err) return;
+    unsigned long long key;
+    unsigned long long top;  // largest key the bucket can hold
+    if (m.shift == 0) {
+        key = m.prefix;  // every member equals it
+        top = m.prefix;
+    } else {
+        const long long n = (long long)*count;
+        if (n != m.bucket || n > kMedianCompact) {
+            if (threadIdx.x == 0) {
+                st->err = 2;
+            }
+            return;
+        }
+        unsigned long long prefix = m.prefix, mask = m.mask;
+        long long rank = m.rank;
+        int shift = m.shift;
+        while (shift > 0) {
+            const int b = shift < 11 ? shift : 11;
+            shift -= b;
+            const int nb = 1 << b;
+            for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
+            __syncthreads();
+            for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+                const unsigned long long k = order_key(band[i]);
+                if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & (unsigned long long)(nb - 1)], 1ull);
+            }
+            __syncthreads();
+            int digit;
+            long long below;
+            if (!find_digit(hist, nb, rank, &digit, &below)) {
+                if (threadIdx.x == 0) st->err = 3;
+                return;
+            }
+            rank -= below;
+            prefix |= (unsigned long long)digit << shift;
+            mask |= ((unsigned long long)nb - 1) << shift;
+            __syncthreads();
+        }
+        key = prefix;
+        top = m.prefix | ~m.mask;
+    }
+    const double xk = key_to_double(key);
+    double xk1 = 0;
+    int needAbove = 0;
+    if (m.even) {
+        if (m.rank + 1 >= m.bucket) {
+            needAbove = 1;  // the next key lies above the bucket
+        } else if (m.shift == 0) {
+            xk1 = xk;
+        } else {
+            // keys below and equal to xk's inside the bucket; the next order
+            // statistic is xk again, or the smallest key above it
+            if (threadIdx.x == 0) {
+                sLess = 0;
+                sEq = 0;
+                sMin = ~0ull;
+            }
+            __syncthreads();
+            const long long n = (long long)*count;
+            long long less = 0, eq = 0;
+            unsigned long long mn = ~0ull;
+            for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+                const unsigned long long k = order_key(band[i]);
+                if (k < key) ++less;
+                else if (k == key) ++eq;
+                else if (k < mn) mn = k;
+            }
+            atomicAdd((unsigned long long*)&sLess, (unsigned long long)less);
+            atomicAdd((unsigned long long*)&sEq, (unsigned long long)eq);
+            atomicMin(&sMin, mn);
+            __syncthreads();
+            xk1 = m.rank + 1 < sLess + sEq ? xk : key_to_double(sMin);
+        }
+    }
+    if (threadIdx.x == 0) {
+        st->xk = xk;
+        st->xk1 = xk1;
+        st->needAbove = needAbove;
+        st->bucketTop = top;
+    }
+}
+
+// Smallest key strictly above the bucket over the whole column, when the
+// selection flagged it.
+__global__ void median_min_above_kernel(SelectArgs a, MedianState* st) {
+    __shared__ MedianState m;
+    if (threadIdx.x == 0) m = *st;
+    __syncthreads();
+    if (!m.needAbove || m.err) return;
+    const unsigned long long above = m.bucketTop;
     unsigned long long best = ~0ull;
     for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
                          [&](long long, double x, bool valid, bool) {
@@ -616,17 +833,35 @@ __global__ void select_min_above_kernel(SelectArgs a, unsigned long long above, 
         const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
         best = x < best ? x : best;
     }
-    if ((threadIdx.x & 31) == 0 && best != ~0ull) atomicMin(out, best);
+    if ((threadIdx.x & 31) == 0 && best != ~0ull) atomicMin(&st->minAbove, best);
 }
 
-// x <- min(round(factor * x), clip) on the valid entries: the float copy
-// always, the double column in place only when writeF64 (the host first
-// runs without it and keeps the float copy as the rescaled column when every
-// value is exact); clears *exact when a value is not a float.
-__global__ void rescale_kernel(double* col, float* col32, long long total, long long layerStride,
-                               long long interEntries, int nY, const int* tedgeInter, const int* tedgeIntra,
-                               double factor, double clip, int* exact, int writeF64) {
-    (void)total;
+// median = xk (odd count) or (xk + xk1) / 2; factor = scaling / (2
+// max(median, 0.001)), the host driver's double operations
+// (cost_time_ratio_solver.cpp:709-721, utils.hpp:196-209).
+__global__ void median_finish_kernel(MedianState* st, double scaling) {
+    MedianState m = *st;
+    if (m.err) {
+        st->factor = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const double xk1 = m.needAbove ? key_to_double(m.minAbove) : m.xk1;
+    const double median = m.even ? __ddiv_rn(__dadd_rn(m.xk, xk1), 2.0) : m.xk;
+    const double med = median < 0.001 ? 0.001 : median;
+    st->median = median;
+    st->factor = __ddiv_rn(scaling, __dmul_rn(2.0, med));
+}
+
+// x <- min(round(factor * x), clip) on the valid entries, factor from the
+// selection's state: the float copy always, the double column in place only
+// when writeF64 (the host first runs without it and keeps the float copy as
+// the rescaled column when every value is exact); sets st->inexact when a
+// value is not a float.
+__global__ void rescale_kernel(double* col, float* col32, long long layerStride, long long interEntries, int nY,
+                               const int* tedgeInter, const int* tedgeIntra, MedianState* st, double clip,
+                               int writeF64) {
+    const double factor = st->factor;
+    int* inexact = &st->inexact;
     for_stream_values<4>(col, layerStride, interEntries, nY, tedgeInter, tedgeIntra,
                          [&](long long idx, double v, bool valid, bool inRange) {
                            if (!inRange) return;
@@ -634,12 +869,12 @@ __global__ void rescale_kernel(double* col, float* col32, long long total, long 
                                if (col32) col32[idx] = __int_as_float(0x7fc00000);
                                return;
                            }
-                           double x = round(factor * v);
+                           double x = round(__dmul_rn(factor, v));
                            if (x > clip) x = clip;
                            if (writeF64) col[idx] = x;
                            const float f = (float)x;
                            if (col32) col32[idx] = f;
-                           if ((double)f != x) *exact = 0;
+                           if ((double)f != x) *inexact = 1;
                        });
 }
 // The double column from its exact float copy, on the valid entries.
@@ -1026,11 +1261,16 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
     quaternion_kernel<<<grid_for((long long)a.nY * a.nEX, 128), 128, 0, s>>>(a);
     return cudaGetLastError();
 }
-cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
-    const size_t smem = (size_t)(1 << a.bits) * sizeof(unsigned);
-    if (smem > 48 * 1024) {
-        // digits wider than 13 bits need the opt-in shared memory, set once
-        // per device
+// The whole median-and-rescale chain of one column on stream s; the state
+// holds the median, the factor and the error code when the stream reaches
+// them.  `topHist`: the energy kernel's first-digit histogram of the column,
+// or null (the first digit is counted here).  hist: 1 << kMedianWideBits
+// zeroed counters; band: kMedianCompact doubles; count: one zeroed counter.
+cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHist, MedianState* st,
+                                  unsigned long long* hist, double* band, unsigned long long* count, long long nValues,
+                                  double scaling, float* col32, double clip, cudaStream_t s) {
+    const size_t smem = sizeof(unsigned) << kMedianWideBits;
+    {
         static std::mutex mu;
         static std::set<int> done;
         int dev = 0;
@@ -1038,34 +1278,56 @@ cudaError_t launch_select_hist(const SelectArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         std::lock_guard<std::mutex> lk(mu);
         if (!done.count(dev)) {
-            e = cudaFuncSetAttribute(select_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(unsigned) << 14));
+            // the 14-bit digit's shared histogram is above the default 48 KB
+            e = cudaFuncSetAttribute(median_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
             done.insert(dev);
         }
     }
+    const int histGrid = stream_grid(median_hist_kernel, 512, smem);
+    const int grid = stream_grid(median_compact_kernel, 256, 0);
+    SelectArgs h = a;
+    h.hist = hist;
     note_launch();
-    select_hist_kernel<<<stream_grid(select_hist_kernel, 512, smem), 512, smem, s>>>(a);
+    median_init_kernel<<<1, 1, 0, s>>>(st, nValues);
+    if (topHist) {
+        note_launch();
+        median_scan_kernel<<<1, 1024, 0, s>>>(topHist, st);
+    } else {
+        note_launch();
+        median_hist_kernel<<<histGrid, 512, smem, s>>>(h, st);
+        note_launch();
+        median_scan_kernel<<<1, 1024, 0, s>>>(hist, st);
+    }
+    // at most five more digits fix all 64 bits (12 + 14 + 12 + 12 + 12 + 2);
+    // the passes after the selection is done return at once
+    for (int pass = 0; pass < 5; ++pass) {
+        note_launch();
+        median_hist_kernel<<<histGrid, 512, smem, s>>>(h, st);
+        note_launch();
+        median_scan_kernel<<<1, 1024, 0, s>>>(hist, st);
+    }
+    note_launch();
+    median_compact_kernel<<<grid, 256, 0, s>>>(a, st, band, count, kMedianCompact);
+    note_launch();
+    median_select_kernel<<<1, 1024, 0, s>>>(st, band, count);
+    note_launch();
+    median_min_above_kernel<<<grid, 256, 0, s>>>(a, st);
+    note_launch();
+    median_finish_kernel<<<1, 1, 0, s>>>(st, scaling);
+    note_launch();
+    rescale_kernel<<<grid, 256, 0, s>>>(const_cast<double*>(a.col), col32, a.layerStride, a.interEntries, a.nY,
+                                        a.tedgeInter, a.tedgeIntra, st, clip, 0);
     return cudaGetLastError();
 }
-cudaError_t launch_select_compact(const SelectArgs& a, double* out, unsigned long long* count, long long cap,
-                                  cudaStream_t s) {
+
+// The double column rescaled in place with the factor of the state (when its
+// float copy is not exact).
+cudaError_t launch_rescale_f64(const SelectArgs& a, MedianState* st, double clip, cudaStream_t s) {
     note_launch();
-    select_compact_kernel<<<stream_grid(select_compact_kernel, 256, 0), 256, 0, s>>>(a, out, count, cap);
-    return cudaGetLastError();
-}
-cudaError_t launch_select_min_above(const SelectArgs& a, unsigned long long above, unsigned long long* out,
-                                    cudaStream_t s) {
-    note_launch();
-    select_min_above_kernel<<<stream_grid(select_min_above_kernel, 256, 0), 256, 0, s>>>(a, above, out);
-    return cudaGetLastError();
-}
-cudaError_t launch_rescale(double* col, float* col32, long long total, long long layerStride, long long interEntries,
-                           int nY, const int* ti, const int* tr, double factor, double clip, int* exact,
-                           int writeF64, cudaStream_t s) {
-    note_launch();
-    rescale_kernel<<<stream_grid(rescale_kernel, 256, 0), 256, 0, s>>>(col, col32, total, layerStride, interEntries, nY, ti, tr,
-                                                        factor, clip, exact, writeF64);
+    rescale_kernel<<<stream_grid(rescale_kernel, 256, 0), 256, 0, s>>>(const_cast<double*>(a.col), nullptr,
+                                                                        a.layerStride, a.interEntries, a.nY,
+                                                                        a.tedgeInter, a.tedgeIntra, st, clip, 1);
     return cudaGetLastError();
 }
 cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,

@@ -472,6 +472,7 @@ class Graph {
         int rowCap;         // rows a step buffer holds (0: streams read in place)
         int stageSrcOnly;   // the buffers hold source indices only
         size_t smemBytes;   // dynamic shared memory per CTA
+        int ds = 0, dsCap = 0, dsOffset = 0;  // cluster-resident values (batched teams)
     };
     Run prepare_run(int K, bool ratio);
     // batch mode of prepare_run: a team of up to batchCtas CTAs of
@@ -479,6 +480,7 @@ class Graph {
     // batchSmemCap bytes
     int batchThreads = 0;
     int batchCtas = 1;
+    bool batchDs = false;  // the team is launched as a cluster: its values may live in shared memory
     size_t batchSmemCap = 0;
     void solve_ratio_rescaled(int K);
     void ensure_workspace(int K, int blocks);
@@ -495,8 +497,10 @@ class Graph {
     std::vector<int> read_cycle_buffer(int len);
     void lookup_pairs(const std::vector<int>& src, const std::vector<int>& trgt, std::vector<long long>& edges,
                       std::vector<double>& c, std::vector<double>& t, double tconst);
-    double median_of_column(int col);
-    void rescale_column(int col, double scaling);
+    void rescale_columns(double scaling);
+    DBuf<MedianState> wMedState;
+    DBuf<unsigned long long> wMedHist, wMedCount;
+    DBuf<double> wMedBand;
     void ensure_f32(int col);
     void rows_for_edges(const std::vector<long long>& edges);
 };
@@ -667,148 +671,59 @@ void Graph::generate() {
 // Rescaling: cost_time_ratio_solver.cpp:709-721 with utils::median
 // (utils.hpp:196-209).  The k-th value is found by radix selection.
 // ---------------------------------------------------------------------------
-// The device's order-preserving 64-bit image of a double (order_key).
-static unsigned long long host_order_key(double x) {
-    unsigned long long u;
-    std::memcpy(&u, &x, sizeof(u));
-    return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
-}
-
-double Graph::median_of_column(int col) {
+// Both cost columns' medians and rescales, enqueued whole on the handle's
+// stream (launch_median_rescale: radix selection whose state stays on the
+// device), then one wait.  The double column is rewritten only when some
+// rescaled value is not a float.
+void Graph::rescale_columns(double scaling) {
     const long long stride = T.layerStride();
     const long long total = (long long)(T.nY + 1) * stride;
     const long long count = (long long)T.nY * T.eBlock;
     if (count <= 0) throw Failure(PGC_ERR_STATE, "empty product graph");
-    // Order statistics k (and k+1 for an even count) by MSD radix selection on
-    // the order-preserving 64-bit keys: 12-bit digits; as soon as the bucket
-    // holding rank k has at most kCompact members it is copied out and
-    // finished on the host.  If rank k is the largest of its bucket, rank k+1
-    // is the smallest key above the bucket (one reduction pass).
-    // digit widths: the first (counted by the energy kernel), a wider second
-    // one (a 64 KB shared histogram: on the default pair it leaves a bucket
-    // small enough to copy out, where 12 bits needed a third pass), then 12
-    const int bits = kTopDigitBits, bits2 = 14, bitsMax = 14;
-    const long long kCompact = 1 << 16;
-    DBuf<unsigned long long> hist, cnt;
-    DBuf<double> band;
-    hist.alloc((size_t)1 << bitsMax);
-    cnt.alloc(1);
-    std::vector<unsigned long long> h((size_t)1 << bitsMax);
-    SelectArgs a{};
-    ensure_e64(col);
-    a.col = e64[col].p;
-    a.total = total;
-    a.layerStride = stride;
-    a.interEntries = T.entries[INTER];
-    a.nY = T.nY;
-    a.tedgeInter = dTedge[INTER].p;
-    a.tedgeIntra = dTedge[INTRA].p;
-    a.hist = hist.p;
-    auto key_to_double = [](unsigned long long key) {
-        const unsigned long long u = (key >> 63) ? (key & 0x7fffffffffffffffULL) : ~key;
-        double x;
-        std::memcpy(&x, &u, sizeof(x));
-        return x;
+    wMedState.alloc(2);
+    wMedHist.alloc((size_t)1 << kMedianWideBits);
+    wMedBand.alloc((size_t)kMedianCompact);
+    wMedCount.alloc(1);
+    PGC_CUDA(cudaMemsetAsync(wMedHist.p, 0, sizeof(unsigned long long) << kMedianWideBits, stream));
+    auto args = [&](int col) {
+        SelectArgs a{};
+        a.col = e64[col].p;
+        a.total = total;
+        a.layerStride = stride;
+        a.interEntries = T.entries[INTER];
+        a.nY = T.nY;
+        a.tedgeInter = dTedge[INTER].p;
+        a.tedgeIntra = dTedge[INTRA].p;
+        return a;
     };
-    const bool even = count % 2 == 0;
-    const long long k = even ? (count - 2) / 2 : count / 2;
-    unsigned long long prefix = 0, mask = 0;
-    int shift = 64;
-    long long rank = k, bucket = count;
-    while (shift > 0 && bucket > kCompact) {
-        const int b = std::min(mask == 0 ? bits : shift == 64 - bits ? bits2 : bits, shift);
-        shift -= b;
-        a.prefix = prefix;
-        a.prefixMask = mask;
-        a.shift = shift;
-        a.bits = b;
-        if (mask == 0 && b == kTopDigitBits && topHistValid[col]) {
-            // the first digit was counted when the column was written
-            d2h(h.data(), topHist[col].p, sizeof(unsigned long long) << b);
-        } else {
-            PGC_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) << b, stream));
-            PGC_CUDA(launch_select_hist(a, stream));
-            stats.launches++;
-            d2h(h.data(), hist.p, sizeof(unsigned long long) << b);
-        }
-        PGC_CUDA(sync_stream());
-        int digit = 0;
-        long long acc = 0;
-        for (; digit < (1 << b); ++digit) {
-            if (acc + (long long)h[(size_t)digit] > rank) break;
-            acc += (long long)h[(size_t)digit];
-        }
-        if (digit >= (1 << b)) throw Failure(PGC_ERR_INTERNAL, "median selection lost its rank");
-        rank -= acc;
-        bucket = (long long)h[(size_t)digit];
-        prefix |= (unsigned long long)digit << shift;
-        mask |= (((unsigned long long)1 << b) - 1) << shift;
+    for (int col = 0; col < ncols; ++col) {
+        ensure_e64(col);
+        e32[col].alloc((size_t)total);
+        PGC_CUDA(cudaMemsetAsync(wMedCount.p, 0, sizeof(unsigned long long), stream));
+        PGC_CUDA(launch_median_rescale(args(col), topHistValid[col] ? topHist[col].p : nullptr, wMedState.p + col,
+                                       wMedHist.p, wMedBand.p, wMedCount.p, count, scaling, e32[col].p, 100 * scaling,
+                                       stream));
+        stats.launches += topHistValid[col] ? 17 : 18;
     }
-    double xk, xk1 = 0;
-    unsigned long long bucketTop;  // largest key the bucket can hold
-    if (shift == 0) {
-        xk = key_to_double(prefix);  // every member of the bucket equals it
-        if (even && rank + 1 < bucket) xk1 = xk;
-        bucketTop = prefix;
-    } else {
-        band.alloc((size_t)bucket);
-        a.prefix = prefix;
-        a.prefixMask = mask;
-        PGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), stream));
-        PGC_CUDA(launch_select_compact(a, band.p, cnt.p, bucket, stream));
-        stats.launches++;
-        std::vector<double> vals((size_t)bucket);
-        d2h(vals.data(), band.p, sizeof(double) * (size_t)bucket);
-        PGC_CUDA(sync_stream());
-        // the bucket's order statistics rank (and rank + 1) in the key order
-        // of the passes (numeric order for every non-NaN value)
-        auto keyLess = [](double x, double y) { return host_order_key(x) < host_order_key(y); };
-        std::nth_element(vals.begin(), vals.begin() + rank, vals.end(), keyLess);
-        xk = vals[(size_t)rank];
-        if (even && rank + 1 < bucket) xk1 = *std::min_element(vals.begin() + rank + 1, vals.end(), keyLess);
-        bucketTop = prefix | ~mask;
-    }
-    if (!even) return xk;
-    if (rank + 1 >= bucket) {
-        unsigned long long best = ~0ull;
-        PGC_CUDA(cudaMemcpyAsync(cnt.p, &best, sizeof(best), cudaMemcpyHostToDevice, stream));
-        PGC_CUDA(launch_select_min_above(a, bucketTop, cnt.p, stream));
-        stats.launches++;
-        d2h(&best, cnt.p, sizeof(best));
-        PGC_CUDA(sync_stream());
-        xk1 = key_to_double(best);
-    }
-    return (xk + xk1) / 2.0;
-}
-
-void Graph::rescale_column(int col, double scaling) {
-    const double med = std::max(median_of_column(col), 0.001);
-    const double factor = scaling / (2.0 * med);
-    const long long stride = T.layerStride();
-    const long long total = (long long)(T.nY + 1) * stride;
-    e32[col].alloc((size_t)total);
-    wCount.alloc(1);
-    const int one = 1;
-    PGC_CUDA(cudaMemcpyAsync(wCount.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
-    // the float copy first; the double column only when a value is not exact
-    PGC_CUDA(launch_rescale(e64[col].p, e32[col].p, total, stride, T.entries[INTER], T.nY, dTedge[INTER].p,
-                            dTedge[INTRA].p, factor, 100 * scaling, wCount.p, 0, stream));
-    stats.launches++;
-    int exact = 0;
-    d2h(&exact, wCount.p, sizeof(int));
+    MedianState st[2];
+    d2h(st, wMedState.p, sizeof(MedianState) * (size_t)ncols);
     PGC_CUDA(sync_stream());
-    if (exact) {
-        e64Stale[col] = true;
-    } else {
-        PGC_CUDA(launch_rescale(e64[col].p, e32[col].p, total, stride, T.entries[INTER], T.nY, dTedge[INTER].p,
-                                dTedge[INTRA].p, factor, 100 * scaling, wCount.p, 1, stream));
-        stats.launches++;
-        PGC_CUDA(sync_stream());
+    bool rewrite = false;
+    for (int col = 0; col < ncols; ++col) {
+        if (st[col].err) throw Failure(PGC_ERR_INTERNAL, "median selection lost its rank");
+        if (st[col].inexact) {
+            PGC_CUDA(launch_rescale_f64(args(col), wMedState.p + col, 100 * scaling, stream));
+            stats.launches++;
+            rewrite = true;
+        } else {
+            e64Stale[col] = true;
+        }
+        f32Valid[col] = st[col].inexact == 0;
+        f32Known[col] = true;
+        topHistValid[col] = false;
+        colScale[col] *= st[col].factor;
     }
-    f32Valid[col] = exact != 0;
-    f32Known[col] = true;
-    topHistValid[col] = false;
-    colScale[col] *= factor;
+    if (rewrite) PGC_CUDA(sync_stream());
 }
 
 void Graph::ensure_e64(int col) {
@@ -912,6 +827,30 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
             } else {
                 r.rowCap = 0;
                 need = bf_stage_offset(maxSl);
+            }
+        }
+        // cluster-resident values: each CTA's own nodes' records ([2][cap][Kp]
+        // doubles) and the slice owner table after the staging area, when
+        // they fit beside the full staging or beside the source indices alone
+        if (batchDs && r.blocks > 1 && r.blocks <= 8 && env_int("PGC_BATCH_DS", 1)) {
+            int ownCap = 0;
+            for (int c = 0; c < r.blocks; ++c)
+                ownCap = std::max(ownCap, std::min(cut[(size_t)c + 1] * 32, T.n) - cut[(size_t)c] * 32);
+            const size_t dsBytes = (size_t)2 * ownCap * r.Kp * sizeof(double) + (size_t)T.nslices;
+            auto at = [](size_t b) { return (b + 31) / 32 * 32; };
+            size_t stage = need;
+            if (at(stage) + dsBytes > batchSmemCap && stageOn && r.rowCap > 0 && !r.stageSrcOnly) {
+                const size_t srcOnly = bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(r.rowCap, 0, 0);
+                if (at(srcOnly) + dsBytes <= batchSmemCap) {
+                    r.stageSrcOnly = 1;
+                    stage = srcOnly;
+                }
+            }
+            if (at(stage) + dsBytes <= batchSmemCap) {
+                r.ds = 1;
+                r.dsCap = ownCap;
+                r.dsOffset = (int)at(stage);
+                need = at(stage) + dsBytes;
             }
         }
         if (need > batchSmemCap) throw Failure(PGC_ERR_ARG, "the graph's slice lists exceed the batch's shared memory");
@@ -1100,6 +1039,9 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.maxCtaSlices = r.maxCtaSlices;
     p.rowCap = r.rowCap;
     p.stageSrcOnly = r.stageSrcOnly;
+    p.ds = r.ds;
+    p.dsCap = r.dsCap;
+    p.dsOffset = r.dsOffset;
     p.lapNext = wLapNext.p;
     p.lapSteps = wLapSteps.p;
     p.walks = wWalks.p;
@@ -1276,8 +1218,7 @@ void Graph::solve_ratio(int K) {
     const auto wall0 = std::chrono::steady_clock::now();
     const double scaling = 100000.0;
     // In-place rescale of the generator's costs (cost_time_ratio_solver.cpp:875-882).
-    rescale_column(0, scaling);
-    if (ncols > 1) rescale_column(1, scaling);
+    rescale_columns(scaling);
     solve_ratio_rescaled(K);
     (void)wall0;
 }
@@ -1491,16 +1432,36 @@ void Graph::solve_ratio_rescaled(int K) {
     adjLambda = fin.ratio;
 }
 
+// Host wall time the batch workers spent in batch_begin's phases, summed
+// over workers (ns): costs generated, columns rescaled, team prepared.
+// Printed by pgc_solve_batch when PGC_BATCH_PHASES is set.
+std::atomic<long long> g_batchPhaseNs[3];
+
 void Graph::batch_begin(int K, PairJob& J, int threads, int ctas, size_t smemCap, bool regenerate) {
+    const auto t0 = std::chrono::steady_clock::now();
     if (regenerate) generate();
     else ensure_generated();
+    if (blockingSync) PGC_CUDA(sync_stream());
+    const auto t1 = std::chrono::steady_clock::now();
     stats = Stats();
     batchK = K;
     const double scaling = 100000.0;
-    rescale_column(0, scaling);
-    if (ncols > 1) rescale_column(1, scaling);
+    rescale_columns(scaling);
+    const auto t2 = std::chrono::steady_clock::now();
+    struct PhaseTimer {
+        std::chrono::steady_clock::time_point a, b, c;
+        ~PhaseTimer() {
+            const auto ns = [](auto x, auto y) {
+                return (long long)std::chrono::duration_cast<std::chrono::nanoseconds>(y - x).count();
+            };
+            g_batchPhaseNs[0] += ns(a, b);
+            g_batchPhaseNs[1] += ns(b, c);
+            g_batchPhaseNs[2] += ns(c, std::chrono::steady_clock::now());
+        }
+    } phaseTimer{t0, t1, t2};
     batchThreads = threads;
     batchCtas = std::max(1, ctas);
+    batchDs = batchCtas > 1 && batchCtas <= 8;
     batchSmemCap = smemCap;
     Run r;
     try {
@@ -1526,6 +1487,7 @@ void Graph::batch_begin(int K, PairJob& J, int threads, int ctas, size_t smemCap
     J.bf = params(r, 0, 0, 0.0, std::numeric_limits<float>::infinity());
     J.bf.ctaSlice = wCtaSlice.p;
     J.ctas = r.blocks;
+    J.threads = r.threads;
     LookupArgs& a = J.lk;
     a.n = T.n;
     a.nY = T.nY;
@@ -1589,7 +1551,7 @@ void Graph::batch_end(const PairJob& J) {
             stats.deviceMs = (double)J.cycles / info.clockKhz;  // the CTA's time on this graph at the top SM clock
     }
     stats.ctas = J.ctas;
-    stats.threads = J.bf.maxCtaSlices >= 0 ? kBatchThreads : 0;
+    stats.threads = J.threads;
     switch (J.status) {
         case PAIR_DONE: {
             std::vector<long long> edges((size_t)std::max(0, J.nEdges));
@@ -2401,7 +2363,8 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
             const size_t smemCap = (size_t)std::max(0, info.smemOptin / pgc::kBatchBlocksPerSm - 2048);
             // CTAs per team (PGC_BATCH_TEAM, default 8): a team relaxes a
             // graph's steps side by side, so more CTAs per graph shorten each
-            // solve; fewer overlap more graphs' latencies
+            // solve; fewer overlap more graphs' latencies.  Teams of 2-8 CTAs
+            // are launched as thread-block clusters.
             int team = ctas_per_graph > 0 ? ctas_per_graph : pgc::env_int("PGC_BATCH_TEAM", 8);
             team = std::max(1, std::min(team, sms * pgc::kBatchBlocksPerSm));
             const unsigned spin = (unsigned)std::max(1, pgc::env_int("PGC_BF_SPIN_LIMIT", (int)pgc::kDefaultSpinLimit));
@@ -2431,6 +2394,12 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
                 });
             });
             g_batchProfile[0] = ms_since(tStart);
+            if (std::getenv("PGC_BATCH_PHASES")) {
+                std::fprintf(stderr, "[pgc] batch preparation, summed over %d workers: generate %.1f ms, rescale %.1f ms, "
+                             "team %.1f ms; wall %.1f ms\n", workers, pgc::g_batchPhaseNs[0].exchange(0) * 1e-6,
+                             pgc::g_batchPhaseNs[1].exchange(0) * 1e-6, pgc::g_batchPhaseNs[2].exchange(0) * 1e-6,
+                             g_batchProfile[0]);
+            }
             const auto tKernel = std::chrono::steady_clock::now();
             // one launch per (cost type, time kind) group, largest graphs first
             pgc::DBuf<PairJob> dJobs;
@@ -2472,10 +2441,17 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
                     int perSm = 0;
                     PGC_CUDA(pgc::bf_batch_max_blocks(cf, tk, threads, smem, &perSm));
                     if (perSm < 1) throw Failure(PGC_ERR_CUDA, "the batched solve kernel cannot be resident");
-                    // whole teams, all resident (the launch is cooperative
-                    // when a team has more than one CTA)
+                    // whole teams, all resident: clusters of 2-8 CTAs, or a
+                    // cooperative launch for larger teams
                     const int g = std::min(team, sms * perSm);
-                    const int teams = (int)std::min<size_t>({k1 - k0, (size_t)(sms * perSm / g), maxTeams});
+                    int residentTeams = sms * perSm / g;
+                    if (g > 1 && g <= 8) {
+                        int clusters = 0;
+                        PGC_CUDA(pgc::bf_batch_max_clusters(cf, tk, threads, smem, g, &clusters));
+                        if (clusters < 1) throw Failure(PGC_ERR_CUDA, "no cluster of the batched solve kernel fits");
+                        residentTeams = std::min(residentTeams, clusters);
+                    }
+                    const int teams = (int)std::min<size_t>({k1 - k0, (size_t)residentTeams, maxTeams});
                     const int blocks = teams * g;
                     PGC_CUDA(cudaMemsetAsync(dTeamWords.p, 0, (size_t)teams * pgc::kTeamWordStride * sizeof(unsigned), bs));
                     g_batchProfile[5] += blocks;
