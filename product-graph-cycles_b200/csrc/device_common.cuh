@@ -117,12 +117,6 @@ struct BfParams {
     unsigned spinLimit;            // polls of any wait before it gives up and raises the error word
     int stallCta;                  // test hook (-1: none): this CTA's hand-off also waits on ctl->neverSet
     int literalAll;                // test hook: decide every candidate by the literal walk
-    // cluster-resident values of a batched team: each CTA keeps [2][dsCap][Kp]
-    // doubles of the nodes it owns at byte dsOffset of its dynamic shared
-    // memory, followed by the owner CTA of every slice (nslices bytes)
-    int ds;
-    int dsCap;
-    int dsOffset;
     Control* ctl;
     int* cycleBuf;                 // original node ids, walk order (reversed on the host)
     long long cycleCap;
@@ -339,9 +333,6 @@ cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamW
                             int costIsF32, int timeKind, int blocks, int threads, size_t smemBytes,
                             cudaStream_t stream);
 cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
-// Clusters of clusterCtas CTAs of the batched kernel that fit the device at once.
-cudaError_t bf_batch_max_clusters(int costIsF32, int timeKind, int threads, size_t smemBytes, int clusterCtas,
-                                  int* clusters);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);

@@ -375,51 +375,6 @@ __device__ __forceinline__ void stage_drain(Stage& st) {
 // fold.  Returns whether this thread improved a node.
 // ---------------------------------------------------------------------------
 
-// Cluster-resident DP values of a batched team (BfParams::ds): every CTA of
-// the team (a thread-block cluster) keeps the values of the nodes it owns,
-// [2 parities][cap][Kp] doubles, in its shared memory; a source's values are
-// read from its owner's copy over distributed shared memory.
-constexpr int kMaxDsCtas = 8;
-struct DsCtx {
-    unsigned base[kMaxDsCtas];    // shared::cluster address of each team CTA's copy
-    int lo[kMaxDsCtas];           // first node each CTA owns
-    const unsigned char* owner;   // owner CTA of every 32-node slice
-    double* mine;                 // this CTA's copy
-    int myLo, myCount, cap;
-};
-
-__device__ __forceinline__ unsigned ds_addr(const DsCtx& c, unsigned parityOff, int s, int Kp, int kofs) {
-    const int o = c.owner[s >> 5];
-    return c.base[o] + parityOff + (unsigned)(((s - c.lo[o]) * Kp + kofs) * 8);
-}
-
-// The NK values of consecutive depths at shared::cluster address `a` (the
-// record of one node in its owner's copy; 16-byte aligned when NK >= 2).
-template <int NK>
-__device__ __forceinline__ void ld_row_ds(unsigned a, double (&d)[NK]) {
-    if constexpr (NK == 1) {
-        asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(d[0]) : "r"(a) : "memory");
-    } else {
-        static_assert(NK <= 4, "a node row holds at most four depths here");
-        double x0, x1;
-        asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(x0), "=d"(x1) : "r"(a) : "memory");
-        d[0] = x0;
-        d[1] = x1;
-        if constexpr (NK >= 3) {
-            double y0, y1;
-            asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(y0), "=d"(y1) : "r"(a + 16) : "memory");
-            d[2] = y0;
-            if constexpr (NK == 4) d[3] = y1;
-            else (void)y1;
-        }
-    }
-}
-__device__ __forceinline__ double ld_ds(unsigned a) {
-    double x;
-    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(x) : "r"(a) : "memory");
-    return x;
-}
-
 struct StepView {
     const int* src;     // source index per entry, from the step's first row
     const void* cost;
@@ -428,8 +383,6 @@ struct StepView {
     size_t sbase;       // record index of the source layer's record 0
     int Kp, kofs, nk;
     double lam, tconst;
-    const DsCtx* ds;    // cluster-resident values (DS), and the byte offset of the source parity in a copy
-    unsigned parityOff;
 };
 
 template <class CT, int TK>
@@ -445,7 +398,7 @@ __device__ __forceinline__ double edge_weight(const StepView& v, int q) {
 // One batch of exactly NR rows starting at `row`: every source value is
 // gathered first, then the batch is folded in edge order.  `win` records the
 // position of the last improvement (row * 8 + depth); thr is its value.
-template <class CT, int TK, bool S, int NK, int NR, bool DS>
+template <class CT, int TK, bool S, int NK, int NR>
 __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row, double& thr, int& win) {
     int sv[NR];
     double d[NR][NK];
@@ -453,8 +406,7 @@ __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row,
     for (int r = 0; r < NR; ++r) {
         sv[r] = v.src[(row + r) * 32 + lane];
         if (sv[r] >= 0) {
-            if constexpr (DS) ld_row_ds<NK>(ds_addr(*v.ds, v.parityOff, sv[r], v.Kp, v.kofs), d[r]);
-            else ld_row<S, NK>(v.srcv + (size_t)sv[r] * v.Kp + v.kofs, d[r]);
+            ld_row<S, NK>(v.srcv + (size_t)sv[r] * v.Kp + v.kofs, d[r]);
         } else {
 #pragma unroll
             for (int kk = 0; kk < NK; ++kk) d[r][kk] = kInfD;
@@ -475,26 +427,26 @@ __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row,
 // The last nr (1 <= nr <= NR) rows as one batch of exactly nr rows.  The row
 // count is the slice's, the same in every lane, so no lane runs row slots
 // that do not exist.
-template <class CT, int TK, bool S, int NK, int NR, bool DS>
+template <class CT, int TK, bool S, int NK, int NR>
 __device__ __forceinline__ void fold_tail(const StepView& v, int lane, int row, int nr, double& thr, int& win) {
     if constexpr (NR <= 1) {
-        fold_batch<CT, TK, S, NK, 1, DS>(v, lane, row, thr, win);
+        fold_batch<CT, TK, S, NK, 1>(v, lane, row, thr, win);
     } else {
-        if (nr == NR) fold_batch<CT, TK, S, NK, NR, DS>(v, lane, row, thr, win);
-        else fold_tail<CT, TK, S, NK, NR - 1, DS>(v, lane, row, nr, thr, win);
+        if (nr == NR) fold_batch<CT, TK, S, NK, NR>(v, lane, row, thr, win);
+        else fold_tail<CT, TK, S, NK, NR - 1>(v, lane, row, nr, thr, win);
     }
 }
 
 // Rows [row, j1) of one slice for lane `lane`.  Returns the position of the
 // winning candidate -- row * 8 + depth for NK > 0, row * nk + depth for the
 // run-time depth count (NK == 0) -- or -1; thr holds its value.
-template <class CT, int TK, bool S, int NK, bool DS>
+template <class CT, int TK, bool S, int NK>
 __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, int j1, double& thr) {
     int win = -1;
     if constexpr (NK > 0) {
         constexpr int RB = bf_rows_per_batch(NK);
-        for (; j1 - row >= RB; row += RB) fold_batch<CT, TK, S, NK, RB, DS>(v, lane, row, thr, win);
-        if (row < j1) fold_tail<CT, TK, S, NK, RB, DS>(v, lane, row, j1 - row, thr, win);
+        for (; j1 - row >= RB; row += RB) fold_batch<CT, TK, S, NK, RB>(v, lane, row, thr, win);
+        if (row < j1) fold_tail<CT, TK, S, NK, RB>(v, lane, row, j1 - row, thr, win);
     } else {
         for (; row < j1; ++row) {
             const int sv = v.src[row * 32 + lane];
@@ -502,10 +454,7 @@ __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, i
             const double w = edge_weight<CT, TK>(v, row * 32 + lane);
             const double* rec = v.srcv + (size_t)sv * v.Kp + v.kofs;
             for (int kk = 0; kk < v.nk; ++kk) {
-                double x;
-                if constexpr (DS) x = ld_ds(ds_addr(*v.ds, v.parityOff, sv, v.Kp, v.kofs + kk));
-                else x = S ? rec[kk] : __ldcg(rec + kk);
-                const double cand = __dadd_rn(x, w);
+                const double cand = __dadd_rn(S ? rec[kk] : __ldcg(rec + kk), w);
                 if (cand < thr) { thr = cand; win = row * v.nk + kk; }
             }
         }
@@ -513,7 +462,7 @@ __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, i
     return win;
 }
 
-template <class CT, int TK, bool S, int NK, bool DS>
+template <class CT, int TK, bool S, int NK>
 __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* spl, const int* act, int nAct, int s0,
                              int s1, int l, int k) {
     const int n = p.n, K = p.K, Kp = p.Kp;
@@ -543,7 +492,7 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
         double best = (l == 0 && valid) ? ldV<S>(p, me) : kInfD;
         double thr = best < ub ? best : ub;
         int win = -1;
-        if (!empty) win = fold_rows<CT, TK, S, NK, DS>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, thr);
+        if (!empty) win = fold_rows<CT, TK, S, NK>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, thr);
         if (!valid) continue;
         int o = kLapUnknown, h = 0;
         int bs = -1, bk = -1;
@@ -584,17 +533,12 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
             }
         }
         stE(p, cur, v, k, best, o, h);
-        if constexpr (DS) {
-            const DsCtx& c = *sv.ds;
-            c.mine[((size_t)(l & 1) * c.cap + (v - c.myLo)) * Kp + k] = best;
-        }
     }
     return any;
 }
 
-template <class CT, int TK, bool S, bool DS = false>
-__device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, int s1, int l, int k,
-                           const DsCtx* ds = nullptr) {
+template <class CT, int TK, bool S>
+__device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, int s1, int l, int k) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const bool inter = (k == 0);
     const int part = inter ? 0 : 1;
@@ -623,17 +567,15 @@ __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, i
     v.nk = inter ? K : 1;
     v.lam = p.lambda;
     v.tconst = p.tconst;
-    v.ds = ds;
-    v.parityOff = DS ? (unsigned)(((inter ? l - 1 : l) & 1) * (size_t)p.dsCap * Kp * 8) : 0u;
     const int* act = st.act(part);
     const int na = st.nAct(part);
-    if (!inter) return relax_slices<CT, TK, S, 1, DS>(p, v, spl, act, na, s0, s1, l, k);
+    if (!inter) return relax_slices<CT, TK, S, 1>(p, v, spl, act, na, s0, s1, l, k);
     switch (K) {
-        case 1: return relax_slices<CT, TK, S, 1, DS>(p, v, spl, act, na, s0, s1, l, k);
-        case 2: return relax_slices<CT, TK, S, 2, DS>(p, v, spl, act, na, s0, s1, l, k);
-        case 3: return relax_slices<CT, TK, S, 3, DS>(p, v, spl, act, na, s0, s1, l, k);
-        case 4: return relax_slices<CT, TK, S, 4, DS>(p, v, spl, act, na, s0, s1, l, k);
-        default: return relax_slices<CT, TK, S, 0, DS>(p, v, spl, act, na, s0, s1, l, k);
+        case 1: return relax_slices<CT, TK, S, 1>(p, v, spl, act, na, s0, s1, l, k);
+        case 2: return relax_slices<CT, TK, S, 2>(p, v, spl, act, na, s0, s1, l, k);
+        case 3: return relax_slices<CT, TK, S, 3>(p, v, spl, act, na, s0, s1, l, k);
+        case 4: return relax_slices<CT, TK, S, 4>(p, v, spl, act, na, s0, s1, l, k);
+        default: return relax_slices<CT, TK, S, 0>(p, v, spl, act, na, s0, s1, l, k);
     }
 }
 
@@ -930,7 +872,7 @@ __device__ int dij_walk_end(const BfParams& p, int v) {
 // the dynamic shared memory after the DP tables: [row offsets and lists of
 // slices with rows][two step buffers].
 // ---------------------------------------------------------------------------
-template <class CT, int TK, bool S, bool DS = false>
+template <class CT, int TK, bool S>
 __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* smem) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const long long tid = t.thread(), nth = t.nthreads();
@@ -995,33 +937,6 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
         st.nActInter = nActive[0];
         st.nActIntra = nActive[1];
     }
-    // cluster-resident values (DS): the team is a cluster whose CTA ranks are
-    // the team's CTA indices; every CTA's copy sits at the same offset
-    __shared__ DsCtx dsc;
-    if constexpr (DS) {
-        double* mine = reinterpret_cast<double*>(smem + p.dsOffset);
-        unsigned char* owner = reinterpret_cast<unsigned char*>(smem + p.dsOffset) + (size_t)2 * p.dsCap * Kp * 8;
-        if (threadIdx.x < t.ncta) {
-            const int c = threadIdx.x;
-            unsigned a;
-            asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_addr(mine)), "r"(c));
-            dsc.base[c] = a;
-            dsc.lo[c] = __ldg(p.ctaSlice + c) * 32;
-        }
-        for (int i = threadIdx.x; i < p.nslices; i += blockDim.x) {
-            int c = 0;
-            while (c + 1 < t.ncta && __ldg(p.ctaSlice + c + 1) <= i) ++c;
-            owner[i] = (unsigned char)c;
-        }
-        if (threadIdx.x == 0) {
-            dsc.owner = owner;
-            dsc.mine = mine;
-            dsc.myLo = s0 * 32;
-            dsc.myCount = min(s1 * 32, n) - s0 * 32;
-            dsc.cap = p.dsCap;
-        }
-        __syncthreads();
-    }
 
     // set-up (cost_time_ratio_solver.cpp:264-287): DP := inf, branch starts := 0
     // (each record is written once, by one thread)
@@ -1085,17 +1000,6 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
         // the first step of the sweep is staged while the backup row is copied
         stage_issue(p, st, s0, s1, 0, kSteps > 1 ? 0 : 1, kSteps > 1 ? 1 : 0);
         for (long long i = tid; i < n; i += nth) p.bak[i] = ldV<S>(p, (size_t)i * Kp);
-        if constexpr (DS) {
-            // the copy of this CTA's nodes from the global records, which the
-            // set-up and the last sweep's wrap-around wrote; the team barrier
-            // below publishes it before any CTA gathers from it
-            const int cnt = dsc.myCount * Kp;
-            for (int i = threadIdx.x; i < 2 * cnt; i += blockDim.x) {
-                const int par = i >= cnt ? 1 : 0, rem = i - par * cnt;
-                dsc.mine[(size_t)par * dsc.cap * Kp + rem] =
-                    __ldcg(p.dv + (size_t)par * n * Kp + (size_t)dsc.myLo * Kp + rem);
-            }
-        }
         if (!team_sync(t)) { stage_drain(st); return; }
         // Layers are relaxed in order; a CTA hands each step off to its
         // graph neighbours only (one team barrier closes the sweep).  The
@@ -1119,7 +1023,7 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
                 if (isLead) cycStage += clock64() - ta;
                 const bool last = l == p.nY && k == kSteps - 1;
                 if (!last) stage_issue(p, st, s0, s1, sb ^ 1, k + 1 < kSteps ? l : l + 1, k + 1 < kSteps ? k + 1 : 0);
-                const bool any = relax_step<CT, TK, S, DS>(p, st, sb, s0, s1, l, k, &dsc);
+                const bool any = relax_step<CT, TK, S>(p, st, sb, s0, s1, l, k);
                 if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) p.layerFlag[l] = stamp;
                 const unsigned long long tb = isLead ? clock64() : 0;
                 ++step;
@@ -1624,10 +1528,6 @@ template <class CT, int TK>
 __device__ __noinline__ void bf_call(const BfParams& P, const Team& t, char* smem) {
     bf_body<CT, TK, false>(P, t, smem);
 }
-template <class CT, int TK>
-__device__ __noinline__ void bf_call_ds(const BfParams& P, const Team& t, char* smem) {
-    bf_body<CT, TK, false, true>(P, t, smem);
-}
 
 // One Bellman-Ford call of the team: the lead publishes the call's state,
 // the Bellman-Ford CTAs run it, and every CTA reads its verdict after the
@@ -1639,10 +1539,7 @@ __device__ bool team_bf_call(PairJob& J, const BfParams& P, const SolveTeam& S, 
         if (resetError) P.ctl->error = 0;
     }
     if (!team_sync(S.all)) return false;
-    if (S.in_bf()) {
-        if (P.ds) bf_call_ds<CT, TK>(P, S.bf, smem);
-        else bf_call<CT, TK>(P, S.bf, smem);
-    }
+    if (S.in_bf()) bf_call<CT, TK>(P, S.bf, smem);
     if (!team_sync(S.all)) return false;
     if (S.lead()) {
         J.bfCalls++;
@@ -1896,11 +1793,11 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchBlocksPerSm)
     const bool lead = cta == 0 && threadIdx.x == 0;
     for (;;) {
         if (lead) w[3] = (unsigned)atomicAdd(next, 1);
-        if (!team_sync(all)) break;
+        if (!team_sync(all)) return;
         if (threadIdx.x == 0) sJob = (int)__ldcg(w + 3);
         __syncthreads();
         const int j = sJob;
-        if (j >= count) break;
+        if (j >= count) return;
         if (threadIdx.x == 0) {
             P = jobs[j].bf;
             sCtas = jobs[j].ctas < 1 ? 1 : jobs[j].ctas > teamCtas ? teamCtas : jobs[j].ctas;
@@ -1915,12 +1812,8 @@ __global__ void __launch_bounds__(kBatchThreads, kBatchBlocksPerSm)
             jobs[j].cycles = clock64() - c0;
         }
         // nobody draws the next job before every CTA has read this one
-        if (!team_sync(all)) break;
+        if (!team_sync(all)) return;
     }
-    // A team launched as a cluster reads its CTAs' shared memory: no CTA
-    // leaves before every CTA of the cluster is done.  Every path of the loop
-    // above ends here (its waits are bounded), so every thread arrives.
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 // Host-side launch helpers -------------------------------------------------
@@ -2023,72 +1916,29 @@ cudaError_t launch_extract_path(const BfParams& p, int v, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-// The batched kernel for CTAs of `threads` threads (kBatchThreads), or null.
-static const void* bf_batch_fn(int costIsF32, int timeKind, int threads) {
-    if (threads != kBatchThreads) return nullptr;
+static const void* bf_batch_fn(int costIsF32, int timeKind) {
     if (costIsF32)
         return timeKind == 0 ? (const void*)bf_batch_kernel<float, 0>
-                             : timeKind == 1 ? (const void*)bf_batch_kernel<float, 1>
-                                             : (const void*)bf_batch_kernel<float, 2>;
+                             : timeKind == 1 ? (const void*)bf_batch_kernel<float, 1> : (const void*)bf_batch_kernel<float, 2>;
     return timeKind == 0 ? (const void*)bf_batch_kernel<double, 0>
-                         : timeKind == 1 ? (const void*)bf_batch_kernel<double, 1>
-                                         : (const void*)bf_batch_kernel<double, 2>;
+                         : timeKind == 1 ? (const void*)bf_batch_kernel<double, 1> : (const void*)bf_batch_kernel<double, 2>;
 }
 
 cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamWords, int teamCtas, unsigned spin,
                             int costIsF32, int timeKind, int blocks, int threads, size_t smemBytes,
                             cudaStream_t stream) {
     if (teamCtas < 1 || blocks < teamCtas || blocks % teamCtas != 0) return cudaErrorInvalidValue;
-    const void* fn = bf_batch_fn(costIsF32, timeKind, threads);
-    if (!fn) return cudaErrorInvalidValue;
+    const void* fn = bf_batch_fn(costIsF32, timeKind);
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&jobs, (void*)&count, (void*)&next, (void*)&teamWords, (void*)&teamCtas, (void*)&spin};
     note_launch();
-    if (teamCtas > 1 && teamCtas <= 8) {
-        // a team is a thread-block cluster: its CTAs are co-scheduled and may
-        // read one another's shared memory
-        cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3(blocks);
-        cfg.blockDim = dim3(threads);
-        cfg.dynamicSmemBytes = smemBytes;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = (unsigned)teamCtas;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        return cudaLaunchKernelExC(&cfg, fn, args);
-    }
     if (teamCtas > 1) return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smemBytes, stream);
 }
 
-cudaError_t bf_batch_max_clusters(int costIsF32, int timeKind, int threads, size_t smemBytes, int clusterCtas,
-                                  int* clusters) {
-    const void* fn = bf_batch_fn(costIsF32, timeKind, threads);
-    if (!fn) return cudaErrorInvalidValue;
-    cudaError_t e = allow_max_dynamic_smem(fn);
-    if (e != cudaSuccess) return e;
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)clusterCtas);
-    cfg.blockDim = dim3((unsigned)threads);
-    cfg.dynamicSmemBytes = smemBytes;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)clusterCtas;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaOccupancyMaxActiveClusters(clusters, fn, &cfg);
-}
-
 cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm) {
-    const void* fn = bf_batch_fn(costIsF32, timeKind, threads);
-    if (!fn) return cudaErrorInvalidValue;
+    const void* fn = bf_batch_fn(costIsF32, timeKind);
     const cudaError_t e = allow_max_dynamic_smem(fn);
     if (e != cudaSuccess) return e;
     return max_blocks_per_sm(fn, threads, smemBytes, blocksPerSm);

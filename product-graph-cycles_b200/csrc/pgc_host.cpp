@@ -472,7 +472,6 @@ class Graph {
         int rowCap;         // rows a step buffer holds (0: streams read in place)
         int stageSrcOnly;   // the buffers hold source indices only
         size_t smemBytes;   // dynamic shared memory per CTA
-        int ds = 0, dsCap = 0, dsOffset = 0;  // cluster-resident values (batched teams)
     };
     Run prepare_run(int K, bool ratio);
     // batch mode of prepare_run: a team of up to batchCtas CTAs of
@@ -480,7 +479,6 @@ class Graph {
     // batchSmemCap bytes
     int batchThreads = 0;
     int batchCtas = 1;
-    bool batchDs = false;  // the team is launched as a cluster: its values may live in shared memory
     size_t batchSmemCap = 0;
     void solve_ratio_rescaled(int K);
     void ensure_workspace(int K, int blocks);
@@ -829,30 +827,6 @@ Graph::Run Graph::prepare_run(int K, bool ratio) {
                 need = bf_stage_offset(maxSl);
             }
         }
-        // cluster-resident values: each CTA's own nodes' records ([2][cap][Kp]
-        // doubles) and the slice owner table after the staging area, when
-        // they fit beside the full staging or beside the source indices alone
-        if (batchDs && r.blocks > 1 && r.blocks <= 8 && env_int("PGC_BATCH_DS", 1)) {
-            int ownCap = 0;
-            for (int c = 0; c < r.blocks; ++c)
-                ownCap = std::max(ownCap, std::min(cut[(size_t)c + 1] * 32, T.n) - cut[(size_t)c] * 32);
-            const size_t dsBytes = (size_t)2 * ownCap * r.Kp * sizeof(double) + (size_t)T.nslices;
-            auto at = [](size_t b) { return (b + 31) / 32 * 32; };
-            size_t stage = need;
-            if (at(stage) + dsBytes > batchSmemCap && stageOn && r.rowCap > 0 && !r.stageSrcOnly) {
-                const size_t srcOnly = bf_stage_offset(maxSl) + 2 * bf_stage_buffer_bytes(r.rowCap, 0, 0);
-                if (at(srcOnly) + dsBytes <= batchSmemCap) {
-                    r.stageSrcOnly = 1;
-                    stage = srcOnly;
-                }
-            }
-            if (at(stage) + dsBytes <= batchSmemCap) {
-                r.ds = 1;
-                r.dsCap = ownCap;
-                r.dsOffset = (int)at(stage);
-                need = at(stage) + dsBytes;
-            }
-        }
         if (need > batchSmemCap) throw Failure(PGC_ERR_ARG, "the graph's slice lists exceed the batch's shared memory");
         r.maxCtaSlices = maxSl;
         r.smemBytes = need;
@@ -1039,9 +1013,6 @@ BfParams Graph::params(const Run& r, int mode, int branchId, double lambda, doub
     p.maxCtaSlices = r.maxCtaSlices;
     p.rowCap = r.rowCap;
     p.stageSrcOnly = r.stageSrcOnly;
-    p.ds = r.ds;
-    p.dsCap = r.dsCap;
-    p.dsOffset = r.dsOffset;
     p.lapNext = wLapNext.p;
     p.lapSteps = wLapSteps.p;
     p.walks = wWalks.p;
@@ -1461,7 +1432,6 @@ void Graph::batch_begin(int K, PairJob& J, int threads, int ctas, size_t smemCap
     } phaseTimer{t0, t1, t2};
     batchThreads = threads;
     batchCtas = std::max(1, ctas);
-    batchDs = batchCtas > 1 && batchCtas <= 8;
     batchSmemCap = smemCap;
     Run r;
     try {
@@ -2363,8 +2333,7 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
             const size_t smemCap = (size_t)std::max(0, info.smemOptin / pgc::kBatchBlocksPerSm - 2048);
             // CTAs per team (PGC_BATCH_TEAM, default 8): a team relaxes a
             // graph's steps side by side, so more CTAs per graph shorten each
-            // solve; fewer overlap more graphs' latencies.  Teams of 2-8 CTAs
-            // are launched as thread-block clusters.
+            // solve; fewer overlap more graphs' latencies
             int team = ctas_per_graph > 0 ? ctas_per_graph : pgc::env_int("PGC_BATCH_TEAM", 8);
             team = std::max(1, std::min(team, sms * pgc::kBatchBlocksPerSm));
             const unsigned spin = (unsigned)std::max(1, pgc::env_int("PGC_BF_SPIN_LIMIT", (int)pgc::kDefaultSpinLimit));
@@ -2441,17 +2410,10 @@ int pgc_solve_batch(pgc_graph* const* graphs, int64_t count, const char* solver,
                     int perSm = 0;
                     PGC_CUDA(pgc::bf_batch_max_blocks(cf, tk, threads, smem, &perSm));
                     if (perSm < 1) throw Failure(PGC_ERR_CUDA, "the batched solve kernel cannot be resident");
-                    // whole teams, all resident: clusters of 2-8 CTAs, or a
-                    // cooperative launch for larger teams
+                    // whole teams, all resident (the launch is cooperative
+                    // when a team has more than one CTA)
                     const int g = std::min(team, sms * perSm);
-                    int residentTeams = sms * perSm / g;
-                    if (g > 1 && g <= 8) {
-                        int clusters = 0;
-                        PGC_CUDA(pgc::bf_batch_max_clusters(cf, tk, threads, smem, g, &clusters));
-                        if (clusters < 1) throw Failure(PGC_ERR_CUDA, "no cluster of the batched solve kernel fits");
-                        residentTeams = std::min(residentTeams, clusters);
-                    }
-                    const int teams = (int)std::min<size_t>({k1 - k0, (size_t)residentTeams, maxTeams});
+                    const int teams = (int)std::min<size_t>({k1 - k0, (size_t)(sms * perSm / g), maxTeams});
                     const int blocks = teams * g;
                     PGC_CUDA(cudaMemsetAsync(dTeamWords.p, 0, (size_t)teams * pgc::kTeamWordStride * sizeof(unsigned), bs));
                     g_batchProfile[5] += blocks;
