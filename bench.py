@@ -543,11 +543,13 @@ def _fwdbwd_config(workload, pairs, k, world):
             "l2": "per-pair streams of all pairs exceed L2"}
 
 
-def _batch_pairs(name, seed):
+def _batch_pairs(name, seed, limit=0):
     """The batch's seeded pairs, built in parallel host processes (spawned, before any GPU work)."""
     import multiprocessing as mp
 
     specs = _batch_specs(name, seed)
+    if limit > 0:
+        specs = specs[:limit]  # the batch's first pairs (small profiling cases)
     with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
         pairs = pool.map(_batch_pair, specs, chunksize=4)
     return specs, pairs
@@ -559,7 +561,7 @@ def run_batch(args, world, rank):
     persistent launch in which teams of CTAs run each pair's whole ratio
     solve, largest pairs first).  Also timed: the same pairs solved one after
     the other with full-GPU teams (the plain per-pair GPU Lawler)."""
-    specs, pairs = _batch_pairs(args.workload, args.seed + rank)
+    specs, pairs = _batch_pairs(args.workload, args.seed + rank, args.pairs)
     import numpy as np
     import torch
 
@@ -946,6 +948,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--sub-steps", type=int, default=5, help="timed steps of each configuration under 'configs'")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pairs", type=int, default=0,
+                    help="batched workload: solve only its first N pairs (small profiling cases; 0 = all)")
     args = ap.parse_args()
     world, rank, local = _dist_env()
 
