@@ -892,12 +892,16 @@ def full_metric_line(args, world, rank):
 
     import cyclic_product_graphs as cpg
 
+    # Every GPU timing first, the CPU baselines after them: host-driven steps
+    # measured after the oracle's OpenMP runs (16 threads) were slower than
+    # alone (fwd/bwd: 49 vs 21 ms per step), so the CPU work waits.
     line = measure_pair(args, world, rank, DEFAULT_WORKLOAD, args.steps, args.warmup, args.e2e_steps,
-                        with_min_cost=True, with_cpu=not args.no_cpu_baseline)
+                        with_min_cost=True, with_cpu=False)
     sub_steps, sub_warmup = max(1, min(args.steps, args.sub_steps)), max(3, min(args.warmup, 3))
     configs = {}
     for name in SUB_CONFIGS:
         sub = _sub_args(args, name, sub_steps, sub_warmup)
+        sub.no_cpu_baseline = True
         if name in BATCHES:
             configs[name] = run_batch(sub, world, rank)
         elif name in FWDBWD:
@@ -910,6 +914,13 @@ def full_metric_line(args, world, rank):
         gc.collect()
         cpg.release_cached_memory()
     line["configs"] = configs
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pair, cfg = _make_pair(DEFAULT_WORKLOAD, seed=args.seed + rank)
+        line["cpu_baseline"] = cpu_baseline(pair, cfg)
+        for name in SUB_CONFIGS:
+            if name in BATCHES:
+                specs, pairs = _batch_pairs(name, args.seed + rank)
+                configs[name]["cpu_baseline"] = _batch_cpu_sample(specs, pairs)
     return line
 
 

@@ -754,9 +754,20 @@ __global__ void median_select_kernel(MedianState* st, const double* band, const 
             const int nb = 1 << b;
             for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
             __syncthreads();
-            for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-                const unsigned long long k = order_key(band[i]);
-                if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & (unsigned long long)(nb - 1)], 1ull);
+            // eight loads in flight per thread: one block reads the whole bucket
+            for (long long i0 = threadIdx.x; i0 < n; i0 += 8LL * blockDim.x) {
+                double x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const long long i = i0 + (long long)u * blockDim.x;
+                    x[u] = i < n ? __ldcg(band + i) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (i0 + (long long)u * blockDim.x >= n) break;
+                    const unsigned long long k = order_key(x[u]);
+                    if ((k & mask) == prefix) atomicAdd(&hist[(k >> shift) & (unsigned long long)(nb - 1)], 1ull);
+                }
             }
             __syncthreads();
             int digit;
@@ -793,11 +804,21 @@ __global__ void median_select_kernel(MedianState* st, const double* band, const 
             const long long n = (long long)*count;
             long long less = 0, eq = 0;
             unsigned long long mn = ~0ull;
-            for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-                const unsigned long long k = order_key(band[i]);
-                if (k < key) ++less;
-                else if (k == key) ++eq;
-                else if (k < mn) mn = k;
+            for (long long i0 = threadIdx.x; i0 < n; i0 += 8LL * blockDim.x) {
+                double x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const long long i = i0 + (long long)u * blockDim.x;
+                    x[u] = i < n ? __ldcg(band + i) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (i0 + (long long)u * blockDim.x >= n) break;
+                    const unsigned long long k = order_key(x[u]);
+                    if (k < key) ++less;
+                    else if (k == key) ++eq;
+                    else if (k < mn) mn = k;
+                }
             }
             atomicAdd((unsigned long long*)&sLess, (unsigned long long)less);
             atomicAdd((unsigned long long*)&sEq, (unsigned long long)eq);
