@@ -135,6 +135,13 @@ int pgc_solve_with_minimum_cost(pgc_graph* g, const char* solver_name, int max_d
  * result. */
 int pgc_backward_feat_diff(pgc_graph* g, double grad_objective, double* grad_feat_diff, int accumulate);
 
+/* No reference counterpart.  pgc_backward_feat_diff for `count` distinct
+ * graphs (grad_objectives[i], grad_feat_diffs[i] a device buffer of graph i):
+ * the adjoint kernels are enqueued on the graphs' streams, then each stream
+ * is waited for once. */
+int pgc_backward_feat_diff_batch(pgc_graph* const* graphs, int64_t count, const double* grad_objectives,
+                                 double* const* grad_feat_diffs, int accumulate);
+
 /* No reference counterpart (the oracle's setCostVector).  Sets the edge costs
  * [rows x cols] (rows = nY * edges per layer block, in edge-id order, cols 1
  * or 2) in place of generate(); solves then use (and rescale) them. */
@@ -150,6 +157,11 @@ int pgc_set_feat_diff(pgc_graph* g, const double* feat_diff, int64_t rows, int64
  * The caller orders the buffer's producer before the call (synchronize the
  * producing stream, or give the handle that stream with pgc_set_stream). */
 int pgc_set_feat_diff_device(pgc_graph* g, const double* feat_diff, int64_t rows, int64_t cols);
+
+/* No reference counterpart.  pgc_set_feat_diff_device for `count` distinct
+ * graphs (feat_diffs[i] is graph i's |VX| x |VY| matrix on its device): the
+ * copies are enqueued on the graphs' streams and waited for once each. */
+int pgc_set_feat_diff_device_batch(pgc_graph* const* graphs, int64_t count, const double* const* feat_diffs);
 
 /* No reference counterpart.  Most CTAs one Bellman-Ford launch of this graph
  * may use (0, the default: as many as shorten a step).  A small team is

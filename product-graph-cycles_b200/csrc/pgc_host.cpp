@@ -424,10 +424,12 @@ class Graph {
     long long fdArgmax = 0;   // the first feat_diff entry holding the maximum
     DBuf<long long> wAdjEdges;
     DBuf<double> wImport;
-    void backward_feat_diff(double grad, double* gradFd, bool accumulate);
+    // `wait`: finish the stream before returning (batched callers wait once
+    // for all graphs instead)
+    void backward_feat_diff(double grad, double* gradFd, bool accumulate, bool wait = true);
     void set_cost_vector(const double* in, int64_t rows, int64_t cols);
     void set_feat_diff(const double* fd, int64_t rows, int64_t cols);
-    void set_feat_diff_device(const double* fd, int64_t rows, int64_t cols);
+    void set_feat_diff_device(const double* fd, int64_t rows, int64_t cols, bool wait = true);
     // After set_feat_diff_device the matrix lives only in dFD; the host copy
     // is read back when a host reader needs it (the feature-time maximum, the
     // CSV export).
@@ -1854,7 +1856,7 @@ void Graph::cost_vector_noalloc(double* out) {
 // cycle].  The rescale is taken with its factor fixed and its rounding passed
 // straight through (d c_scaled / d c = product of the factors applied), and
 // the energy's adjoint scatters into feat_diff (plain_energy_backward_kernel).
-void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
+void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate, bool wait) {
     int cm = 0, tm = 0;
     if (conj) {
         // The conjugate energies read feat_diff once per edge, fd[x2, y2]:
@@ -1887,7 +1889,7 @@ void Graph::backward_feat_diff(double grad, double* gradFd, bool accumulate) {
                                                  gradFd, stream));
     }
     stats.launches++;
-    PGC_CUDA(sync_stream());
+    if (wait) PGC_CUDA(sync_stream());
 }
 
 // The edge costs set directly ([rows x cols] in edge-id order), in place of
@@ -1926,12 +1928,12 @@ void Graph::set_feat_diff(const double* fd, int64_t rows, int64_t cols) {
 
 // feat_diff from device memory: one device-to-device copy on the handle's
 // stream, finished before returning (the caller may free its buffer then).
-void Graph::set_feat_diff_device(const double* fd, int64_t rows, int64_t cols) {
+void Graph::set_feat_diff_device(const double* fd, int64_t rows, int64_t cols, bool wait) {
     if (rows != nvx || cols != nvy) throw Failure(PGC_ERR_ARG, "feat_diff must be |VX| x |VY|");
     const size_t n = (size_t)(rows * cols);
     dFD.alloc(n);
     PGC_CUDA(cudaMemcpyAsync(dFD.p, fd, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    PGC_CUDA(sync_stream());
+    if (wait) PGC_CUDA(sync_stream());
     FD.resize(n);
     fdHostStale = true;
     generated = false;
@@ -2220,6 +2222,42 @@ int pgc_backward_feat_diff(pgc_graph* h, double grad_objective, double* grad_fea
         if (!h || !grad_feat_diff) throw Failure(PGC_ERR_ARG, "null argument");
         PGC_CUDA(cudaSetDevice(h->g.device));
         h->g.backward_feat_diff(grad_objective, grad_feat_diff, accumulate != 0);
+    });
+}
+
+int pgc_backward_feat_diff_batch(pgc_graph* const* graphs, int64_t count, const double* grad_objectives,
+                                 double* const* grad_feat_diffs, int accumulate) {
+    return guarded([&] {
+        if (count < 0 || (count > 0 && (!graphs || !grad_objectives || !grad_feat_diffs)))
+            throw Failure(PGC_ERR_ARG, "null argument");
+        for (int64_t i = 0; i < count; ++i)
+            if (!graphs[i] || !grad_feat_diffs[i]) throw Failure(PGC_ERR_ARG, "null handle or output of graph " + std::to_string(i));
+        // every adjoint enqueued on its graph's stream, then one wait per stream
+        for (int64_t i = 0; i < count; ++i) {
+            PGC_CUDA(cudaSetDevice(graphs[i]->g.device));
+            graphs[i]->g.backward_feat_diff(grad_objectives[i], grad_feat_diffs[i], accumulate != 0, false);
+        }
+        for (int64_t i = 0; i < count; ++i) {
+            PGC_CUDA(cudaSetDevice(graphs[i]->g.device));
+            PGC_CUDA(cudaStreamSynchronize(graphs[i]->g.stream));
+        }
+    });
+}
+
+int pgc_set_feat_diff_device_batch(pgc_graph* const* graphs, int64_t count, const double* const* feat_diffs) {
+    return guarded([&] {
+        if (count < 0 || (count > 0 && (!graphs || !feat_diffs))) throw Failure(PGC_ERR_ARG, "null argument");
+        for (int64_t i = 0; i < count; ++i)
+            if (!graphs[i] || !feat_diffs[i]) throw Failure(PGC_ERR_ARG, "null handle or input of graph " + std::to_string(i));
+        for (int64_t i = 0; i < count; ++i) {
+            Graph& g = graphs[i]->g;
+            PGC_CUDA(cudaSetDevice(g.device));
+            g.set_feat_diff_device(feat_diffs[i], g.nvx, g.nvy, false);
+        }
+        for (int64_t i = 0; i < count; ++i) {
+            PGC_CUDA(cudaSetDevice(graphs[i]->g.device));
+            PGC_CUDA(cudaStreamSynchronize(graphs[i]->g.stream));
+        }
     });
 }
 

@@ -26,7 +26,8 @@ import numpy as np
 
 __all__ = ["product_graph_generator", "compute_normals_3d", "compute_normals_2d", "compute_local_thickness_3d",
            "compute_local_thickness_2d", "library_path", "PGCError", "solve_batch", "load_export", "from_export", "autotune", "release_cached_memory",
-           "product_graph_sizes", "vertex_correspondences"]
+           "product_graph_sizes", "vertex_correspondences", "last_batch_profile", "kernel_launches",
+           "set_feat_diffs_device", "backward_feat_diffs"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(os.path.dirname(_PKG), "lib", "libpgc.so")
@@ -76,6 +77,9 @@ def _declare(L):
     L.pgc_set_cost_vector.argtypes = [_h, _dp, _i64, _i64]
     L.pgc_set_feat_diff.argtypes = [_h, _dp, _i64, _i64]
     L.pgc_set_feat_diff_device.argtypes = [_h, ctypes.c_void_p, _i64, _i64]
+    L.pgc_set_feat_diff_device_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.POINTER(ctypes.c_void_p)]
+    L.pgc_backward_feat_diff_batch.argtypes = [ctypes.POINTER(_h), _i64, _dp, ctypes.POINTER(ctypes.c_void_p),
+                                               ctypes.c_int]
     L.pgc_solve_batch.argtypes = [ctypes.POINTER(_h), _i64, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.pgc_device_name.argtypes = [_h, ctypes.c_char_p, _i64]
@@ -467,6 +471,32 @@ def solve_batch(generators, solver_name: str, max_depth: int | None = None, ctas
     _check(_lib.pgc_solve_batch(arr, len(gens), str(solver_name).encode(), -1 if max_depth is None else int(max_depth),
                                 int(ctas_per_graph), int(workers), int(bool(regenerate)), status))
     return [g._result() for g in gens]
+
+
+def set_feat_diffs_device(generators, pointers):
+    """``set_feat_diff_device`` for many distinct generators at once (no
+    counterpart in the reference): pointers[i] addresses generator i's
+    |VX| x |VY| float64 matrix on its GPU, already written.  The copies are
+    enqueued together and waited for once per generator."""
+    gens = list(generators)
+    if len(set(id(g) for g in gens)) != len(gens):
+        raise ValueError("set_feat_diffs_device needs distinct generators")
+    arr = (_h * len(gens))(*[g._h for g in gens])
+    ptrs = (ctypes.c_void_p * len(gens))(*[int(p) for p in pointers])
+    _check(_lib.pgc_set_feat_diff_device_batch(arr, len(gens), ptrs))
+
+
+def backward_feat_diffs(generators, grad_objectives, grad_pointers, accumulate: bool = False):
+    """``backward_feat_diff`` for many distinct generators at once (no
+    counterpart in the reference): the adjoint kernels are enqueued together,
+    then every generator's stream is waited for once."""
+    gens = list(generators)
+    if len(set(id(g) for g in gens)) != len(gens):
+        raise ValueError("backward_feat_diffs needs distinct generators")
+    arr = (_h * len(gens))(*[g._h for g in gens])
+    grads = (ctypes.c_double * len(gens))(*[float(x) for x in grad_objectives])
+    ptrs = (ctypes.c_void_p * len(gens))(*[int(p) for p in grad_pointers])
+    _check(_lib.pgc_backward_feat_diff_batch(arr, len(gens), grads, ptrs, int(bool(accumulate))))
 
 
 def last_batch_profile() -> dict:

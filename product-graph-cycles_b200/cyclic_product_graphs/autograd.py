@@ -23,7 +23,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import solve_batch
+from . import backward_feat_diffs, set_feat_diffs_device, solve_batch
 
 
 def _as_host(fd: torch.Tensor) -> np.ndarray:
@@ -94,10 +94,15 @@ class MinCostCycleObjective(torch.autograd.Function):
 class _BatchedRatio(torch.autograd.Function):
     @staticmethod
     def forward(ctx, gens, max_depth, *feat_diffs):
-        if any(fd.is_cuda for fd in feat_diffs):
-            torch.cuda.synchronize()  # every producer, once
-        for g, fd in zip(gens, feat_diffs):
-            _set_feat_diff(g, fd, synced=True)
+        if all(fd.is_cuda for fd in feat_diffs):
+            # every producer once, then one batched device-to-device copy
+            srcs = [fd.detach().to(dtype=torch.float64).contiguous() for fd in feat_diffs]
+            torch.cuda.synchronize()
+            set_feat_diffs_device(gens, [s.data_ptr() for s in srcs])
+            del srcs
+        else:
+            for g, fd in zip(gens, feat_diffs):
+                _set_feat_diff(g, fd)
         results = solve_batch(gens, "lawlergpu", max_depth)
         ctx.gens = gens
         ctx.save_for_backward(*feat_diffs)
@@ -109,7 +114,14 @@ class _BatchedRatio(torch.autograd.Function):
         fds = ctx.saved_tensors
         torch.cuda.synchronize()
         go = grad_out.detach().cpu()
-        return (None, None) + tuple(_adjoint(g, go[i], fd, synced=True) for i, (g, fd) in enumerate(zip(ctx.gens, fds)))
+        if not all(fd.is_cuda for fd in fds):
+            return (None, None) + tuple(_adjoint(g, go[i], fd, synced=True)
+                                        for i, (g, fd) in enumerate(zip(ctx.gens, fds)))
+        # every adjoint enqueued at once, one wait per graph
+        grads = [torch.empty(fd.shape, dtype=torch.float64, device=fd.device) for fd in fds]
+        torch.cuda.synchronize()  # the buffers exist before the library's streams write them
+        backward_feat_diffs(ctx.gens, [float(x) for x in go], [g.data_ptr() for g in grads])
+        return (None, None) + tuple(g.to(dtype=fd.dtype) for g, fd in zip(grads, fds))
 
 
 def ratio_cycle_objectives(gens, feat_diffs, max_depth=None) -> torch.Tensor:
