@@ -12,7 +12,9 @@
 // arithmetic modes are therefore bit-identical to the CPU formulas.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <set>
@@ -1230,8 +1232,17 @@ cudaError_t launch_normals_2d(const double* Vin, int nv, const int* E, double* V
 // (one full wave; a partial second wave would double the pass).
 // The grid is cached per (kernel, device, block, shared memory): the
 // occupancy query is not free and every pass of every solve asks it.
+// PGC_STREAM_GRID (measurement) caps it, so that the passes of many small
+// graphs on concurrent streams can share the device.
+static int stream_grid_cap() {
+    static const int cap = [] {
+        const char* v = std::getenv("PGC_STREAM_GRID");
+        return v ? std::max(0, std::atoi(v)) : 0;
+    }();
+    return cap;
+}
 template <class K>
-static int stream_grid(K kernel, int threads, size_t smem) {
+static int stream_grid_full(K kernel, int threads, size_t smem) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
@@ -1256,6 +1267,13 @@ static int stream_grid(K kernel, int threads, size_t smem) {
     std::lock_guard<std::mutex> lk(mu);
     cache[key] = grid;
     return grid;
+}
+
+template <class K>
+static int stream_grid(K kernel, int threads, size_t smem) {
+    const int g = stream_grid_full(kernel, threads, smem);
+    const int cap = stream_grid_cap();
+    return cap > 0 && cap < g ? cap : g;
 }
 
 static int grid_for(long long total, int threads) {

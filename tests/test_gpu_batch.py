@@ -119,3 +119,26 @@ def test_batch_adjoint_after_device_solves(cpg, oracle):
         buf = torch.zeros(gb.shape, dtype=torch.float64, device="cuda")
         g.backward_feat_diff(1.0, buf.data_ptr())
         assert np.array_equal(buf.cpu().numpy(), gb)
+
+
+def test_launch_counter_and_batch_profile(cpg, oracle):
+    """kernel_launches() counts the library's launches (the bench's
+    gpu_launches); last_batch_profile() describes the last batched call."""
+    pairs = [synthetic.make_pair(n_vertices=200 + 40 * i, n_curve=8, feat_dim=8, seed=60 + i) for i in range(3)]
+    gens = []
+    for p in pairs:
+        g = cpg.product_graph_generator(p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], False, False)
+        g.set_cost_time_ratio_mode("vanilla", "nomode")
+        gens.append(g)
+    n0 = cpg.kernel_launches()
+    cpg.solve_batch(gens, "lawlergpu", 2, regenerate=True)
+    n1 = cpg.kernel_launches()
+    # per graph at least the energy kernel and the median chain, plus the batched launch
+    assert n1 - n0 >= 3 * 2 + 1
+    prof = cpg.last_batch_profile()
+    assert prof["solved_on_device"] + prof["handed_back"] == 3
+    assert prof["ctas"] >= 1 and prof["threads_per_cta"] == 256
+    assert prof["launch_ms"] > 0 and prof["prepare_ms"] > 0
+    # a single solve launches too, and the counter only grows
+    gens[0].solve_with_cost_time_ratio("lawlergpu", 2)
+    assert cpg.kernel_launches() > n1
