@@ -194,7 +194,7 @@ struct MedianState {
     unsigned long long prefix, mask;
     long long rank, bucket;
     int shift, bits, done, even;
-    int err;                     // 1-3: the selection lost its rank
+    int err;                     // 1-4: the selection lost its rank; 5: it needs more digit passes
     int needAbove;               // even count, rank the bucket's largest: xk1 is the smallest key above it
     unsigned long long bucketTop, minAbove;
     double xk, xk1, median, factor;
@@ -339,9 +339,11 @@ cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s);
 // Median of a column and its rescale (cost_time_ratio_solver.cpp:709-721),
 // enqueued whole on stream s (kernels_energy.cu).
+// allPasses: every digit pass that 64 key bits can need (else the first two;
+// a column that needs more comes back with err 5).
 cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHist, MedianState* st,
                                   unsigned long long* hist, double* band, unsigned long long* count, long long nValues,
-                                  double scaling, float* col32, double clip, cudaStream_t s);
+                                  double scaling, float* col32, double clip, bool allPasses, cudaStream_t s);
 cudaError_t launch_rescale_f64(const SelectArgs& a, MedianState* st, double clip, cudaStream_t s);
 cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
                           const int* ti, const int* tr, cudaStream_t s);

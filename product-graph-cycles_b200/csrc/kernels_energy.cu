@@ -576,7 +576,7 @@ __device__ __forceinline__ int median_digit_bits(int shift) {
     return b < shift ? b : shift;
 }
 
-__global__ void median_init_kernel(MedianState* st, long long count) {
+__device__ __forceinline__ MedianState median_start(long long count) {
     MedianState m{};
     m.even = count % 2 == 0;
     m.rank = m.even ? (count - 2) / 2 : count / 2;
@@ -584,8 +584,10 @@ __global__ void median_init_kernel(MedianState* st, long long count) {
     m.shift = 64;
     m.bits = median_digit_bits(64);
     m.minAbove = ~0ull;
-    *st = m;
+    return m;
 }
+
+__global__ void median_init_kernel(MedianState* st, long long count) { *st = median_start(count); }
 
 // Histogram of the next digit of the keys that match the state's prefix.
 // A grid of one wave (occupancy-sized) keeps the final flush of the block
@@ -669,9 +671,11 @@ __device__ bool find_digit(const unsigned long long* hist, int nb, long long ran
 // The digit holding the wanted rank from the last pass's histogram: the
 // prefix grows by it, the rank becomes the rank inside its bucket.  The
 // histogram is cleared for the next pass.  One block of 1024 threads.
-__global__ void median_scan_kernel(unsigned long long* hist, MedianState* st) {
+// init >= 0: the state starts here, for a column of `init` values (the first
+// digit's histogram was counted before, by the energy kernel).
+__global__ void median_scan_kernel(unsigned long long* hist, MedianState* st, long long init) {
     __shared__ MedianState m;
-    if (threadIdx.x == 0) m = *st;
+    if (threadIdx.x == 0) m = init >= 0 ? median_start(init) : *st;
     __syncthreads();
     if (m.done) return;
     if (m.bits < 1 || m.bits > kMedianWideBits || m.bits > m.shift) {
@@ -706,11 +710,18 @@ __global__ void median_scan_kernel(unsigned long long* hist, MedianState* st) {
 
 // Copies the last bucket's values (keys matching the prefix) to out[0..cap);
 // nothing when every bit is fixed (the bucket's values are all equal).
-__global__ void median_compact_kernel(SelectArgs a, const MedianState* st, double* out, unsigned long long* count,
+// A selection that is not done after the passes enqueued (a column of few
+// distinct values) is flagged (err 5) for the host, which runs the chain
+// again with every pass.
+__global__ void median_compact_kernel(SelectArgs a, MedianState* st, double* out, unsigned long long* count,
                                       long long cap) {
     __shared__ MedianState m;
     if (threadIdx.x == 0) m = *st;
     __syncthreads();
+    if (!m.done && !m.err) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->err = 5;
+        return;
+    }
     if (m.shift == 0 || m.err) return;
     const unsigned long long prefix = m.prefix, mask = m.mask;
     for_stream_values<4>(a.col, a.layerStride, a.interEntries, a.nY, a.tedgeInter, a.tedgeIntra,
@@ -862,17 +873,11 @@ __global__ void median_min_above_kernel(SelectArgs a, MedianState* st) {
 // median = xk (odd count) or (xk + xk1) / 2; factor = scaling / (2
 // max(median, 0.001)), the host driver's double operations
 // (cost_time_ratio_solver.cpp:709-721, utils.hpp:196-209).
-__global__ void median_finish_kernel(MedianState* st, double scaling) {
-    MedianState m = *st;
-    if (m.err) {
-        st->factor = __longlong_as_double(0x7ff8000000000000LL);
-        return;
-    }
+__device__ __forceinline__ double median_factor(const MedianState& m, double scaling, double* median) {
     const double xk1 = m.needAbove ? key_to_double(m.minAbove) : m.xk1;
-    const double median = m.even ? __ddiv_rn(__dadd_rn(m.xk, xk1), 2.0) : m.xk;
-    const double med = median < 0.001 ? 0.001 : median;
-    st->median = median;
-    st->factor = __ddiv_rn(scaling, __dmul_rn(2.0, med));
+    *median = m.even ? __ddiv_rn(__dadd_rn(m.xk, xk1), 2.0) : m.xk;
+    const double med = *median < 0.001 ? 0.001 : *median;
+    return __ddiv_rn(scaling, __dmul_rn(2.0, med));
 }
 
 // x <- min(round(factor * x), clip) on the valid entries, factor from the
@@ -880,10 +885,29 @@ __global__ void median_finish_kernel(MedianState* st, double scaling) {
 // when writeF64 (the host first runs without it and keeps the float copy as
 // the rescaled column when every value is exact); sets st->inexact when a
 // value is not a float.
+// The factor comes from the selection (the first pass, writeF64 == 0, also
+// stores it and the median in the state) or, for the second pass, from the
+// state; nothing is written when the selection failed.
 __global__ void rescale_kernel(double* col, float* col32, long long layerStride, long long interEntries, int nY,
-                               const int* tedgeInter, const int* tedgeIntra, MedianState* st, double clip,
-                               int writeF64) {
-    const double factor = st->factor;
+                               const int* tedgeInter, const int* tedgeIntra, MedianState* st, double scaling,
+                               double clip, int writeF64) {
+    __shared__ double sFactor;
+    __shared__ int sErr;
+    if (threadIdx.x == 0) {
+        const MedianState m = *st;
+        sErr = m.err;
+        if (!m.err) {
+            double median;
+            sFactor = writeF64 ? m.factor : median_factor(m, scaling, &median);
+            if (!writeF64 && blockIdx.x == 0) {
+                st->median = median;
+                st->factor = sFactor;
+            }
+        }
+    }
+    __syncthreads();
+    if (sErr) return;
+    const double factor = sFactor;
     int* inexact = &st->inexact;
     for_stream_values<4>(col, layerStride, interEntries, nY, tedgeInter, tedgeIntra,
                          [&](long long idx, double v, bool valid, bool inRange) {
@@ -1307,7 +1331,7 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
 // zeroed counters; band: kMedianCompact doubles; count: one zeroed counter.
 cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHist, MedianState* st,
                                   unsigned long long* hist, double* band, unsigned long long* count, long long nValues,
-                                  double scaling, float* col32, double clip, cudaStream_t s) {
+                                  double scaling, float* col32, double clip, bool allPasses, cudaStream_t s) {
     const size_t smem = sizeof(unsigned) << kMedianWideBits;
     {
         static std::mutex mu;
@@ -1327,24 +1351,27 @@ cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHi
     const int grid = stream_grid(median_compact_kernel, 256, 0);
     SelectArgs h = a;
     h.hist = hist;
-    note_launch();
-    median_init_kernel<<<1, 1, 0, s>>>(st, nValues);
     if (topHist) {
         note_launch();
-        median_scan_kernel<<<1, 1024, 0, s>>>(topHist, st);
+        median_scan_kernel<<<1, 1024, 0, s>>>(topHist, st, nValues);
     } else {
         note_launch();
+        median_init_kernel<<<1, 1, 0, s>>>(st, nValues);
+        note_launch();
         median_hist_kernel<<<histGrid, 512, smem, s>>>(h, st);
         note_launch();
-        median_scan_kernel<<<1, 1024, 0, s>>>(hist, st);
+        median_scan_kernel<<<1, 1024, 0, s>>>(hist, st, -1);
     }
-    // at most five more digits fix all 64 bits (12 + 14 + 12 + 12 + 12 + 2);
-    // the passes after the selection is done return at once
-    for (int pass = 0; pass < 5; ++pass) {
+    // One more digit (14 bits) leaves a bucket of at most kMedianCompact
+    // values on every column but those of few distinct values; for those the
+    // compaction flags the state and the host runs the chain with all
+    // passes: at most five more digits fix all 64 bits (12 + 14 + 12 + 12 +
+    // 12 + 2), and the passes after the selection is done return at once.
+    for (int pass = 0; pass < (allPasses ? 5 : 1); ++pass) {
         note_launch();
         median_hist_kernel<<<histGrid, 512, smem, s>>>(h, st);
         note_launch();
-        median_scan_kernel<<<1, 1024, 0, s>>>(hist, st);
+        median_scan_kernel<<<1, 1024, 0, s>>>(hist, st, -1);
     }
     note_launch();
     median_compact_kernel<<<grid, 256, 0, s>>>(a, st, band, count, kMedianCompact);
@@ -1353,10 +1380,8 @@ cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHi
     note_launch();
     median_min_above_kernel<<<grid, 256, 0, s>>>(a, st);
     note_launch();
-    median_finish_kernel<<<1, 1, 0, s>>>(st, scaling);
-    note_launch();
     rescale_kernel<<<grid, 256, 0, s>>>(const_cast<double*>(a.col), col32, a.layerStride, a.interEntries, a.nY,
-                                        a.tedgeInter, a.tedgeIntra, st, clip, 0);
+                                        a.tedgeInter, a.tedgeIntra, st, scaling, clip, 0);
     return cudaGetLastError();
 }
 
@@ -1366,7 +1391,7 @@ cudaError_t launch_rescale_f64(const SelectArgs& a, MedianState* st, double clip
     note_launch();
     rescale_kernel<<<stream_grid(rescale_kernel, 256, 0), 256, 0, s>>>(const_cast<double*>(a.col), nullptr,
                                                                         a.layerStride, a.interEntries, a.nY,
-                                                                        a.tedgeInter, a.tedgeIntra, st, clip, 1);
+                                                                        a.tedgeInter, a.tedgeIntra, st, 0.0, clip, 1);
     return cudaGetLastError();
 }
 cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,

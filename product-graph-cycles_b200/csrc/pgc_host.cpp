@@ -696,18 +696,34 @@ void Graph::rescale_columns(double scaling) {
         a.tedgeIntra = dTedge[INTRA].p;
         return a;
     };
+    auto enqueue = [&](int col, bool allPasses) {
+        PGC_CUDA(cudaMemsetAsync(wMedCount.p, 0, sizeof(unsigned long long), stream));
+        const bool top = topHistValid[col] && !allPasses;
+        PGC_CUDA(launch_median_rescale(args(col), top ? topHist[col].p : nullptr, wMedState.p + col, wMedHist.p,
+                                       wMedBand.p, wMedCount.p, count, scaling, e32[col].p, 100 * scaling, allPasses,
+                                       stream));
+        stats.launches += (top ? 1 : 3) + (allPasses ? 10 : 2) + 4;
+    };
     for (int col = 0; col < ncols; ++col) {
         ensure_e64(col);
         e32[col].alloc((size_t)total);
-        PGC_CUDA(cudaMemsetAsync(wMedCount.p, 0, sizeof(unsigned long long), stream));
-        PGC_CUDA(launch_median_rescale(args(col), topHistValid[col] ? topHist[col].p : nullptr, wMedState.p + col,
-                                       wMedHist.p, wMedBand.p, wMedCount.p, count, scaling, e32[col].p, 100 * scaling,
-                                       stream));
-        stats.launches += topHistValid[col] ? 17 : 18;
+        enqueue(col, false);
     }
     MedianState st[2];
     d2h(st, wMedState.p, sizeof(MedianState) * (size_t)ncols);
     PGC_CUDA(sync_stream());
+    // a column of few distinct values needs more digit passes: its chain
+    // again with every pass (its float copy was not written)
+    bool again = false;
+    for (int col = 0; col < ncols; ++col) {
+        if (st[col].err != 5) continue;
+        enqueue(col, true);
+        again = true;
+    }
+    if (again) {
+        d2h(st, wMedState.p, sizeof(MedianState) * (size_t)ncols);
+        PGC_CUDA(sync_stream());
+    }
     bool rewrite = false;
     for (int col = 0; col < ncols; ++col) {
         if (st[col].err) throw Failure(PGC_ERR_INTERNAL, "median selection lost its rank");

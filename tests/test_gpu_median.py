@@ -37,13 +37,20 @@ KINDS = ["equal", "few", "split", "signed", "tiny", "spread"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
-@pytest.mark.parametrize("conj,odd", [(False, False), (True, False), (False, True)])
-def test_rescale_selection_paths_match_oracle(cpg, oracle, kind, conj, odd):
+@pytest.mark.parametrize("conj,odd,large", [(False, False, False), (True, False, False), (False, True, False),
+                                            (False, False, True)])
+def test_rescale_selection_paths_match_oracle(cpg, oracle, kind, conj, odd, large):
     # an icosphere with six curve points gives an even count of costs (the
     # median is the mean of the two middle values); a 101-vertex mesh with five
-    # curve points an odd one
-    p = synthetic.make_pair(n_vertices=101, n_curve=5, feat_dim=4, seed=31) if odd else \
-        synthetic.make_pair(icosphere_level=1, n_curve=6, feat_dim=4, seed=31)
+    # curve points an odd one; a 2,000-vertex mesh with 40 curve points over
+    # half a million, so that columns of few distinct values need every digit
+    # pass (their buckets stay above the compaction's 65,536 values)
+    if large:
+        p = synthetic.make_pair(n_vertices=2000, n_curve=40, feat_dim=4, seed=31)
+    elif odd:
+        p = synthetic.make_pair(n_vertices=101, n_curve=5, feat_dim=4, seed=31)
+    else:
+        p = synthetic.make_pair(icosphere_level=1, n_curve=6, feat_dim=4, seed=31)
     args = (p["VX"], p["EX"], p["VY"], p["EY"], p["feat_diff"], conj, False, False)
     g, o = cpg.product_graph_generator(*args), oracle.OracleGenerator(*args)
     if conj:
@@ -51,6 +58,7 @@ def test_rescale_selection_paths_match_oracle(cpg, oracle, kind, conj, odd):
             x.set_normals(p["NX"], p["NY"])
     rows = o.get_cost_vector().shape[0]
     assert rows % 2 == (1 if odd else 0)
+    assert not large or rows > 4 * 65536
     rng = np.random.default_rng(KINDS.index(kind))
     cost = _column(kind, rows, rng)
     time = _column("spread" if kind == "equal" else kind, rows, rng)
