@@ -398,7 +398,11 @@ __device__ __forceinline__ double edge_weight(const StepView& v, int q) {
 // One batch of exactly NR rows starting at `row`: every source value is
 // gathered first, then the batch is folded in edge order.  `win` records the
 // position of the last improvement (row * 8 + depth); thr is its value.
-template <class CT, int TK, bool S, int NK, int NR>
+// TREE: the batch's candidates are reduced as a balanced tree of (value,
+// position) minima instead of one sequential compare chain (the batched
+// kernel, whose register budget holds the extra live values; the
+// single-graph kernel's 96-register budget does not).
+template <class CT, int TK, bool S, int NK, int NR, bool TREE>
 __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row, double& thr, int& win) {
     int sv[NR];
     double d[NR][NK];
@@ -412,14 +416,53 @@ __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row,
             for (int kk = 0; kk < NK; ++kk) d[r][kk] = kInfD;
         }
     }
+    if constexpr (!TREE) {
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-        if (sv[r] < 0) continue;
-        const double w = edge_weight<CT, TK>(v, (row + r) * 32 + lane);
+        for (int r = 0; r < NR; ++r) {
+            if (sv[r] < 0) continue;
+            const double w = edge_weight<CT, TK>(v, (row + r) * 32 + lane);
 #pragma unroll
-        for (int kk = 0; kk < NK; ++kk) {
-            const double cand = __dadd_rn(d[r][kk], w);
-            if (cand < thr) { thr = cand; win = ((row + r) << 3) | kk; }
+            for (int kk = 0; kk < NK; ++kk) {
+                const double cand = __dadd_rn(d[r][kk], w);
+                if (cand < thr) { thr = cand; win = ((row + r) << 3) | kk; }
+            }
+        }
+    } else {
+        // The candidates in edge order (row, then depth), reduced so that
+        // the left -- earlier -- candidate wins ties: the first minimum,
+        // which is what the sequential scan `cand < thr` ends with.  A NaN
+        // candidate, which that scan never takes, enters as +inf; neither
+        // is ever below thr.
+        constexpr int N = NR * NK;
+        double cv[N];
+        int ci[N];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const double w = sv[r] >= 0 ? edge_weight<CT, TK>(v, (row + r) * 32 + lane) : 0.0;
+#pragma unroll
+            for (int kk = 0; kk < NK; ++kk) {
+                double c = kInfD;
+                if (sv[r] >= 0) {
+                    c = __dadd_rn(d[r][kk], w);
+                    if (c != c) c = kInfD;
+                }
+                cv[r * NK + kk] = c;
+                ci[r * NK + kk] = r * NK + kk;
+            }
+        }
+#pragma unroll
+        for (int s = 1; s < N; s <<= 1) {
+#pragma unroll
+            for (int i = 0; i + s < N; i += 2 * s) {
+                if (cv[i + s] < cv[i]) {
+                    cv[i] = cv[i + s];
+                    ci[i] = ci[i + s];
+                }
+            }
+        }
+        if (cv[0] < thr) {
+            thr = cv[0];
+            win = ((row + ci[0] / NK) << 3) | (ci[0] % NK);
         }
     }
 }
@@ -427,26 +470,26 @@ __device__ __forceinline__ void fold_batch(const StepView& v, int lane, int row,
 // The last nr (1 <= nr <= NR) rows as one batch of exactly nr rows.  The row
 // count is the slice's, the same in every lane, so no lane runs row slots
 // that do not exist.
-template <class CT, int TK, bool S, int NK, int NR>
+template <class CT, int TK, bool S, int NK, int NR, bool TREE>
 __device__ __forceinline__ void fold_tail(const StepView& v, int lane, int row, int nr, double& thr, int& win) {
     if constexpr (NR <= 1) {
-        fold_batch<CT, TK, S, NK, 1>(v, lane, row, thr, win);
+        fold_batch<CT, TK, S, NK, 1, TREE>(v, lane, row, thr, win);
     } else {
-        if (nr == NR) fold_batch<CT, TK, S, NK, NR>(v, lane, row, thr, win);
-        else fold_tail<CT, TK, S, NK, NR - 1>(v, lane, row, nr, thr, win);
+        if (nr == NR) fold_batch<CT, TK, S, NK, NR, TREE>(v, lane, row, thr, win);
+        else fold_tail<CT, TK, S, NK, NR - 1, TREE>(v, lane, row, nr, thr, win);
     }
 }
 
 // Rows [row, j1) of one slice for lane `lane`.  Returns the position of the
 // winning candidate -- row * 8 + depth for NK > 0, row * nk + depth for the
 // run-time depth count (NK == 0) -- or -1; thr holds its value.
-template <class CT, int TK, bool S, int NK>
+template <class CT, int TK, bool S, int NK, bool TREE>
 __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, int j1, double& thr) {
     int win = -1;
     if constexpr (NK > 0) {
         constexpr int RB = bf_rows_per_batch(NK);
-        for (; j1 - row >= RB; row += RB) fold_batch<CT, TK, S, NK, RB>(v, lane, row, thr, win);
-        if (row < j1) fold_tail<CT, TK, S, NK, RB>(v, lane, row, j1 - row, thr, win);
+        for (; j1 - row >= RB; row += RB) fold_batch<CT, TK, S, NK, RB, TREE>(v, lane, row, thr, win);
+        if (row < j1) fold_tail<CT, TK, S, NK, RB, TREE>(v, lane, row, j1 - row, thr, win);
     } else {
         for (; row < j1; ++row) {
             const int sv = v.src[row * 32 + lane];
@@ -462,7 +505,7 @@ __device__ __forceinline__ int fold_rows(const StepView& v, int lane, int row, i
     return win;
 }
 
-template <class CT, int TK, bool S, int NK>
+template <class CT, int TK, bool S, int NK, bool TREE>
 __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* spl, const int* act, int nAct, int s0,
                              int s1, int l, int k) {
     const int n = p.n, K = p.K, Kp = p.Kp;
@@ -492,7 +535,7 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
         double best = (l == 0 && valid) ? ldV<S>(p, me) : kInfD;
         double thr = best < ub ? best : ub;
         int win = -1;
-        if (!empty) win = fold_rows<CT, TK, S, NK>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, thr);
+        if (!empty) win = fold_rows<CT, TK, S, NK, TREE>(sv, lane, spl[s - s0] - r0, spl[s + 1 - s0] - r0, thr);
         if (!valid) continue;
         int o = kLapUnknown, h = 0;
         int bs = -1, bk = -1;
@@ -537,7 +580,7 @@ __device__ bool relax_slices(const BfParams& p, const StepView& sv, const int* s
     return any;
 }
 
-template <class CT, int TK, bool S>
+template <class CT, int TK, bool S, bool TREE>
 __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, int s1, int l, int k) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const bool inter = (k == 0);
@@ -569,13 +612,13 @@ __device__ bool relax_step(const BfParams& p, const Stage& st, int sb, int s0, i
     v.tconst = p.tconst;
     const int* act = st.act(part);
     const int na = st.nAct(part);
-    if (!inter) return relax_slices<CT, TK, S, 1>(p, v, spl, act, na, s0, s1, l, k);
+    if (!inter) return relax_slices<CT, TK, S, 1, TREE>(p, v, spl, act, na, s0, s1, l, k);
     switch (K) {
-        case 1: return relax_slices<CT, TK, S, 1>(p, v, spl, act, na, s0, s1, l, k);
-        case 2: return relax_slices<CT, TK, S, 2>(p, v, spl, act, na, s0, s1, l, k);
-        case 3: return relax_slices<CT, TK, S, 3>(p, v, spl, act, na, s0, s1, l, k);
-        case 4: return relax_slices<CT, TK, S, 4>(p, v, spl, act, na, s0, s1, l, k);
-        default: return relax_slices<CT, TK, S, 0>(p, v, spl, act, na, s0, s1, l, k);
+        case 1: return relax_slices<CT, TK, S, 1, TREE>(p, v, spl, act, na, s0, s1, l, k);
+        case 2: return relax_slices<CT, TK, S, 2, TREE>(p, v, spl, act, na, s0, s1, l, k);
+        case 3: return relax_slices<CT, TK, S, 3, TREE>(p, v, spl, act, na, s0, s1, l, k);
+        case 4: return relax_slices<CT, TK, S, 4, TREE>(p, v, spl, act, na, s0, s1, l, k);
+        default: return relax_slices<CT, TK, S, 0, TREE>(p, v, spl, act, na, s0, s1, l, k);
     }
 }
 
@@ -872,7 +915,7 @@ __device__ int dij_walk_end(const BfParams& p, int v) {
 // the dynamic shared memory after the DP tables: [row offsets and lists of
 // slices with rows][two step buffers].
 // ---------------------------------------------------------------------------
-template <class CT, int TK, bool S>
+template <class CT, int TK, bool S, bool TREE = false>
 __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* smem) {
     const int n = p.n, K = p.K, Kp = p.Kp;
     const long long tid = t.thread(), nth = t.nthreads();
@@ -1023,7 +1066,7 @@ __device__ __forceinline__ void bf_body(const BfParams& p, const Team& t, char* 
                 if (isLead) cycStage += clock64() - ta;
                 const bool last = l == p.nY && k == kSteps - 1;
                 if (!last) stage_issue(p, st, s0, s1, sb ^ 1, k + 1 < kSteps ? l : l + 1, k + 1 < kSteps ? k + 1 : 0);
-                const bool any = relax_step<CT, TK, S>(p, st, sb, s0, s1, l, k);
+                const bool any = relax_step<CT, TK, S, TREE>(p, st, sb, s0, s1, l, k);
                 if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) p.layerFlag[l] = stamp;
                 const unsigned long long tb = isLead ? clock64() : 0;
                 ++step;
@@ -1526,7 +1569,7 @@ enum Outcome { OUT_FOUND = 0, OUT_NONE = 1, OUT_ZERO = 2 };
 
 template <class CT, int TK>
 __device__ __noinline__ void bf_call(const BfParams& P, const Team& t, char* smem) {
-    bf_body<CT, TK, false>(P, t, smem);
+    bf_body<CT, TK, false, true>(P, t, smem);
 }
 
 // One Bellman-Ford call of the team: the lead publishes the call's state,
