@@ -1340,9 +1340,16 @@ static int stream_grid_full(K kernel, int threads, size_t smem) {
     return grid;
 }
 
+// `work`: the stream entries the pass visits.  A small column gets one CTA
+// per 128 entries a thread, fewer than a full wave, so that the passes of
+// many small graphs on concurrent streams share the device.
 template <class K>
-static int stream_grid(K kernel, int threads, size_t smem) {
-    const int g = stream_grid_full(kernel, threads, smem);
+static int stream_grid(K kernel, int threads, size_t smem, long long work = -1) {
+    int g = stream_grid_full(kernel, threads, smem);
+    if (work >= 0) {
+        const long long want = std::max(1LL, work / ((long long)threads * 128));
+        if (want < g) g = (int)want;
+    }
     const int cap = stream_grid_cap();
     return cap > 0 && cap < g ? cap : g;
 }
@@ -1357,7 +1364,7 @@ static int grid_for(long long total, int threads) {
 cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s) {
     const size_t smem = a.hist0 ? 2 * kTopBins * sizeof(unsigned) : 0;
     note_launch();
-    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, smem), 256, smem, s>>>(a);
+    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, smem, a.total), 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
@@ -1394,8 +1401,8 @@ cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHi
             done.insert(dev);
         }
     }
-    const int histGrid = stream_grid(median_hist_kernel, 512, smem);
-    const int grid = stream_grid(median_compact_kernel, 256, 0);
+    const int histGrid = stream_grid(median_hist_kernel, 512, smem, a.total);
+    const int grid = stream_grid(median_compact_kernel, 256, 0, a.total);
     SelectArgs h = a;
     h.hist = hist;
     if (topHist) {
