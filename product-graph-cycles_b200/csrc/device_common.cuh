@@ -334,7 +334,9 @@ cudaError_t launch_bf_batch(PairJob* jobs, int count, int* next, unsigned* teamW
                             cudaStream_t stream);
 cudaError_t bf_batch_max_blocks(int costIsF32, int timeKind, int threads, size_t smemBytes, int* blocksPerSm);
 cudaError_t launch_lookup_pairs(const LookupArgs& a, cudaStream_t stream);
-cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s);
+// shared: many graphs' passes run side by side (batched solves): a small
+// column's pass takes a grid proportional to its entries
+cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s, bool shared = false);
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s);
 cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s);
 // Median of a column and its rescale (cost_time_ratio_solver.cpp:709-721),
@@ -343,7 +345,8 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s);
 // a column that needs more comes back with err 5).
 cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHist, MedianState* st,
                                   unsigned long long* hist, double* band, unsigned long long* count, long long nValues,
-                                  double scaling, float* col32, double clip, bool allPasses, cudaStream_t s);
+                                  double scaling, float* col32, double clip, bool allPasses, bool shared,
+                                  cudaStream_t s);
 cudaError_t launch_rescale_f64(const SelectArgs& a, MedianState* st, double clip, cudaStream_t s);
 cudaError_t launch_to_f64(const float* col32, double* col, long long layerStride, long long interEntries, int nY,
                           const int* ti, const int* tr, cudaStream_t s);

@@ -1340,9 +1340,10 @@ static int stream_grid_full(K kernel, int threads, size_t smem) {
     return grid;
 }
 
-// `work`: the stream entries the pass visits.  A small column gets one CTA
-// per 128 entries a thread, fewer than a full wave, so that the passes of
-// many small graphs on concurrent streams share the device.
+// `work` (>= 0 when many graphs' passes run side by side on concurrent
+// streams): the stream entries the pass visits; a small column then gets
+// one CTA per 128 entries a thread, fewer than a full wave, so that the
+// passes share the device.  A lone graph's passes take a full wave.
 template <class K>
 static int stream_grid(K kernel, int threads, size_t smem, long long work = -1) {
     int g = stream_grid_full(kernel, threads, smem);
@@ -1361,10 +1362,10 @@ static int grid_for(long long total, int threads) {
     return (int)b;
 }
 
-cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s) {
+cudaError_t launch_plain_energy(const EnergyArgs& a, cudaStream_t s, bool shared) {
     const size_t smem = a.hist0 ? 2 * kTopBins * sizeof(unsigned) : 0;
     note_launch();
-    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, smem, a.total), 256, smem, s>>>(a);
+    plain_energy_kernel<<<stream_grid(plain_energy_kernel, 256, smem, shared ? a.total : -1), 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_ho_energy(const EnergyArgs& a, cudaStream_t s) {
@@ -1385,7 +1386,8 @@ cudaError_t launch_quaternions(const QuatArgs& a, cudaStream_t s) {
 // zeroed counters; band: kMedianCompact doubles; count: one zeroed counter.
 cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHist, MedianState* st,
                                   unsigned long long* hist, double* band, unsigned long long* count, long long nValues,
-                                  double scaling, float* col32, double clip, bool allPasses, cudaStream_t s) {
+                                  double scaling, float* col32, double clip, bool allPasses, bool shared,
+                                  cudaStream_t s) {
     const size_t smem = sizeof(unsigned) << kMedianWideBits;
     {
         static std::mutex mu;
@@ -1401,8 +1403,8 @@ cudaError_t launch_median_rescale(const SelectArgs& a, unsigned long long* topHi
             done.insert(dev);
         }
     }
-    const int histGrid = stream_grid(median_hist_kernel, 512, smem, a.total);
-    const int grid = stream_grid(median_compact_kernel, 256, 0, a.total);
+    const int histGrid = stream_grid(median_hist_kernel, 512, smem, shared ? a.total : -1);
+    const int grid = stream_grid(median_compact_kernel, 256, 0, shared ? a.total : -1);
     SelectArgs h = a;
     h.hist = hist;
     if (topHist) {

@@ -603,7 +603,7 @@ void Graph::generate() {
             a.out1 = e64[1].p;
         }
         count_top_digits(a);
-        PGC_CUDA(launch_plain_energy(a, s));
+        PGC_CUDA(launch_plain_energy(a, s, blockingSync));  // batch workers share the device
     } else {
         const int cm = string_to_mode(costName), tm = string_to_mode(timeName);
         if (!ho_supported(cm, tm))
@@ -701,7 +701,7 @@ void Graph::rescale_columns(double scaling) {
         const bool top = topHistValid[col] && !allPasses;
         PGC_CUDA(launch_median_rescale(args(col), top ? topHist[col].p : nullptr, wMedState.p + col, wMedHist.p,
                                        wMedBand.p, wMedCount.p, count, scaling, e32[col].p, 100 * scaling, allPasses,
-                                       stream));
+                                       blockingSync, stream));
         stats.launches += (top ? 1 : 3) + (allPasses ? 10 : 2) + 4;
     };
     for (int col = 0; col < ncols; ++col) {
