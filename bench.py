@@ -766,7 +766,9 @@ def run_fwdbwd(args, world, rank):
     fY = [torch.tensor(p["fY"], device="cuda", requires_grad=True) for p in pairs]
 
     def step():
-        fds = [torch.cdist(a, b).double() for a, b in zip(fX, fY)]
+        # the pairs share their shapes: one batched distance computation (and
+        # one backward) for all of them, the same per-pair values
+        fds = torch.cdist(torch.stack(fX), torch.stack(fY)).double().unbind(0)
         lam = ratio_cycle_objectives(gens, fds, k)
         lam.sum().backward()
         return lam
@@ -822,7 +824,7 @@ def run_fwdbwd(args, world, rank):
     fresh = [make(p) for p in pairs]
     ax = [torch.from_numpy(p["fX"]).pin_memory().to("cuda", non_blocking=True).requires_grad_(True) for p in pairs]
     by = [torch.from_numpy(p["fY"]).pin_memory().to("cuda", non_blocking=True) for p in pairs]
-    lam_e = ratio_cycle_objectives(fresh, [torch.cdist(a, b).double() for a, b in zip(ax, by)], k)
+    lam_e = ratio_cycle_objectives(fresh, torch.cdist(torch.stack(ax), torch.stack(by)).double().unbind(0), k)
     lam_e.sum().backward()
     host_grads = [a.grad.cpu() for a in ax]
     e2e_s = time.perf_counter() - t0
